@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark of the batched LU chain on B200.
+
+Workload (one step): the plain FP32 chain at scale -- n = lda = 32, 131072 matrices,
+aclblasSgetrfBatched -> aclblasSgetrsBatched (trans N, nrhs = 4) -> aclblasSgetriBatched,
+A i.i.d. N(0,1), B i.i.d. U(-1,1), synthetic and seeded. Every step factors its own fresh
+copy of the inputs (getrf works in place), so each step reads 512 MiB of matrices that are
+not in L2 (126 MB) when the step starts; no L2 flush is needed.
+
+  value       matrices/s of the whole chain, device time, inputs resident in HBM;
+  e2e         the same through the C ABI from pinned host buffers: H2D of A and B, the chain,
+              D2H of X, inv(A) and info inside the timed region;
+  roofline    the dominant kernel's algorithmic bytes per launch / its CUDA-event duration,
+              against the measured HBM copy bandwidth (MEASURED_PEAKS.json);
+  cpu_baseline  the reference's CPU golden path (LAPACK through its test headers, built in
+              oracle/_ref) on a bounded sample, all host threads.
+
+--impl reference times that CPU golden path alone on the same workload (rank 0 only).
+Multi-GPU (torchrun): replicas only -- every rank runs its own batch, no collective on the
+data path; value = all ranks' matrices / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "getrf+getrs batched matrices/s: mixed/grouped vs plain FP32 at equal FP64 err"
+N, BATCH, NRHS = 32, 131072, 4
+FALLBACK_HBM_GBS = 6650.0
+
+# Algorithmic bytes per matrix (reads + writes of each kernel):
+#   getrf  8n^2 + 4n + 12          A read and written, pivots, info, pointer
+#   getrs  4n^2 + 4n + 8n*nrhs + 16  LU read, pivots, B read and written, two pointers
+#   getri  8n^2 + 4n + 20          LU read, C written, pivots, info, two pointers
+ALG_BYTES = {
+    "getrf": 8 * N * N + 4 * N + 12,
+    "getrs": 4 * N * N + 4 * N + 8 * N * NRHS + 16,
+    "getri": 8 * N * N + 4 * N + 20,
+}
+FLOPS = {"getrf": 2 * N ** 3 / 3, "getrs": 2 * N * N * NRHS, "getri": 4 * N ** 3 / 3}
+
+
+def load_package():
+    name = "ops_blas_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    path = os.path.join(ROOT, "ops-blas_b200", "__init__.py")
+    spec = importlib.util.spec_from_file_location(name, path, submodule_search_locations=[os.path.dirname(path)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """Samples SM clock and clock-event reasons through NVML while the timed region runs."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+    }
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self.nv:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons - {"gpu_idle"}), "samples": len(self.samples)}
+
+
+def cpu_reference_rate(n_sample, nthreads=0, reps=1):
+    """Matrices/s of the reference's CPU golden chain (getrf, getrs N nrhs=4, getri) on a
+    sample of n_sample matrices of the workload's distribution; all host threads by default."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    import oracle as O
+
+    rng = np.random.default_rng(123)
+    a = rng.standard_normal((n_sample, N, N)).astype(np.float32)
+    b = rng.uniform(-1, 1, (n_sample, NRHS, N)).astype(np.float32)
+    best = None
+    for _ in range(reps):
+        lu, x = a.copy(), b.copy()
+        c = np.empty_like(a)
+        t0 = time.perf_counter()
+        piv, _ = O.ref_getrf(lu, N, N, True, nthreads)
+        O.ref_getrs("N", lu, N, N, piv, x, NRHS, N, nthreads)
+        O.ref_getri(lu, N, N, piv, c, N, nthreads)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    cores = O.ref().ref_max_threads() if nthreads <= 0 else nthreads
+    return n_sample / best, cores, O.ref().ref_openblas_config().decode()
+
+
+def cpu_baseline(target_s=10.0):
+    """The reference golden chain sized to about target_s seconds of host time."""
+    rate, cores, cfg = cpu_reference_rate(2048)
+    sample = int(min(BATCH, max(2048, rate * target_s)))
+    rate, cores, cfg = cpu_reference_rate(sample)
+    return {"value": rate, "unit": "matrices/s", "cores": cores, "kind": "reference",
+            "sample": f"{sample} of the {BATCH} n=32 matrices (same distribution), getrf+getrs(nrhs=4)+getri, "
+                      f"reference golden headers over {cfg}, OpenMP over batch chunks"}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return None
+    sys.path.insert(0, ROOT)
+    import oracle as O
+
+    if O.ref() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/librefgold.so (the reference's CPU "
+                                                               "golden path) was not built on this machine"}))
+        return None
+    rate, cores, cfg = cpu_reference_rate(2048)
+    sample = int(min(BATCH, max(1024, rate * 2.0)))  # about 2 s per step
+    for _ in range(args.warmup):
+        cpu_reference_rate(sample)
+    times = []
+    for _ in range(args.steps):
+        r, cores, cfg = cpu_reference_rate(sample)
+        times.append(sample / r)
+    total = sum(times)
+    value = sample * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic seeded: A ~ N(0,1), B ~ U(-1,1)",
+        "config": {"workload": "lu_chain_n32_b131072", "n": N, "batch": BATCH, "nrhs": NRHS,
+                   "ops": "getrf+getrs(N)+getri", "step_sample": sample},
+        "cpu_baseline": {"value": value, "unit": "matrices/s", "cores": cores, "kind": "reference",
+                         "sample": f"{sample} matrices per step, reference golden headers over {cfg}"},
+        "e2e": {"value": value, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("OPSBLAS_BENCH_ALLOW_SHORT"), \
+        "at least 3 warm-up steps"
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ob = load_package()
+    h = ob.Handle()
+    stream = torch.cuda.current_stream()
+
+    nbuf = args.warmup + args.steps
+    g = torch.Generator(device=dev).manual_seed(1000 + rank)
+    A0 = [torch.randn((BATCH, N, N), device=dev, generator=g) for _ in range(nbuf)]
+    B0 = [torch.rand((BATCH, NRHS, N), device=dev, generator=g) * 2 - 1 for _ in range(nbuf)]
+    aptr = [ob.ptr_array(a) for a in A0]
+    bptr = [ob.ptr_array(b) for b in B0]
+    Cinv = torch.empty((BATCH, N, N), device=dev)
+    cptr = ob.ptr_array(Cinv)
+    piv = torch.empty((BATCH, N), dtype=torch.int32, device=dev)
+    info = torch.empty(BATCH, dtype=torch.int32, device=dev)
+    rinfo = torch.empty(BATCH, dtype=torch.int32, device=dev)
+
+    def step(i, ev=None):
+        if ev:
+            ev[0].record(stream)
+        h.getrf(A0[i], N, N, piv=piv, info=info, aptr=aptr[i])
+        if ev:
+            ev[1].record(stream)
+        h.getrs("N", A0[i], N, N, piv, B0[i], NRHS, N, aptr=aptr[i], bptr=bptr[i])
+        if ev:
+            ev[2].record(stream)
+        h.getri(A0[i], N, N, piv, Cinv, N, info=rinfo, aptr=aptr[i], cptr=cptr)
+        if ev:
+            ev[3].record(stream)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    assert int(info.max()) == 0 and int(rinfo.max()) == 0
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for s in range(args.steps):
+            step(args.warmup + s, evs[s])
+        stop.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = start.elapsed_time(stop)
+    per = {"getrf": [], "getrs": [], "getri": []}
+    for e in evs:
+        per["getrf"].append(e[0].elapsed_time(e[1]))
+        per["getrs"].append(e[1].elapsed_time(e[2]))
+        per["getri"].append(e[2].elapsed_time(e[3]))
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # e2e through the C ABI from pinned host memory
+    hostA = torch.empty((BATCH, N, N), dtype=torch.float32).pin_memory()
+    hostB = torch.empty((BATCH, NRHS, N), dtype=torch.float32).pin_memory()
+    hostA.copy_(A0[0].cpu())
+    hostB.copy_(B0[0].cpu())
+    hostX = torch.empty_like(hostB).pin_memory()
+    hostC = torch.empty_like(hostA).pin_memory()
+    hostI = torch.empty(BATCH, dtype=torch.int32).pin_memory()
+    dA, dB = A0[0], B0[0]
+
+    def e2e_step():
+        dA.copy_(hostA, non_blocking=True)
+        dB.copy_(hostB, non_blocking=True)
+        h.getrf(dA, N, N, piv=piv, info=info, aptr=aptr[0])
+        h.getrs("N", dA, N, N, piv, dB, NRHS, N, aptr=aptr[0], bptr=bptr[0])
+        h.getri(dA, N, N, piv, Cinv, N, info=rinfo, aptr=aptr[0], cptr=cptr)
+        hostX.copy_(dB, non_blocking=True)
+        hostC.copy_(Cinv, non_blocking=True)
+        hostI.copy_(rinfo, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = hostA.numel() * 4 + hostB.numel() * 4
+    d2h = hostX.numel() * 4 + hostC.numel() * 4 + hostI.numel() * 4
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        tot = {k: sum(v) for k, v in per.items()}
+        dom = max(tot, key=tot.get)
+        kern = {}
+        for k, v in per.items():
+            avg = sum(v) / len(v)
+            gbs = ALG_BYTES[k] * BATCH / (avg * 1e-3) / 1e9
+            kern[k] = {"ms_avg": avg, "GB_s": gbs, "frac_hbm": gbs / peak,
+                       "GFLOP_s": FLOPS[k] * BATCH / (avg * 1e-3) / 1e9}
+        traffic = profiled_traffic().get(dom)
+        line = {
+            "metric": METRIC,
+            "value": BATCH * world * args.steps / (ms * 1e-3),
+            "unit": "matrices/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic seeded: A ~ N(0,1), B ~ U(-1,1); fresh input copy per step, inputs (512 MiB) > L2",
+            "config": {"workload": "lu_chain_n32_b131072", "n": N, "lda": N, "batch_per_gpu": BATCH, "nrhs": NRHS,
+                       "ops": "getrf+getrs(N)+getri", "parallelism": f"replicas{world}", "l2": "inputs larger than L2"},
+            "kernels": kern,
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["GB_s"], "peak": peak,
+                         "unit": "GB/s", "frac": kern[dom]["frac_hbm"], "peak_source": peak_kind,
+                         "traffic": traffic, "alg_bytes_per_launch": ALG_BYTES[dom] * BATCH},
+            "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "matrices/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline()
+            except Exception as e:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+        print(json.dumps(line))
+    h.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,115 @@
+/*
+ * aclblas C API for the batched LU chain, B200 (sm_100a) build.
+ *
+ * Every entry point keeps the name, argument order, argument meaning, status codes and
+ * validation order of the hicann/ops-blas function it replaces (cited per declaration), so that
+ * code written against the reference's include/cann_ops_blas.h links against
+ * libopsblas_b200.so unchanged. `aclrtStream` is a CUDA stream (include/acl/acl.h).
+ *
+ * Conventions shared by every batched routine:
+ *   - matrices are FP32, column-major, element (i, j) at A[i + j * lda];
+ *   - `Aarray` / `Barray` / `Carray` are DEVICE arrays of DEVICE pointers, one per matrix;
+ *   - pivot and info arrays are DEVICE memory unless stated otherwise;
+ *   - calls are asynchronous on the handle's stream: they never synchronise, never copy
+ *     between host and device and never allocate, so they can be captured in a CUDA graph.
+ */
+#ifndef OPSBLAS_B200_CANN_OPS_BLAS_H
+#define OPSBLAS_B200_CANN_OPS_BLAS_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include "acl/acl.h"
+#include "cann_ops_blas_common.h"
+
+#if defined(__GNUC__)
+#define ACLBLAS_EXPORT __attribute__((visibility("default")))
+#else
+#define ACLBLAS_EXPORT
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct _aclblas_handle* aclblasHandle_t;
+typedef void (*aclblasLogCallback)(const char*);
+
+/* ---------------------------------------------------------------- handle and runtime --- */
+
+/* Replaces aclblasCreate (include/cann_ops_blas.h:41; blas/common/helper/aclblas_auxiliary.cpp:24-48).
+ * *handle must be NULL on entry. Allocates the 32 MiB default device workspace on the current
+ * device. HANDLE_IS_NULLPTR if handle is NULL, INVALID_VALUE if *handle is not NULL,
+ * ALLOC_FAILED if the workspace cannot be allocated. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasCreate(aclblasHandle_t* handle);
+
+/* Replaces aclblasDestroy (include/cann_ops_blas.h:54; aclblas_auxiliary.cpp:50-71).
+ * Synchronises the bound stream, frees the library workspace, never frees user workspace.
+ * EXECUTION_FAILED if the stream synchronisation fails. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasDestroy(aclblasHandle_t handle);
+
+/* Replaces aclblasSetStream (include/cann_ops_blas.h:66; aclblas_auxiliary.cpp:73-90).
+ * Switching streams reverts the handle to the library workspace. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSetStream(aclblasHandle_t handle, aclrtStream stream);
+
+/* Replaces aclblasGetStream (include/cann_ops_blas.h:76; aclblas_auxiliary.cpp:92-104). */
+ACLBLAS_EXPORT aclblasStatus_t aclblasGetStream(aclblasHandle_t handle, aclrtStream* stream);
+
+/* Replaces aclblasSetWorkspace (include/cann_ops_blas.h:93; aclblas_auxiliary.cpp:106-137).
+ * Borrows user device memory; grow-only (a smaller size than the current user workspace is
+ * ignored). INVALID_VALUE if workspace is NULL or workspaceSize is 0. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSetWorkspace(aclblasHandle_t handle, void* workspace, size_t workspaceSize);
+
+/* Replaces aclblasGetVersion (include/cann_ops_blas.h:105; aclblas_auxiliary.cpp:139-148).
+ * MAJOR*10000 + MINOR*100 + PATCH; handle may be NULL. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasGetVersion(aclblasHandle_t handle, int* version);
+
+/* Replace the logger trio (include/cann_ops_blas.h:116-133;
+ * blas/common/helper/aclblas_logger_manager.cpp:19-48). Unlike the reference, whose
+ * configuration is stored but never consumed, messages of this library (validation failures,
+ * launch errors) are delivered to the callback, stdout, stderr and/or the file. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasLoggerConfigure(int logIsOn, int logToStdOut, int logToStdErr, const char* logFile);
+ACLBLAS_EXPORT aclblasStatus_t aclblasSetLoggerCallback(aclblasLogCallback userCallback);
+ACLBLAS_EXPORT aclblasStatus_t aclblasGetLoggerCallback(aclblasLogCallback* userCallback);
+
+/* ------------------------------------------------------------------ batched LU chain --- */
+
+/* Replaces aclblasSgetrfBatched (include/cann_ops_blas.h:403;
+ * blas/getrf_batched/arch35/sgetrf_batched_host.cpp:66-118, kernel sgetrf_batched_kernel.cpp:106-197).
+ * In-place P*A = L*U with partial pivoting; PivotArray == NULL selects no pivoting.
+ * PivotArray: n ints per matrix, 1-based. infoArray: one int per matrix, 0 or the 1-based
+ * column of the first exactly-zero pivot; factorisation of that matrix stops there.
+ * Validation order (sgetrf_batched_host.cpp:32-64): n < 0, batchSize < 0, lda < max(1,n)
+ * -> INVALID_VALUE; n == 0 or batchSize == 0 -> SUCCESS with nothing touched;
+ * Aarray == NULL, or PivotArray != NULL with infoArray == NULL -> INVALID_VALUE.
+ * Deliberate strengthening: for a singular matrix (info = k > 0) PivotArray[k..n-1] is
+ * written as 0, the value the reference's golden model expects
+ * (test/getrf_batched/sgetrf_batched/sgetrf_batched_golden.h:78-82) and its test wrapper
+ * only gets by pre-zeroing. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfBatched(
+    aclblasHandle_t handle, int n, float* const Aarray[], int lda, int* PivotArray, int* infoArray, int batchSize);
+
+/* Replaces aclblasSgetrsBatched (include/cann_ops_blas.h:457;
+ * blas/getrs_batched/arch35/sgetrs_batched_host.cpp:49-185, kernel sgetrs_batched_kernel.cpp:83-388).
+ * Solves op(A) X = B with the LU factors and pivots of aclblasSgetrfBatched; B is overwritten
+ * by X. devIpiv == NULL means no pivoting. `info` is a HOST pointer (may be NULL) that receives
+ * 0, or -position of the first invalid argument (trans=2, n=3, nrhs=4, Aarray=5, lda=6,
+ * Barray=8, ldb=9, batchCount=11). An invalid trans returns INVALID_ENUM; nrhs is limited to
+ * 0..256 as in the reference. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrsBatched(
+    aclblasHandle_t handle, aclblasOperation_t trans, int n, int nrhs, const float* const Aarray[], int lda,
+    const int* devIpiv, float* const Barray[], int ldb, int* info, int batchCount);
+
+/* Replaces aclblasSgetriBatched (include/cann_ops_blas.h:430;
+ * blas/getri_batched/arch35/getri_batched_host.cpp:27-127, kernel getri_batched_kernel.cpp:39-308).
+ * Carray[i] = inverse of the matrix whose LU factors are in Aarray[i] (out of place; C must
+ * not alias A). PivotArray == NULL means no pivoting. infoArray (required) receives 0, or j+1
+ * for the highest-index j with U(j,j) == 0 (the reference's backward sweep stops there). */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetriBatched(
+    aclblasHandle_t handle, int n, const float* const Aarray[], int lda, const int* PivotArray,
+    float* const Carray[], int ldc, int* infoArray, int batchSize);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OPSBLAS_B200_CANN_OPS_BLAS_H */

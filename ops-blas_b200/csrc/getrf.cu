@@ -1,0 +1,263 @@
+// aclblasSgetrfBatched: batched LU factorisation with partial pivoting, FP32, column-major.
+//
+// Replaces blas/getrf_batched/arch35/sgetrf_batched_host.cpp:32-118 (host) and
+// sgetrf_batched_kernel.cpp:38-221 (device) of the reference. The arithmetic is the
+// reference's unblocked right-looking LU: first-maximum pivot search (FindPivotRow :52-79),
+// full-row interchange (SwapRows :81-91), multipliers by true division (ComputeMultipliers
+// :93-104), rank-1 update (Rank1Update :38-50), stop at the first exactly-zero pivot
+// (:127-137). The B200 kernels are:
+//   n <= 32 : getrf_small_kernel, one warp segment per matrix, rows in registers;
+//   n  > 32 : getrf_generic_kernel, one CTA per matrix, matrix in global memory.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+#include "small_common.cuh"
+
+namespace opsblas {
+
+// ---------------------------------------------------------------------------------------
+// n <= 32. Lane r of a segment holds row r of its matrix in registers a[0..n-1].
+// Pivoting is implicit: rows never move between lanes during the factorisation; `pos` is
+// the row index the lane's row currently has in the reference's in-place matrix, and rows
+// are stored at `pos` at the end. Per column k:
+//   1. argmax of |a[k]| over lanes with pos >= k (redux.sync), ties to the lowest pos --
+//      identical to the reference's first-maximum rule, zero/NaN never chosen;
+//   2. the pivot lane publishes its row (from column k on) in shared memory; every lane
+//      reads it back with broadcast 16-byte loads;
+//   3. lanes below the pivot form l = a[k] / pivot and update a[j] -= l * u[j], j > k.
+// Arithmetic per element is the reference's, in its order, one fmaf per update.
+// ---------------------------------------------------------------------------------------
+template <int N, bool PIVOT>
+__global__ void __launch_bounds__(kSmallWarps * 32)
+getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__ piv, int* __restrict__ info,
+                   int batch)
+{
+    using S = SmallShape<N>;
+    __shared__ __align__(16) float rowbuf[kSmallWarps][2][32];
+
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int seg = lane / S::SEG;
+    const int r = lane % S::SEG;
+    const long long m = ((long long)blockIdx.x * kSmallWarps + warp) * S::MPW + seg;
+    const bool mvalid = m < batch;
+    const bool rvalid = mvalid && r < N;
+
+    float* A = mvalid ? Aarray[m] : nullptr;
+    float a[S::NP];
+#pragma unroll
+    for (int j = 0; j < S::NP; j++) a[j] = 0.0f;
+    if (rvalid) {
+#pragma unroll
+        for (int j = 0; j < N; j++) a[j] = A[r + (long long)j * lda];
+    }
+
+    int pos = r;
+    int mypiv = 0;
+    int inf = 0;  // uniform within a segment
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        float* buf = &rowbuf[warp][k & 1][seg * S::SEG];
+        const bool live = rvalid && inf == 0;
+        int prow = k;
+        bool ispiv;
+        if (PIVOT) {
+            const bool elig = live && pos >= k;
+            const float v = fabsf(a[k]);
+            const unsigned key = (elig && v > 0.0f) ? __float_as_uint(v) : 0u;
+            prow = (int)seg_argmax<S::SEG>(key, elig ? (unsigned)pos : 0xffffffffu, seg);
+            ispiv = elig && pos == prow;
+        } else {
+            ispiv = live && pos == k;
+        }
+        if (ispiv) {
+#pragma unroll
+            for (int c = k / 4; c < S::NC; c++)
+                reinterpret_cast<float4*>(buf)[c] = make_float4(a[4 * c], a[4 * c + 1], a[4 * c + 2], a[4 * c + 3]);
+        }
+        __syncwarp();
+        const float4 ck = reinterpret_cast<const float4*>(buf)[k / 4];
+        const float pv = f4get(ck, k % 4);
+        if (mvalid && inf == 0) {
+            if (PIVOT && r == k) mypiv = prow + 1;
+            if (pv == 0.0f) inf = k + 1;
+        }
+        if (live && inf == 0) {
+            if (ispiv)
+                pos = k;
+            else if (pos == k)
+                pos = prow;
+            if (pos > k) {
+                const float l = a[k] / pv;
+                a[k] = l;
+#pragma unroll
+                for (int j = k + 1; j < 4 * (k / 4) + 4 && j < N; j++) a[j] = fmaf(-l, f4get(ck, j % 4), a[j]);
+#pragma unroll
+                for (int c = k / 4 + 1; c < S::NC; c++) {
+                    const float4 u = reinterpret_cast<const float4*>(buf)[c];
+                    if (4 * c + 0 < N) a[4 * c + 0] = fmaf(-l, u.x, a[4 * c + 0]);
+                    if (4 * c + 1 < N) a[4 * c + 1] = fmaf(-l, u.y, a[4 * c + 1]);
+                    if (4 * c + 2 < N) a[4 * c + 2] = fmaf(-l, u.z, a[4 * c + 2]);
+                    if (4 * c + 3 < N) a[4 * c + 3] = fmaf(-l, u.w, a[4 * c + 3]);
+                }
+            }
+        }
+    }
+
+    if (rvalid) {
+#pragma unroll
+        for (int j = 0; j < N; j++) A[pos + (long long)j * lda] = a[j];
+        if (PIVOT) piv[m * N + r] = mypiv;
+        if (r == 0 && info != nullptr) info[m] = inf;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// n > 32: one CTA per matrix working in global memory (L1/L2 resident). Warp 0 searches the
+// pivot, the CTA swaps rows, forms multipliers, and applies the rank-1 update with one thread
+// per trailing row (coalesced along the column).
+// ---------------------------------------------------------------------------------------
+constexpr int kGenericThreads = 256;
+
+template <bool PIVOT>
+__global__ void __launch_bounds__(kGenericThreads)
+getrf_generic_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __restrict__ piv, int* __restrict__ info)
+{
+    const long long m = blockIdx.x;
+    float* A = Aarray[m];
+    int* pm = PIVOT ? piv + m * n : nullptr;
+    __shared__ int s_prow;
+    __shared__ float s_pv;
+    const int tid = threadIdx.x;
+    int inf = 0;
+    int k;
+    for (k = 0; k < n; k++) {
+        const float* colk = A + (long long)k * lda;
+        if (PIVOT) {
+            if (tid < 32) {
+                float best = 0.0f;
+                int brow = k;
+                for (int rr = k + tid; rr < n; rr += 32) {
+                    const float v = fabsf(colk[rr]);
+                    if (v > best) {
+                        best = v;
+                        brow = rr;
+                    }
+                }
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+                    const int orow = __shfl_xor_sync(0xffffffffu, brow, off);
+                    if (ob > best || (ob == best && orow < brow)) {
+                        best = ob;
+                        brow = orow;
+                    }
+                }
+                if (tid == 0) {
+                    s_prow = brow;
+                    s_pv = colk[brow];
+                }
+            }
+        } else if (tid == 0) {
+            s_prow = k;
+            s_pv = colk[k];
+        }
+        __syncthreads();
+        const int p = s_prow;
+        const float pv = s_pv;
+        if (PIVOT && tid == 0) pm[k] = p + 1;
+        if (pv == 0.0f) {
+            inf = k + 1;
+            break;
+        }
+        if (p != k) {
+            for (int c = tid; c < n; c += kGenericThreads) {
+                float* col = A + (long long)c * lda;
+                const float t = col[k];
+                col[k] = col[p];
+                col[p] = t;
+            }
+        }
+        __syncthreads();
+        float* ck = A + (long long)k * lda;
+        for (int i = k + 1 + tid; i < n; i += kGenericThreads) {
+            const float l = ck[i] / pv;
+            ck[i] = l;
+            for (int j = k + 1; j < n; j++) {
+                float* cj = A + (long long)j * lda;
+                cj[i] = fmaf(-l, cj[k], cj[i]);
+            }
+        }
+        __syncthreads();
+    }
+    if (PIVOT && inf) {
+        for (int kk = k + 1 + tid; kk < n; kk += kGenericThreads) pm[kk] = 0;
+    }
+    if (tid == 0 && info != nullptr) info[m] = inf;
+}
+
+}  // namespace opsblas
+
+using namespace opsblas;
+
+extern "C" aclblasStatus_t aclblasSgetrfBatched(
+    aclblasHandle_t handle, int n, float* const Aarray[], int lda, int* PivotArray, int* infoArray, int batchSize)
+{
+    static const char* kApi = "aclblasSgetrfBatched";
+    if (handle == nullptr) {
+        log_error(kApi, "handle is nullptr");
+        return ACLBLAS_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (n < 0) {
+        log_error(kApi, "n must be >= 0, got %d", n);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (batchSize < 0) {
+        log_error(kApi, "batchSize must be >= 0, got %d", batchSize);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (lda < max1(n)) {
+        log_error(kApi, "lda must be >= max(1, n), got lda=%d, n=%d", lda, n);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (n == 0 || batchSize == 0) return ACLBLAS_STATUS_SUCCESS;
+    if (Aarray == nullptr) {
+        log_error(kApi, "Aarray must not be nullptr");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (PivotArray != nullptr && infoArray == nullptr) {
+        log_error(kApi, "infoArray must not be nullptr when PivotArray is provided");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+
+    cudaStream_t st = handle->stream;
+    const bool pivot = PivotArray != nullptr;
+    if (n <= 32) {
+        switch (n) {
+#define OPSBLAS_GETRF_CASE(NN)                                                                                      \
+    case NN: {                                                                                                      \
+        constexpr int per_cta = kSmallWarps * SmallShape<NN>::MPW;                                                  \
+        const unsigned grid = (unsigned)((batchSize + per_cta - 1) / per_cta);                                      \
+        if (pivot)                                                                                                  \
+            getrf_small_kernel<NN, true><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, PivotArray, infoArray,     \
+                                                                            batchSize);                             \
+        else                                                                                                        \
+            getrf_small_kernel<NN, false><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, nullptr, infoArray,       \
+                                                                             batchSize);                            \
+        break;                                                                                                      \
+    }
+            OPSBLAS_FOR_N_1_32(OPSBLAS_GETRF_CASE)
+#undef OPSBLAS_GETRF_CASE
+            default:
+                break;
+        }
+    } else {
+        if (pivot)
+            getrf_generic_kernel<true><<<(unsigned)batchSize, kGenericThreads, 0, st>>>(Aarray, n, lda, PivotArray,
+                                                                                      infoArray);
+        else
+            getrf_generic_kernel<false><<<(unsigned)batchSize, kGenericThreads, 0, st>>>(Aarray, n, lda, nullptr,
+                                                                                       infoArray);
+    }
+    return launch_status(kApi, cudaGetLastError());
+}

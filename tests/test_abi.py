@@ -1,0 +1,177 @@
+"""C-ABI checks that need no GPU: the library loads, exports every entry point that
+include/*.h declares, and applies the reference's host-side validation (status codes, their
+order, getrs' -position info) before touching any device state.
+
+Validation failures and the n == 0 / batch == 0 no-op paths return before the handle is
+dereferenced (as in sgetrf_batched_host.cpp:66-84), so these tests pass a non-null dummy
+handle and dummy non-null pointers, which are never read.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import glob
+import os
+import re
+
+import pytest
+
+from cases import GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS
+from conftest import ROOT
+
+DUMMY = C.create_string_buffer(256)
+H = C.cast(DUMMY, C.c_void_p)
+P = C.c_void_p(0x1000)  # non-null, never dereferenced on these paths
+
+
+def declared_symbols():
+    names = []
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        names += re.findall(r"^\s*(?:ACLBLAS_EXPORT\s+)?aclblasStatus_t\s+(aclblas\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(ob):
+    lib = ob.lib()
+    names = declared_symbols()
+    assert len(names) >= 12
+    for name in names:
+        assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+    assert set(names) == set(ob.SIGNATURES), "the Python binding must cover exactly the declared API"
+
+
+def test_status_and_operation_values_match_reference(ob):
+    text = open(os.path.join(ROOT, "include", "cann_ops_blas_common.h")).read()
+    vals = dict(re.findall(r"ACLBLAS_STATUS_(\w+)\s*=\s*(\d+)", text))
+    for code, name in ob.STATUS.items():
+        assert int(vals[name]) == code
+    assert (ob.OP_N, ob.OP_T, ob.OP_C) == (111, 112, 113)
+
+
+def test_version(ob):
+    v = C.c_int(0)
+    assert ob.lib().aclblasGetVersion(None, C.byref(v)) == ob.SUCCESS
+    assert v.value == 10000
+    assert ob.lib().aclblasGetVersion(None, None) == ob.INVALID_VALUE
+
+
+def test_handle_argument_checks(ob):
+    L = ob.lib()
+    assert L.aclblasCreate(None) == ob.HANDLE_IS_NULLPTR
+    h = C.c_void_p(0x10)
+    assert L.aclblasCreate(C.byref(h)) == ob.INVALID_VALUE  # *handle must be NULL
+    assert L.aclblasDestroy(None) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSetStream(None, None) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasGetStream(None, None) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasGetStream(H, None) == ob.INVALID_VALUE
+    assert L.aclblasSetWorkspace(None, P, 16) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSetWorkspace(H, None, 16) == ob.INVALID_VALUE
+    assert L.aclblasSetWorkspace(H, P, 0) == ob.INVALID_VALUE
+
+
+def test_create_without_device_fails_cleanly(ob):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    h = C.c_void_p()
+    st = ob.lib().aclblasCreate(C.byref(h))
+    assert st in (ob.NOT_INITIALIZED, ob.ALLOC_FAILED)
+    assert not h.value
+
+
+@pytest.mark.parametrize("row", GETRF_ERRORS, ids=lambda r: r[0])
+def test_getrf_error_rows(ob, row):
+    name, n, lda, batch, null_a, null_info, null_h, status = row
+    st = ob.lib().aclblasSgetrfBatched(None if null_h else H, n, None if null_a else P, lda, P,
+                                       None if null_info else P, batch)
+    assert ob.STATUS[st] == status
+
+
+def test_getrf_validation_order(ob):
+    L = ob.lib()
+    # lda is checked before the n == 0 no-op (sgetrf_batched_host.cpp:43-52)
+    assert L.aclblasSgetrfBatched(H, 0, None, 0, None, None, 4) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfBatched(H, 0, None, 1, None, None, 4) == ob.SUCCESS
+    assert L.aclblasSgetrfBatched(H, 8, None, 8, None, None, 0) == ob.SUCCESS
+    # no-pivot mode may omit infoArray; pivot mode may not
+    assert L.aclblasSgetrfBatched(H, 8, None, 8, None, None, 2) == ob.INVALID_VALUE  # Aarray NULL
+    assert L.aclblasSgetrfBatched(H, 8, P, 8, P, None, 2) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfBatched(None, -1, None, 0, None, None, -1) == ob.HANDLE_IS_NULLPTR
+
+
+@pytest.mark.parametrize("row", GETRS_ERRORS, ids=lambda r: r[0])
+def test_getrs_error_rows(ob, row):
+    name, trans, n, nrhs, lda, ldb, batch, null_a, null_b, null_h, status, exp_info = row
+    info = C.c_int(12345)
+    t = 999 if trans == "INVALID" else ob.TRANS[trans]
+    st = ob.lib().aclblasSgetrsBatched(None if null_h else H, t, n, nrhs, None if null_a else P, lda, P,
+                                       None if null_b else P, ldb, C.byref(info), batch)
+    assert ob.STATUS[st] == status
+    if exp_info is None:
+        assert info.value == 12345  # handle errors leave info untouched
+    else:
+        assert info.value == exp_info
+
+
+def test_getrs_info_and_noop(ob):
+    L = ob.lib()
+    info = C.c_int(-99)
+    # valid no-op calls set *info = 0 (sgetrs_batched_host.cpp:178-182) without touching arrays
+    assert L.aclblasSgetrsBatched(H, ob.OP_N, 0, 4, None, 1, None, None, 1, C.byref(info), 4) == ob.SUCCESS
+    assert info.value == 0
+    info.value = -99
+    assert L.aclblasSgetrsBatched(H, ob.OP_T, 32, 0, None, 32, None, None, 32, C.byref(info), 4) == ob.SUCCESS
+    assert info.value == 0
+    # info may be NULL
+    assert L.aclblasSgetrsBatched(H, ob.OP_N, 32, 4, None, 32, None, P, 32, None, 4) == ob.INVALID_VALUE
+    # position precedence: trans beats n
+    info.value = 0
+    assert L.aclblasSgetrsBatched(H, 0, -1, -1, None, 0, None, None, 0, C.byref(info), -1) == ob.INVALID_ENUM
+    assert info.value == -2
+
+
+@pytest.mark.parametrize("row", GETRI_ERRORS, ids=lambda r: r[0])
+def test_getri_error_rows(ob, row):
+    name, n, lda, ldc, batch, null_a, null_c, null_info, null_h, status = row
+    st = ob.lib().aclblasSgetriBatched(None if null_h else H, n, None if null_a else P, lda, P,
+                                       None if null_c else P, ldc, None if null_info else P, batch)
+    assert ob.STATUS[st] == status
+
+
+def test_getri_noop_and_null_handle(ob):
+    L = ob.lib()
+    assert L.aclblasSgetriBatched(None, 32, None, 32, None, None, 32, None, 4) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSgetriBatched(H, 0, None, 1, None, None, 1, None, 4) == ob.SUCCESS
+    assert L.aclblasSgetriBatched(H, 32, None, 32, None, None, 32, None, 0) == ob.SUCCESS
+
+
+def test_logger_callback_receives_validation_errors(ob):
+    L = ob.lib()
+    seen = []
+    cb_t = C.CFUNCTYPE(None, C.c_char_p)
+    cb = cb_t(lambda msg: seen.append(msg.decode()))
+    assert L.aclblasSetLoggerCallback(C.cast(cb, C.c_void_p)) == ob.SUCCESS
+    got = C.c_void_p()
+    assert L.aclblasGetLoggerCallback(C.byref(got)) == ob.SUCCESS
+    assert got.value == C.cast(cb, C.c_void_p).value
+    try:
+        assert L.aclblasSgetrfBatched(H, -3, P, 1, P, P, 1) == ob.INVALID_VALUE
+    finally:
+        L.aclblasSetLoggerCallback(None)
+    assert any("aclblasSgetrfBatched" in s and "n must be >= 0" in s for s in seen)
+    assert L.aclblasGetLoggerCallback(None) == ob.INVALID_VALUE
+    assert L.aclblasLoggerConfigure(0, 0, 0, None) == ob.SUCCESS
+
+
+def test_logger_file_sink(ob, tmp_path):
+    L = ob.lib()
+    path = str(tmp_path / "log.txt").encode()
+    buf = C.create_string_buffer(path)
+    assert L.aclblasLoggerConfigure(1, 0, 0, buf) == ob.SUCCESS
+    try:
+        L.aclblasSgetriBatched(H, 5, P, 3, P, P, 5, P, 4)
+    finally:
+        L.aclblasLoggerConfigure(0, 0, 0, None)
+    text = open(path.decode()).read()
+    assert "lda must be >= max(1, n)" in text
