@@ -269,9 +269,11 @@ def test_chain_n32_at_scale_properties(handle):
     den = Am.abs().sum(2).amax(1) * X.double().abs().amax((1, 2)) + B0.double().abs().amax((1, 2))
     berr = R.abs().amax((1, 2)) / den
     assert float(berr.max()) < 1e-5
-    E = Am @ Cinv.double().transpose(1, 2) - torch.eye(n, device="cuda", dtype=torch.float64)
-    kap = torch.linalg.cond(Am)
-    assert float((E.abs().amax((1, 2)) / kap).max()) < 1e-5
+    # a column-wise backward-stable inverse satisfies ||A C - I|| <= c n eps ||A|| ||C||
+    Cm = Cinv.double().transpose(1, 2)
+    E = Am @ Cm - torch.eye(n, device="cuda", dtype=torch.float64)
+    scale = Am.abs().sum(2).amax(1) * Cm.abs().sum(2).amax(1)
+    assert float((E.abs().sum(2).amax(1) / scale).max()) < 1e-5
     # bit-exact parity on a sample
     idx = torch.randperm(batch, generator=torch.Generator().manual_seed(0))[:256].numpy()
     a = to_host(A0)[idx].copy()
