@@ -56,9 +56,12 @@ def gpu_getri(handle, lu, n, lda, piv, ldc):
 
 
 def assert_bitwise(x, y, what):
-    xb = np.ascontiguousarray(x).view(np.uint32)
-    yb = np.ascontiguousarray(y).view(np.uint32)
-    bad = np.flatnonzero(xb.ravel() != yb.ravel())
+    """Bit-for-bit equality; NaNs compare equal whatever their payload (CPU and GPU NaNs
+    carry different payloads)."""
+    xa, ya = np.ascontiguousarray(x), np.ascontiguousarray(y)
+    xb, yb = xa.view(np.uint32).ravel(), ya.view(np.uint32).ravel()
+    both_nan = np.isnan(xa).ravel() & np.isnan(ya).ravel()
+    bad = np.flatnonzero((xb != yb) & ~both_nan)
     assert bad.size == 0, f"{what}: {bad.size} elements differ, first at {bad[:5]}: " \
                           f"{x.ravel()[bad[:5]]} vs {y.ravel()[bad[:5]]}"
 
