@@ -28,11 +28,12 @@ namespace opsblas {
 // Arithmetic per element is the reference's, in its order, one fmaf per update.
 // ---------------------------------------------------------------------------------------
 template <int N, bool PIVOT>
-__global__ void __launch_bounds__(kSmallWarps * 32)
+__global__ void __launch_bounds__(kSmallWarps * 32, N > 16 ? 4 : (N > 8 ? 5 : 6))
 getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__ piv, int* __restrict__ info,
                    int batch)
 {
     using S = SmallShape<N>;
+    constexpr int NPAIR = S::NP / 2;
     __shared__ __align__(16) float rowbuf[kSmallWarps][2][32];
 
     const int lane = threadIdx.x & 31;
@@ -43,13 +44,15 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
     const bool mvalid = m < batch;
     const bool rvalid = mvalid && r < N;
 
+    // Row r in registers as pairs a2[p] = (a[2p], a[2p+1]); padding entries stay zero.
     float* A = mvalid ? Aarray[m] : nullptr;
-    float a[S::NP];
+    float2 a2[NPAIR];
 #pragma unroll
-    for (int j = 0; j < S::NP; j++) a[j] = 0.0f;
+    for (int p = 0; p < NPAIR; p++) a2[p] = make_float2(0.0f, 0.0f);
     if (rvalid) {
+        const float* Ar = A + r;
 #pragma unroll
-        for (int j = 0; j < N; j++) a[j] = A[r + (long long)j * lda];
+        for (int j = 0; j < N; j++) pset(a2, j, Ar[(long long)j * lda]);
     }
 
     int pos = r;
@@ -59,11 +62,12 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
     for (int k = 0; k < N; k++) {
         float* buf = &rowbuf[warp][k & 1][seg * S::SEG];
         const bool live = rvalid && inf == 0;
+        const float ak = pget(a2, k);
         int prow = k;
         bool ispiv;
         if (PIVOT) {
             const bool elig = live && pos >= k;
-            const float v = fabsf(a[k]);
+            const float v = fabsf(ak);
             const unsigned key = (elig && v > 0.0f) ? __float_as_uint(v) : 0u;
             prow = (int)seg_argmax<S::SEG>(key, elig ? (unsigned)pos : 0xffffffffu, seg);
             ispiv = elig && pos == prow;
@@ -73,7 +77,8 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
         if (ispiv) {
 #pragma unroll
             for (int c = k / 4; c < S::NC; c++)
-                reinterpret_cast<float4*>(buf)[c] = make_float4(a[4 * c], a[4 * c + 1], a[4 * c + 2], a[4 * c + 3]);
+                reinterpret_cast<float4*>(buf)[c] = make_float4(a2[2 * c].x, a2[2 * c].y, a2[2 * c + 1].x,
+                                                                a2[2 * c + 1].y);
         }
         __syncwarp();
         const float4 ck = reinterpret_cast<const float4*>(buf)[k / 4];
@@ -88,25 +93,27 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
             else if (pos == k)
                 pos = prow;
             if (pos > k) {
-                const float l = a[k] / pv;
-                a[k] = l;
+                // Multiplier by true division, then a[j] -= l * u[j] for j > k as one fma each;
+                // fma(u, -l, a) == fma(-l, u, a) exactly, two columns per packed instruction.
+                const float l = ak / pv;
+                pset(a2, k, l);
+                const float2 nl = make_float2(-l, -l);
+                if ((k & 1) == 0 && k + 1 < N) a2[k >> 1].y = fmaf(-l, f4get(ck, (k + 1) % 4), a2[k >> 1].y);
 #pragma unroll
-                for (int j = k + 1; j < 4 * (k / 4) + 4 && j < N; j++) a[j] = fmaf(-l, f4get(ck, j % 4), a[j]);
-#pragma unroll
-                for (int c = k / 4 + 1; c < S::NC; c++) {
-                    const float4 u = reinterpret_cast<const float4*>(buf)[c];
-                    if (4 * c + 0 < N) a[4 * c + 0] = fmaf(-l, u.x, a[4 * c + 0]);
-                    if (4 * c + 1 < N) a[4 * c + 1] = fmaf(-l, u.y, a[4 * c + 1]);
-                    if (4 * c + 2 < N) a[4 * c + 2] = fmaf(-l, u.z, a[4 * c + 2]);
-                    if (4 * c + 3 < N) a[4 * c + 3] = fmaf(-l, u.w, a[4 * c + 3]);
+                for (int c = k / 4; c < S::NC; c++) {
+                    const float4 u = (c == k / 4) ? ck : reinterpret_cast<const float4*>(buf)[c];
+                    if (2 * c >= (k + 2) / 2 && 4 * c < N) a2[2 * c] = __ffma2_rn(make_float2(u.x, u.y), nl, a2[2 * c]);
+                    if (2 * c + 1 >= (k + 2) / 2 && 4 * c + 2 < N)
+                        a2[2 * c + 1] = __ffma2_rn(make_float2(u.z, u.w), nl, a2[2 * c + 1]);
                 }
             }
         }
     }
 
     if (rvalid) {
+        float* Ap = A + pos;
 #pragma unroll
-        for (int j = 0; j < N; j++) A[pos + (long long)j * lda] = a[j];
+        for (int j = 0; j < N; j++) Ap[(long long)j * lda] = pget(a2, j);
         if (PIVOT) piv[m * N + r] = mypiv;
         if (r == 0 && info != nullptr) info[m] = inf;
     }

@@ -7,10 +7,10 @@
 // the reference leaves C as the forward-solve result for n <= 8 (its register path,
 // :163-168) and partially back-substituted for n > 8; both are kept.
 // B200 kernels:
-//   n <= 32 : getri_small_kernel. LU of each matrix is staged in shared memory (coalesced
-//             loads), lane c of a warp segment solves column c of C in registers reading L/U
-//             with broadcast 16-byte loads, and C leaves through shared memory as coalesced
-//             column stores.
+//   n <= 32 : getri_small_kernel. LU of each matrix is staged in shared memory (cp.async),
+//             lane c of a warp segment solves column c of C in registers (two rows per packed
+//             f32x2 FMA) reading L/U with broadcast 16-byte loads, and C leaves through shared
+//             memory as coalesced column stores.
 //   n  > 32 : getri_generic_kernel, thread per column of C in global memory.
 #include <cuda_runtime.h>
 
@@ -20,21 +20,22 @@
 namespace opsblas {
 
 template <int N>
-__global__ void __launch_bounds__(kSmallWarps * 32)
+__global__ void __launch_bounds__(kSmallWarps * 32, N > 16 ? 3 : 4)
 getri_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* __restrict__ ipiv,
                    float* const* __restrict__ Carray, int ldc, int* __restrict__ info, int batch)
 {
     using S = SmallShape<N>;
     constexpr int NP = S::NP;
-    // LU is staged column-major with column stride NP (16-byte aligned columns for the float4
-    // broadcast reads); C is staged with an odd column stride SS so that lane c writing its
-    // column is free of bank conflicts. Segments are offset by 16 bytes so that the broadcast
-    // reads of different segments fall in different banks.
-    constexpr int SS = (N % 2 == 0) ? N + 1 : N + 2;
-    constexpr int BIG = (N * NP > N * SS) ? N * NP : N * SS;
-    constexpr int MAT = ((BIG + 31) / 32) * 32 + 4;
+    constexpr int NC = S::NC;
+    constexpr int NPAIR = NP / 2;
+    // Per matrix: N columns of NP floats. LU is staged column-major (16-byte aligned columns
+    // for the float4 broadcast reads). C is staged in the same space with the 16-byte chunks
+    // of column c rotated by c (chunk q of column c at slot (q + c) % NC), so that the 32
+    // lanes writing their columns chunk-wise hit distinct banks. Matrices are 16 bytes apart
+    // modulo 128 so that the broadcast reads of different segments use different banks.
+    constexpr int MAT = N * NP + 4;
     __shared__ __align__(16) float lu_s[kSmallWarps][S::MPW][MAT];
-    __shared__ int pbuf[kSmallWarps][32];
+    __shared__ __align__(16) int pbuf[kSmallWarps][32];
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -45,35 +46,51 @@ getri_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* 
     const bool cvalid = mvalid && r < N;
     float* sm = lu_s[warp][seg];
 
-    const float* A = mvalid ? Aarray[m] : nullptr;
     if (mvalid) {
-        for (int e = r; e < N * N; e += S::SEG) {
-            const int i = e % N, j = e / N;
-            sm[i + j * NP] = A[i + (long long)j * lda];
+        const float* A = Aarray[m];
+        if (N % 4 == 0 && (lda & 3) == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0) {
+            for (int e = r; e < N * NC; e += S::SEG) {
+                const int q = e % NC, j = e / NC;
+                cp_async16(sm + 4 * q + j * NP, A + 4 * q + (long long)j * lda);
+            }
+        } else {
+            for (int e = r; e < N * N; e += S::SEG) {
+                const int i = e % N, j = e / N;
+                cp_async4(sm + i + j * NP, A + i + (long long)j * lda);
+            }
         }
     }
     int* pv = &pbuf[warp][seg * S::SEG];
     if (r < N) pv[r] = (ipiv != nullptr && mvalid) ? ipiv[m * N + r] : r + 1;
+    cp_async_wait_all();
     __syncwarp();
 
     // Column r of P*I is the unit vector at the position row r moves to.
     const int d = cvalid ? trace_forward<N>(pv, r) : -1;
-    float x[NP];
+    float2 x2[NPAIR];
 #pragma unroll
-    for (int i = 0; i < NP; i++) x[i] = (i == d) ? 1.0f : 0.0f;
+    for (int p = 0; p < NPAIR; p++) x2[p] = make_float2(2 * p == d ? 1.0f : 0.0f, 2 * p + 1 == d ? 1.0f : 0.0f);
 
-    // Unit-L forward solve, column j of L read as float4 chunks (broadcast in the segment).
+    // Unit-L forward solve: x[i] -= L[i][j] * x[j] for i > j; L column j read as float4
+    // chunks (broadcast within the segment); fma(L, -x_j, x) == fma(-L, x_j, x) exactly.
 #pragma unroll
-    for (int j = 0; j < N; j++) {
-        const float xj = x[j];
+    for (int j = 0; j < N - 1; j++) {
+        const float xj = pget(x2, j);
+        const float2 nx = make_float2(-xj, -xj);
         const float* lj = sm + j * NP;
 #pragma unroll
-        for (int c = (j + 1) / 4; c < S::NC; c++) {
+        for (int c = j / 4; c < NC; c++) {
             const float4 l4 = *reinterpret_cast<const float4*>(lj + 4 * c);
-#pragma unroll
-            for (int t = 0; t < 4; t++) {
-                const int i = 4 * c + t;
-                if (i > j && i < N) x[i] = fmaf(-f4get(l4, t), xj, x[i]);
+            // pair 2c = rows 4c, 4c+1; pair 2c+1 = rows 4c+2, 4c+3
+            if (4 * c > j) {
+                x2[2 * c] = __ffma2_rn(make_float2(l4.x, l4.y), nx, x2[2 * c]);
+            } else if (4 * c + 1 > j) {
+                x2[2 * c].y = fmaf(l4.y, -xj, x2[2 * c].y);
+            }
+            if (4 * c + 2 > j && 4 * c + 2 < N) {
+                x2[2 * c + 1] = __ffma2_rn(make_float2(l4.z, l4.w), nx, x2[2 * c + 1]);
+            } else if (4 * c + 3 > j && 4 * c + 3 < N) {
+                x2[2 * c + 1].y = fmaf(l4.w, -xj, x2[2 * c + 1].y);
             }
         }
     }
@@ -89,33 +106,50 @@ getri_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* 
         for (int j = N - 1; j >= 0; j--) {
             if (j >= inf) {  // inf == 0: every j; inf = z+1: only j > z
                 const float* uj = sm + j * NP;
-                const float xj = x[j] / uj[j];
-                x[j] = xj;
+                const float4 dj = *reinterpret_cast<const float4*>(uj + 4 * (j / 4));
+                const float xj = pget(x2, j) / f4get(dj, j % 4);
+                pset(x2, j, xj);
+                const float2 nx = make_float2(-xj, -xj);
 #pragma unroll
-                for (int c = 0; c < (j + 3) / 4; c++) {
-                    const float4 u4 = *reinterpret_cast<const float4*>(uj + 4 * c);
-#pragma unroll
-                    for (int t = 0; t < 4; t++) {
-                        const int i = 4 * c + t;
-                        if (i < j) x[i] = fmaf(-f4get(u4, t), xj, x[i]);
+                for (int c = 0; c <= j / 4; c++) {
+                    const float4 u4 = (c == j / 4) ? dj : *reinterpret_cast<const float4*>(uj + 4 * c);
+                    if (4 * c + 1 < j) {
+                        x2[2 * c] = __ffma2_rn(make_float2(u4.x, u4.y), nx, x2[2 * c]);
+                    } else if (4 * c < j) {
+                        x2[2 * c].x = fmaf(u4.x, -xj, x2[2 * c].x);
+                    }
+                    if (4 * c + 3 < j) {
+                        x2[2 * c + 1] = __ffma2_rn(make_float2(u4.z, u4.w), nx, x2[2 * c + 1]);
+                    } else if (4 * c + 2 < j) {
+                        x2[2 * c + 1].x = fmaf(u4.z, -xj, x2[2 * c + 1].x);
                     }
                 }
             }
         }
     }
 
-    // Stage column r of C in shared memory, then store coalesced along columns.
+    // Stage column r of C (rotated chunks), then store coalesced.
     __syncwarp();
     if (cvalid) {
 #pragma unroll
-        for (int i = 0; i < N; i++) sm[i + r * SS] = x[i];
+        for (int q = 0; q < NC; q++)
+            *reinterpret_cast<float4*>(sm + r * NP + 4 * ((q + r) % NC)) =
+                make_float4(x2[2 * q].x, x2[2 * q].y, x2[2 * q + 1].x, x2[2 * q + 1].y);
     }
     __syncwarp();
     if (mvalid) {
         float* Cm = Carray[m];
-        for (int e = r; e < N * N; e += S::SEG) {
-            const int i = e % N, j = e / N;
-            Cm[i + (long long)j * ldc] = sm[i + j * SS];
+        if (N % 4 == 0 && (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(Cm) & 15) == 0) {
+            for (int e = r; e < N * NC; e += S::SEG) {
+                const int q = e % NC, j = e / NC;
+                *reinterpret_cast<float4*>(Cm + 4 * q + (long long)j * ldc) =
+                    *reinterpret_cast<const float4*>(sm + j * NP + 4 * ((q + j) % NC));
+            }
+        } else {
+            for (int e = r; e < N * N; e += S::SEG) {
+                const int i = e % N, j = e / N;
+                Cm[i + (long long)j * ldc] = sm[j * NP + 4 * ((i / 4 + j) % NC) + (i % 4)];
+            }
         }
         if (r == 0) info[m] = inf;
     }

@@ -5,130 +5,16 @@
 //   N  : row interchanges k = 0..n-1, unit-L forward solve, U backward solve with division;
 //   T/C: U^T forward solve with division, unit L^T backward solve, interchanges k = n-1..0.
 // B200 kernels:
-//   n <= 32 : getrs_small_kernel. Lane r of a warp segment holds row r (N) or column r (T) of
-//             LU in registers and row r of a chunk of RC right-hand sides; the interchanges
-//             are folded into the row the lane loads (N) or stores (T); solution entries are
-//             broadcast through a shuffle (RC == 1) or shared memory (RC == 4).
-//   n  > 32 : getrs_generic_kernel, one CTA per matrix in global memory.
+//   n <= 32, nrhs == 1 : getrs_small_kernel, rows of LU in registers, shuffle broadcasts;
+//   n <= 32, nrhs >= 2 : getrs_rhs_kernel, one lane per right-hand side, LU staged in shared
+//                        memory by cp.async;
+//   n  > 32            : getrs_generic_kernel, one CTA per matrix in global memory.
 #include <cuda_runtime.h>
 
 #include "internal.h"
-#include "small_common.cuh"
+#include "getrs_small.cuh"
 
 namespace opsblas {
-
-// Broadcast chunk x (RC floats) of lane `src` of this segment to every lane of the segment.
-template <int SEG, int RC>
-__device__ __forceinline__ void seg_bcast(const float (&x)[RC], float (&out)[RC], int seg, int r, int src,
-                                          float* slot)
-{
-    if constexpr (RC == 1) {
-        out[0] = __shfl_sync(0xffffffffu, x[0], seg * SEG + src);
-    } else {
-        if (r == src) *reinterpret_cast<float4*>(slot) = make_float4(x[0], x[1], x[2], x[3]);
-        __syncwarp();
-        const float4 v = *reinterpret_cast<const float4*>(slot);
-        out[0] = v.x;
-        out[1] = v.y;
-        out[2] = v.z;
-        out[3] = v.w;
-    }
-}
-
-template <int N, int RC, bool TRANS>
-__global__ void __launch_bounds__(kSmallWarps * 32)
-getrs_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* __restrict__ ipiv,
-                   float* const* __restrict__ Barray, int ldb, int nrhs, int batch)
-{
-    using S = SmallShape<N>;
-    static_assert(RC == 1 || RC == 4, "chunk of 1 or 4 right-hand sides");
-    __shared__ __align__(16) float xbuf[kSmallWarps][2][S::MPW][4];
-    __shared__ int pbuf[kSmallWarps][32];
-
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const int seg = lane / S::SEG;
-    const int r = lane % S::SEG;
-    const long long m = ((long long)blockIdx.x * kSmallWarps + warp) * S::MPW + seg;
-    const bool mvalid = m < batch;
-    const bool rvalid = mvalid && r < N;
-
-    const float* A = mvalid ? Aarray[m] : nullptr;
-    float* B = mvalid ? Barray[m] : nullptr;
-
-    float lu[N];
-#pragma unroll
-    for (int j = 0; j < N; j++) lu[j] = 0.0f;
-    if (rvalid) {
-#pragma unroll
-        for (int j = 0; j < N; j++) lu[j] = TRANS ? A[j + (long long)r * lda] : A[r + (long long)j * lda];
-    }
-
-    int* pv = &pbuf[warp][seg * S::SEG];
-    if (r < N) pv[r] = (ipiv != nullptr && mvalid) ? ipiv[m * N + r] : r + 1;
-    __syncwarp();
-    const int prow = rvalid ? trace_backward<N>(pv, r) : r;
-
-    for (int c0 = 0; c0 < nrhs; c0 += RC) {
-        float x[RC];
-#pragma unroll
-        for (int t = 0; t < RC; t++) {
-            const int c = c0 + t;
-            x[t] = (rvalid && c < nrhs) ? B[(TRANS ? r : prow) + (long long)c * ldb] : 0.0f;
-        }
-        int step = 0;
-        float xj[RC];
-        if (!TRANS) {
-#pragma unroll
-            for (int j = 0; j < N; j++, step++) {
-                seg_bcast<S::SEG, RC>(x, xj, seg, r, j, xbuf[warp][step & 1][seg]);
-                if (r > j) {
-#pragma unroll
-                    for (int t = 0; t < RC; t++) x[t] = fmaf(-lu[j], xj[t], x[t]);
-                }
-            }
-#pragma unroll
-            for (int j = N - 1; j >= 0; j--, step++) {
-                if (r == j) {
-#pragma unroll
-                    for (int t = 0; t < RC; t++) x[t] = x[t] / lu[j];
-                }
-                seg_bcast<S::SEG, RC>(x, xj, seg, r, j, xbuf[warp][step & 1][seg]);
-                if (r < j) {
-#pragma unroll
-                    for (int t = 0; t < RC; t++) x[t] = fmaf(-lu[j], xj[t], x[t]);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < N; j++, step++) {
-                if (r == j) {
-#pragma unroll
-                    for (int t = 0; t < RC; t++) x[t] = x[t] / lu[j];
-                }
-                seg_bcast<S::SEG, RC>(x, xj, seg, r, j, xbuf[warp][step & 1][seg]);
-                if (r > j) {
-#pragma unroll
-                    for (int t = 0; t < RC; t++) x[t] = fmaf(-lu[j], xj[t], x[t]);
-                }
-            }
-#pragma unroll
-            for (int i = N - 1; i >= 0; i--, step++) {
-                seg_bcast<S::SEG, RC>(x, xj, seg, r, i, xbuf[warp][step & 1][seg]);
-                if (r < i) {
-#pragma unroll
-                    for (int t = 0; t < RC; t++) x[t] = fmaf(-lu[i], xj[t], x[t]);
-                }
-            }
-        }
-#pragma unroll
-        for (int t = 0; t < RC; t++) {
-            const int c = c0 + t;
-            if (rvalid && c < nrhs) B[(TRANS ? prow : r) + (long long)c * ldb] = x[t];
-        }
-        __syncwarp();
-    }
-}
 
 // n > 32: one CTA per matrix, global memory. The row interchanges and the L^T sweep run one
 // thread per right-hand side (the reference's order); the other sweeps run in parallel over
@@ -299,33 +185,10 @@ extern "C" aclblasStatus_t aclblasSgetrsBatched(
     cudaStream_t st = handle->stream;
     const bool tr = trans != ACLBLAS_OP_N;
     if (n <= 32) {
-        switch (n) {
-#define OPSBLAS_GETRS_LAUNCH(NN, RCV, TRV)                                                                          \
-    getrs_small_kernel<NN, RCV, TRV><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, devIpiv, Barray, ldb, nrhs,    \
-                                                                        batchCount)
-#define OPSBLAS_GETRS_CASE(NN)                                                                                      \
-    case NN: {                                                                                                      \
-        constexpr int per_cta = kSmallWarps * SmallShape<NN>::MPW;                                                  \
-        const unsigned grid = (unsigned)((batchCount + per_cta - 1) / per_cta);                                     \
-        if (nrhs == 1) {                                                                                            \
-            if (tr)                                                                                                 \
-                OPSBLAS_GETRS_LAUNCH(NN, 1, true);                                                                  \
-            else                                                                                                    \
-                OPSBLAS_GETRS_LAUNCH(NN, 1, false);                                                                 \
-        } else {                                                                                                    \
-            if (tr)                                                                                                 \
-                OPSBLAS_GETRS_LAUNCH(NN, 4, true);                                                                  \
-            else                                                                                                    \
-                OPSBLAS_GETRS_LAUNCH(NN, 4, false);                                                                 \
-        }                                                                                                           \
-        break;                                                                                                      \
-    }
-            OPSBLAS_FOR_N_1_32(OPSBLAS_GETRS_CASE)
-#undef OPSBLAS_GETRS_CASE
-#undef OPSBLAS_GETRS_LAUNCH
-            default:
-                break;
-        }
+        if (tr)
+            getrs_small_dispatch_t(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
+        else
+            getrs_small_dispatch_n(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
     } else {
         getrs_generic_kernel<<<(unsigned)batchCount, kGenericThreads, 0, st>>>(Aarray, n, lda, devIpiv, Barray, ldb,
                                                                                nrhs, tr ? 1 : 0);

@@ -25,6 +25,39 @@ __device__ __forceinline__ float f4get(const float4& v, int i)
     return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w));
 }
 
+// Element j of a row held as float2 pairs (j compile-time after unrolling).
+template <int NPAIR>
+__device__ __forceinline__ float pget(const float2 (&v)[NPAIR], int j)
+{
+    return (j & 1) ? v[j >> 1].y : v[j >> 1].x;
+}
+
+template <int NPAIR>
+__device__ __forceinline__ void pset(float2 (&v)[NPAIR], int j, float x)
+{
+    if (j & 1)
+        v[j >> 1].y = x;
+    else
+        v[j >> 1].x = x;
+}
+
+// Asynchronous global -> shared copies (cp.async, sm_80+): no registers held while in flight.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
+}
+
+// Waits for this thread's outstanding cp.async copies; a __syncwarp()/__syncthreads() must
+// follow before other threads read the data.
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Per-segment max of `key` over the lanes of each segment, then the minimum `cand` among the
 // lanes whose key equals that max. Full-warp redux.sync per segment, other lanes contribute
 // the identity, so the result never mixes segments. Must be called by all 32 lanes.
@@ -53,33 +86,40 @@ __device__ __forceinline__ unsigned seg_argmax(unsigned key, unsigned cand, int 
     }
 }
 
-// Position that row `r` takes after the row interchanges k = 0..n-1 of a pivot vector
-// (LAPACK laswp forward order) -- equivalently the source row of position r after the
-// interchanges applied in reverse order. `pv` holds the 1-based pivots in shared memory;
-// out-of-range and self pivots are skipped as in the reference (sgetrs_batched_kernel.cpp:94-100).
-template <int N>
-__device__ __forceinline__ int trace_forward(const int* pv, int r)
+// Applies the row interchanges of a pivot vector to a row index. `pv` holds the 1-based
+// pivots in shared memory (16-byte aligned); out-of-range and self pivots are skipped as in the
+// reference (sgetrs_batched_kernel.cpp:94-100). FORWARD = true applies k = 0..n-1 in order
+// (the row that row r moves to under LAPACK laswp); FORWARD = false applies k = n-1..0 (the
+// source row of position r after laswp, equivalently where row r goes under the reverse
+// interchanges).
+template <int N, bool FORWARD>
+__device__ __forceinline__ int trace_pivots(const int* pv, int r)
 {
+    constexpr int NC = (N + 3) / 4;
+    int4 q[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) q[c] = reinterpret_cast<const int4*>(pv)[c];
     int pos = r;
 #pragma unroll
-    for (int k = 0; k < N; k++) {
-        const int p = pv[k] - 1;
-        if (p >= 0 && p < N && p != k) pos = (pos == k) ? p : (pos == p ? k : pos);
+    for (int t = 0; t < N; t++) {
+        const int k = FORWARD ? t : N - 1 - t;
+        const int4& qc = q[k / 4];
+        const int p = ((k % 4) == 0 ? qc.x : (k % 4) == 1 ? qc.y : (k % 4) == 2 ? qc.z : qc.w) - 1;
+        if ((unsigned)p < (unsigned)N && p != k) pos = (pos == k) ? p : (pos == p ? k : pos);
     }
     return pos;
 }
 
-// Same interchanges traced in reverse order (k = n-1..0).
+template <int N>
+__device__ __forceinline__ int trace_forward(const int* pv, int r)
+{
+    return trace_pivots<N, true>(pv, r);
+}
+
 template <int N>
 __device__ __forceinline__ int trace_backward(const int* pv, int r)
 {
-    int pos = r;
-#pragma unroll
-    for (int k = N - 1; k >= 0; k--) {
-        const int p = pv[k] - 1;
-        if (p >= 0 && p < N && p != k) pos = (pos == k) ? p : (pos == p ? k : pos);
-    }
-    return pos;
+    return trace_pivots<N, false>(pv, r);
 }
 
 }  // namespace opsblas

@@ -4,7 +4,8 @@ Two references:
   * the CPU oracle (oracle/lu_oracle.c, the reference kernels restated with one fmaf per
     update and true division): the CUDA kernels follow the same operation order, so factors,
     pivots, info, solutions and inverses must agree BIT FOR BIT -- except the transposed solve
-    of the n <= 32 kernel, whose L^T sweep accumulates in a different order (tolerance below);
+    with a single right-hand side at n <= 32, whose L^T sweep accumulates in a different
+    order (tolerance below);
   * the reference's own golden outputs (tests/golden/*.npz, LAPACK through the reference's
     golden headers): info exact, pivots exact when untied, factors under the reference's
     MIXED_TOLERANCE rule and 1e-5 normwise, solutions within the conditioning bound.
@@ -119,7 +120,7 @@ def test_getrs_csv(handle, c):
     assert hinfo == 0
     ox = b.copy()
     O.port_getrs(c.trans, a, c.n, c.lda, piv if c.pivot else None, ox, c.nrhs, c.ldb)
-    if c.trans == "N" or c.n > 32:
+    if c.trans == "N" or c.n > 32 or c.nrhs > 1:
         assert_bitwise(x, ox, "X")
     else:
         for k in range(c.batch):
@@ -210,7 +211,7 @@ def test_noop_calls_touch_nothing(handle, ob):
 def test_getrs_nrhs_chunks_and_ldb(handle):
     """nrhs that is not a multiple of the 4-column chunk, ldb > n, both transposes."""
     rng = np.random.default_rng(3)
-    for n, nrhs in [(7, 3), (16, 5), (32, 9), (32, 256), (33, 6)]:
+    for n, nrhs in [(7, 3), (16, 5), (32, 9), (32, 256), (33, 6), (12, 1), (31, 2), (30, 4)]:
         a = rng.standard_normal((11, n, n)).astype(np.float32)
         piv, _, _ = O.port_getrf(a, n, n)
         b = rng.standard_normal((11, nrhs, n + 2)).astype(np.float32)
@@ -218,7 +219,7 @@ def test_getrs_nrhs_chunks_and_ldb(handle):
             x, _ = gpu_getrs(handle, trans, a, n, n, piv, b, nrhs, n + 2)
             ox = b.copy()
             O.port_getrs(trans, a, n, n, piv, ox, nrhs, n + 2)
-            if trans == "N" or n > 32:
+            if trans == "N" or n > 32 or nrhs > 1:
                 assert_bitwise(x, ox, f"X n={n} nrhs={nrhs} {trans}")
             else:
                 np.testing.assert_allclose(x, ox, rtol=2e-4, atol=1e-5)
@@ -321,3 +322,42 @@ def test_handle_stream_and_workspace(ob, cuda):
     assert L.aclblasSetWorkspace(h, C.c_void_p(ws.data_ptr()), 16) == ob.SUCCESS  # grow-only: ignored
     assert L.aclblasSetStream(h, None) == ob.SUCCESS  # back to the library workspace
     assert L.aclblasDestroy(h) == ob.SUCCESS
+
+
+def test_unaligned_matrices_take_the_scalar_paths(handle, ob):
+    """Matrices whose addresses are 4- but not 16-byte aligned (and lda not a multiple of 4)
+    use the element-wise staging paths; results must not change."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    for n, lda, nrhs in [(32, 32, 4), (16, 17, 3), (8, 8, 2)]:
+        batch = 19
+        a = rng.standard_normal((batch, n, lda)).astype(np.float32)
+        piv, _, _ = O.port_getrf(a, n, lda)
+        b = rng.standard_normal((batch, nrhs, n)).astype(np.float32)
+        # one extra float in front of every matrix: element stride lda*n + 1
+        flat = np.zeros((batch, n * lda + 1), np.float32)
+        flat[:, 1:] = a.reshape(batch, -1)
+        fb = np.zeros((batch, nrhs * n + 1), np.float32)
+        fb[:, 1:] = b.reshape(batch, -1)
+        A = to_dev(flat, "cuda")
+        Bd = to_dev(fb, "cuda")
+        P = to_dev(piv, "cuda")
+        aptr = ob.ptr_array(A) + 4
+        bptr = ob.ptr_array(Bd) + 4
+        for trans in ("N", "T"):
+            Bd.copy_(to_dev(fb, "cuda"))
+            handle.getrs(trans, A, n, lda, P, Bd, nrhs, n, aptr=aptr, bptr=bptr)
+            torch.cuda.synchronize()
+            x = to_host(Bd)[:, 1:].reshape(batch, nrhs, n)
+            ox = b.copy()
+            O.port_getrs(trans, a, n, lda, piv, ox, nrhs, n)
+            assert_bitwise(x, ox, f"getrs {trans} n={n}")
+        Cm = torch.zeros((batch, n * n + 1), dtype=torch.float32, device="cuda")
+        cptr = ob.ptr_array(Cm) + 4
+        info = handle.getri(A, n, lda, P, Cm, n, aptr=aptr, cptr=cptr)
+        torch.cuda.synchronize()
+        oc = np.zeros((batch, n, n), np.float32)
+        oinfo = O.port_getri(a, n, lda, piv, oc, n)
+        assert_bitwise(to_host(Cm)[:, 1:].reshape(batch, n, n), oc, f"getri n={n}")
+        np.testing.assert_array_equal(to_host(info), oinfo)
