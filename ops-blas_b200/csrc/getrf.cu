@@ -27,13 +27,46 @@ namespace opsblas {
 //   3. lanes below the pivot form l = a[k] / pivot and update a[j] -= l * u[j], j > k.
 // Arithmetic per element is the reference's, in its order, one fmaf per update.
 // ---------------------------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ float qget(const float4 (&v)[(N + 3) / 4], int j)
+{
+    return f4get(v[j >> 2], j & 3);
+}
+
+template <int N>
+__device__ __forceinline__ void qset(float4 (&v)[(N + 3) / 4], int j, float x)
+{
+    float4& c = v[j >> 2];
+    if ((j & 3) == 0) c.x = x;
+    else if ((j & 3) == 1) c.y = x;
+    else if ((j & 3) == 2) c.z = x;
+    else c.w = x;
+}
+
+// a[j] -= l * u[j] on the pairs (x, y) / (z, w) of a float4 chunk, one packed fma per pair;
+// fma(u, -l, a) == fma(-l, u, a) exactly.
+__device__ __forceinline__ void ffma2_lo(float4& a, float ux, float uy, float2 nl)
+{
+    const float2 r = __ffma2_rn(make_float2(ux, uy), nl, make_float2(a.x, a.y));
+    a.x = r.x;
+    a.y = r.y;
+}
+
+__device__ __forceinline__ void ffma2_hi(float4& a, float uz, float uw, float2 nl)
+{
+    const float2 r = __ffma2_rn(make_float2(uz, uw), nl, make_float2(a.z, a.w));
+    a.z = r.x;
+    a.w = r.y;
+}
+
 template <int N, bool PIVOT>
 __global__ void __launch_bounds__(kSmallWarps * 32, N > 16 ? 4 : (N > 8 ? 5 : 6))
 getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__ piv, int* __restrict__ info,
                    int batch)
 {
     using S = SmallShape<N>;
-    constexpr int NPAIR = S::NP / 2;
+    constexpr int NC = S::NC;
+    constexpr bool UNIFORM = S::MPW == 1;  // one matrix per warp: segment state is warp-uniform
     __shared__ __align__(16) float rowbuf[kSmallWarps][2][32];
 
     const int lane = threadIdx.x & 31;
@@ -44,15 +77,16 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
     const bool mvalid = m < batch;
     const bool rvalid = mvalid && r < N;
 
-    // Row r in registers as pairs a2[p] = (a[2p], a[2p+1]); padding entries stay zero.
+    // Row r in registers as float4 chunks (contiguous quads: published with one 16-byte store,
+    // updated two columns per packed fma); padding entries stay zero.
     float* A = mvalid ? Aarray[m] : nullptr;
-    float2 a2[NPAIR];
+    float4 a4[NC];
 #pragma unroll
-    for (int p = 0; p < NPAIR; p++) a2[p] = make_float2(0.0f, 0.0f);
+    for (int c = 0; c < NC; c++) a4[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (rvalid) {
         const float* Ar = A + r;
 #pragma unroll
-        for (int j = 0; j < N; j++) pset(a2, j, Ar[(long long)j * lda]);
+        for (int j = 0; j < N; j++) qset<N>(a4, j, Ar[(long long)j * lda]);
     }
 
     int pos = r;
@@ -61,8 +95,8 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
 #pragma unroll
     for (int k = 0; k < N; k++) {
         float* buf = &rowbuf[warp][k & 1][seg * S::SEG];
-        const bool live = rvalid && inf == 0;
-        const float ak = pget(a2, k);
+        const bool live = UNIFORM ? rvalid : (rvalid && inf == 0);
+        const float ak = qget<N>(a4, k);
         int prow = k;
         bool ispiv;
         if (PIVOT) {
@@ -76,35 +110,45 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
         }
         if (ispiv) {
 #pragma unroll
-            for (int c = k / 4; c < S::NC; c++)
-                reinterpret_cast<float4*>(buf)[c] = make_float4(a2[2 * c].x, a2[2 * c].y, a2[2 * c + 1].x,
-                                                                a2[2 * c + 1].y);
+            for (int c = k / 4; c < NC; c++) reinterpret_cast<float4*>(buf)[c] = a4[c];
         }
         __syncwarp();
         const float4 ck = reinterpret_cast<const float4*>(buf)[k / 4];
         const float pv = f4get(ck, k % 4);
-        if (mvalid && inf == 0) {
+        if (UNIFORM) {
+            if (PIVOT && r == k) mypiv = prow + 1;
+            if (pv == 0.0f) {  // warp-uniform: every lane read the same pivot
+                inf = k + 1;
+                break;
+            }
+        } else if (mvalid && inf == 0) {
             if (PIVOT && r == k) mypiv = prow + 1;
             if (pv == 0.0f) inf = k + 1;
         }
-        if (live && inf == 0) {
+        if (UNIFORM ? live : (live && inf == 0)) {
             if (ispiv)
                 pos = k;
             else if (pos == k)
                 pos = prow;
             if (pos > k) {
-                // Multiplier by true division, then a[j] -= l * u[j] for j > k as one fma each;
-                // fma(u, -l, a) == fma(-l, u, a) exactly, two columns per packed instruction.
+                // Multiplier by true division, then a[j] -= l * u[j] for j > k, one fma each.
                 const float l = ak / pv;
-                pset(a2, k, l);
+                qset<N>(a4, k, l);
                 const float2 nl = make_float2(-l, -l);
-                if ((k & 1) == 0 && k + 1 < N) a2[k >> 1].y = fmaf(-l, f4get(ck, (k + 1) % 4), a2[k >> 1].y);
 #pragma unroll
-                for (int c = k / 4; c < S::NC; c++) {
+                for (int c = k / 4; c < NC; c++) {
                     const float4 u = (c == k / 4) ? ck : reinterpret_cast<const float4*>(buf)[c];
-                    if (2 * c >= (k + 2) / 2 && 4 * c < N) a2[2 * c] = __ffma2_rn(make_float2(u.x, u.y), nl, a2[2 * c]);
-                    if (2 * c + 1 >= (k + 2) / 2 && 4 * c + 2 < N)
-                        a2[2 * c + 1] = __ffma2_rn(make_float2(u.z, u.w), nl, a2[2 * c + 1]);
+                    // columns 4c..4c+3 that lie right of k
+                    if (4 * c > k) {
+                        ffma2_lo(a4[c], u.x, u.y, nl);
+                    } else if (4 * c + 1 > k) {
+                        a4[c].y = fmaf(-l, u.y, a4[c].y);
+                    }
+                    if (4 * c + 2 > k && 4 * c + 2 < N) {
+                        ffma2_hi(a4[c], u.z, u.w, nl);
+                    } else if (4 * c + 3 > k && 4 * c + 3 < N) {
+                        a4[c].w = fmaf(-l, u.w, a4[c].w);
+                    }
                 }
             }
         }
@@ -113,7 +157,7 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
     if (rvalid) {
         float* Ap = A + pos;
 #pragma unroll
-        for (int j = 0; j < N; j++) Ap[(long long)j * lda] = pget(a2, j);
+        for (int j = 0; j < N; j++) Ap[(long long)j * lda] = qget<N>(a4, j);
         if (PIVOT) piv[m * N + r] = mypiv;
         if (r == 0 && info != nullptr) info[m] = inf;
     }

@@ -95,34 +95,47 @@ getri_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* 
         }
     }
 
-    // Highest zero diagonal (the backward sweep stops there).
+    // U backward sweep j = n-1..0; it stops at the first zero U(j,j) it meets, so info is the
+    // highest zero diagonal + 1. For n <= 8 the reference keeps the forward result in C on a
+    // stop, so the diagonal is scanned first; for n > 8 the sweep detects the zero itself.
     int inf = 0;
+    if (N <= 8) {
 #pragma unroll
-    for (int j = N - 1; j >= 0; j--)
-        if (inf == 0 && sm[j + j * NP] == 0.0f) inf = j + 1;
-
-    if (!(inf != 0 && N <= 8)) {
+        for (int j = N - 1; j >= 0; j--)
+            if (inf == 0 && sm[j + j * NP] == 0.0f) inf = j + 1;
+    }
+    if (!(N <= 8 && inf != 0)) {
 #pragma unroll
         for (int j = N - 1; j >= 0; j--) {
-            if (j >= inf) {  // inf == 0: every j; inf = z+1: only j > z
-                const float* uj = sm + j * NP;
-                const float4 dj = *reinterpret_cast<const float4*>(uj + 4 * (j / 4));
-                const float xj = pget(x2, j) / f4get(dj, j % 4);
-                pset(x2, j, xj);
-                const float2 nx = make_float2(-xj, -xj);
+            const float* uj = sm + j * NP;
+            const float4 dj = *reinterpret_cast<const float4*>(uj + 4 * (j / 4));
+            const float ujj = f4get(dj, j % 4);
+            if (N > 8) {
+                if (S::MPW == 1) {
+                    if (ujj == 0.0f) {  // warp-uniform
+                        inf = j + 1;
+                        break;
+                    }
+                } else {
+                    if (inf == 0 && ujj == 0.0f) inf = j + 1;
+                    if (inf != 0) continue;
+                }
+            }
+            const float xj = pget(x2, j) / ujj;
+            pset(x2, j, xj);
+            const float2 nx = make_float2(-xj, -xj);
 #pragma unroll
-                for (int c = 0; c <= j / 4; c++) {
-                    const float4 u4 = (c == j / 4) ? dj : *reinterpret_cast<const float4*>(uj + 4 * c);
-                    if (4 * c + 1 < j) {
-                        x2[2 * c] = __ffma2_rn(make_float2(u4.x, u4.y), nx, x2[2 * c]);
-                    } else if (4 * c < j) {
-                        x2[2 * c].x = fmaf(u4.x, -xj, x2[2 * c].x);
-                    }
-                    if (4 * c + 3 < j) {
-                        x2[2 * c + 1] = __ffma2_rn(make_float2(u4.z, u4.w), nx, x2[2 * c + 1]);
-                    } else if (4 * c + 2 < j) {
-                        x2[2 * c + 1].x = fmaf(u4.z, -xj, x2[2 * c + 1].x);
-                    }
+            for (int c = 0; c <= j / 4; c++) {
+                const float4 u4 = (c == j / 4) ? dj : *reinterpret_cast<const float4*>(uj + 4 * c);
+                if (4 * c + 1 < j) {
+                    x2[2 * c] = __ffma2_rn(make_float2(u4.x, u4.y), nx, x2[2 * c]);
+                } else if (4 * c < j) {
+                    x2[2 * c].x = fmaf(u4.x, -xj, x2[2 * c].x);
+                }
+                if (4 * c + 3 < j) {
+                    x2[2 * c + 1] = __ffma2_rn(make_float2(u4.z, u4.w), nx, x2[2 * c + 1]);
+                } else if (4 * c + 2 < j) {
+                    x2[2 * c + 1].x = fmaf(u4.z, -xj, x2[2 * c + 1].x);
                 }
             }
         }

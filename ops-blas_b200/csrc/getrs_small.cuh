@@ -93,8 +93,9 @@ struct RhsShape {
     static constexpr int MPW = 32 / LPM;
     static constexpr int MAT = N * NP + 4;       // floats of one staged matrix (16-byte stagger)
     static constexpr int SLOT = MAT + 64;        // + pivots and row map (32 ints each)
-    static constexpr int WARP_WORDS = MPW * SLOT;
-    static constexpr int W0 = 24576 / WARP_WORDS;  // about 96 KiB per CTA
+    static constexpr int BCOL = NP;              // staged right-hand-side column per lane
+    static constexpr int WARP_WORDS = MPW * SLOT + 32 * BCOL;
+    static constexpr int W0 = 9216 / WARP_WORDS;  // about 36 KiB per CTA: several CTAs per SM
     static constexpr int WARPS = W0 < 1 ? 1 : (W0 > 8 ? 8 : W0);
     static constexpr size_t SMEM = (size_t)WARPS * WARP_WORDS * 4;
 };
@@ -114,12 +115,29 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
     const int q = lane % LPM;
     const long long m = ((long long)blockIdx.x * R::WARPS + warp) * R::MPW + seg;
     const bool mvalid = m < batch;
-    float* sm = dsm + (warp * R::MPW + seg) * R::SLOT;
+    float* wbase = dsm + warp * R::WARP_WORDS;
+    float* sm = wbase + seg * R::SLOT;
     int* pv = reinterpret_cast<int*>(sm + R::MAT);
     int* map = pv + 32;
+    float* bs = wbase + R::MPW * R::SLOT + lane * R::BCOL;  // this lane's right-hand side
 
+    const float* A = mvalid ? Aarray[m] : nullptr;
+    float* B = mvalid ? Barray[m] : nullptr;
+    const bool bvec = N % 4 == 0 && (ldb & 3) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0;
+
+    // Issue every global read of the first right-hand side up front: LU and B by cp.async,
+    // the pivots as plain loads; the row map is built while the copies are in flight.
+    auto stage_rhs = [&](int c) {
+        const float* Bc = B + (long long)c * ldb;
+        if (bvec) {
+#pragma unroll
+            for (int t = 0; t < NC; t++) cp_async16(bs + 4 * t, Bc + 4 * t);
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; i++) cp_async4(bs + i, Bc + i);
+        }
+    };
     if (mvalid) {
-        const float* A = Aarray[m];
         if (N % 4 == 0 && (lda & 3) == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0) {
             for (int e = q; e < N * NC; e += LPM) {
                 const int c = e % NC, j = e / NC;
@@ -131,12 +149,12 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
                 cp_async4(sm + i + j * NP, A + i + (long long)j * lda);
             }
         }
+        if (q < nrhs) stage_rhs(q);
         for (int k = q; k < N; k += LPM) {
             pv[k] = ipiv != nullptr ? ipiv[m * N + k] : k + 1;
             map[k] = k;
         }
     }
-    cp_async_wait_all();
     __syncwarp();
     if (mvalid && q == 0 && ipiv != nullptr) {
         // The interchanges k = 0..n-1 applied to the identity row map.
@@ -149,13 +167,16 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
             }
         }
     }
+    cp_async_wait_all();
     __syncwarp();
     if (!mvalid) return;
 
-    float* B = Barray[m];
-    const bool bvec = N % 4 == 0 && (ldb & 3) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0;
     for (int c = q; c < nrhs; c += LPM) {
         float* Bc = B + (long long)c * ldb;
+        if (c != q) {  // later right-hand sides of this lane (nrhs > LPM)
+            stage_rhs(c);
+            cp_async_wait_all();
+        }
         float2 x2[NPAIR];
 #pragma unroll
         for (int p = 0; p < NPAIR; p++) x2[p] = make_float2(0.0f, 0.0f);
@@ -163,10 +184,10 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
 #pragma unroll
             for (int t = 0; t < NC; t++) {
                 const int4 mp = reinterpret_cast<const int4*>(map)[t];
-                if (4 * t + 0 < N) x2[2 * t].x = Bc[mp.x];
-                if (4 * t + 1 < N) x2[2 * t].y = Bc[mp.y];
-                if (4 * t + 2 < N) x2[2 * t + 1].x = Bc[mp.z];
-                if (4 * t + 3 < N) x2[2 * t + 1].y = Bc[mp.w];
+                if (4 * t + 0 < N) x2[2 * t].x = bs[mp.x];
+                if (4 * t + 1 < N) x2[2 * t].y = bs[mp.y];
+                if (4 * t + 2 < N) x2[2 * t + 1].x = bs[mp.z];
+                if (4 * t + 3 < N) x2[2 * t + 1].y = bs[mp.w];
             }
             // unit-L forward: x[i] -= L[i][j] * x[j], i > j
 #pragma unroll
@@ -218,16 +239,11 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
                 for (int i = 0; i < N; i++) Bc[i] = pget(x2, i);
             }
         } else {
-            if (bvec) {
 #pragma unroll
-                for (int t = 0; t < NC; t++) {
-                    const float4 v = *reinterpret_cast<const float4*>(Bc + 4 * t);
-                    x2[2 * t] = make_float2(v.x, v.y);
-                    x2[2 * t + 1] = make_float2(v.z, v.w);
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < N; i++) pset(x2, i, Bc[i]);
+            for (int t = 0; t < NC; t++) {
+                const float4 v = *reinterpret_cast<const float4*>(bs + 4 * t);
+                x2[2 * t] = make_float2(v.x, v.y);
+                x2[2 * t + 1] = make_float2(v.z, v.w);
             }
             // U^T forward: x[i] = (x[i] - sum_{j<i} U[j][i] x[j]) / U[i][i], j ascending
 #pragma unroll
