@@ -54,6 +54,14 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem));
 }
 
+// Closes the current group of cp.async copies / waits until at most N groups are pending.
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Waits for this thread's outstanding cp.async copies; a __syncwarp()/__syncthreads() must
 // follow before other threads read the data.
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
