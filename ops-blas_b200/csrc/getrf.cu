@@ -43,31 +43,24 @@ __device__ __forceinline__ void qset(float4 (&v)[(N + 3) / 4], int j, float x)
     else c.w = x;
 }
 
-// Predicated updates a[j] = fma(u[j], m, a[j]) with m = -l (== fma(-l, u[j], a[j]) exactly):
-// rows that must not change are masked by the predicate instead of a divergent branch, so a
-// column step is one straight-line instruction stream for the whole warp.
-__device__ __forceinline__ void pfma2(float& a0, float& a1, float u0, float u1, float m, unsigned p)
+// a[j] -= l * u[j] on the pairs (x, y) / (z, w) of a float4 chunk, one packed fma per pair;
+// fma(u, -l, a) == fma(-l, u, a) exactly.
+__device__ __forceinline__ void ffma2_lo(float4& a, float ux, float uy, float2 nl)
 {
-    asm("{\n\t.reg .pred q;\n\t.reg .b64 ra, rb, rc;\n\t"
-        "setp.ne.u32 q, %4, 0;\n\t"
-        "mov.b64 ra, {%2, %3};\n\t"
-        "mov.b64 rb, {%5, %5};\n\t"
-        "mov.b64 rc, {%0, %1};\n\t"
-        "@q fma.rn.f32x2 rc, ra, rb, rc;\n\t"
-        "mov.b64 {%0, %1}, rc;\n\t}"
-        : "+f"(a0), "+f"(a1)
-        : "f"(u0), "f"(u1), "r"(p), "f"(m));
+    const float2 r = __ffma2_rn(make_float2(ux, uy), nl, make_float2(a.x, a.y));
+    a.x = r.x;
+    a.y = r.y;
 }
 
-__device__ __forceinline__ void pfma1(float& a, float u, float m, unsigned p)
+__device__ __forceinline__ void ffma2_hi(float4& a, float uz, float uw, float2 nl)
 {
-    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q fma.rn.f32 %0, %1, %3, %0;\n\t}"
-        : "+f"(a)
-        : "f"(u), "r"(p), "f"(m));
+    const float2 r = __ffma2_rn(make_float2(uz, uw), nl, make_float2(a.z, a.w));
+    a.z = r.x;
+    a.w = r.y;
 }
 
 template <int N, bool PIVOT>
-__global__ void __launch_bounds__(kSmallWarps * 32, N > 8 ? 4 : 6)
+__global__ void __launch_bounds__(kSmallWarps * 32, N > 16 ? 4 : (N > 8 ? 5 : 6))
 getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__ piv, int* __restrict__ info,
                    int batch)
 {
@@ -132,26 +125,32 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
             if (PIVOT && r == k) mypiv = prow + 1;
             if (pv == 0.0f) inf = k + 1;
         }
-        const bool act = UNIFORM ? live : (live && inf == 0);
-        if (act) pos = ispiv ? k : (pos == k ? prow : pos);
-        // Multiplier by true division (every lane computes it; only rows below the pivot keep
-        // it), then a[j] -= l * u[j] for j > k, one fma each, masked for the other rows.
-        const unsigned upd = (act && pos > k) ? 1u : 0u;
-        const float l = ak / pv;
-        if (upd) qset<N>(a4, k, l);
-        const float nl = -l;
+        if (UNIFORM ? live : (live && inf == 0)) {
+            if (ispiv)
+                pos = k;
+            else if (pos == k)
+                pos = prow;
+            if (pos > k) {
+                // Multiplier by true division, then a[j] -= l * u[j] for j > k, one fma each.
+                const float l = ak / pv;
+                qset<N>(a4, k, l);
+                const float2 nl = make_float2(-l, -l);
 #pragma unroll
-        for (int c = k / 4; c < NC; c++) {
-            const float4 u = (c == k / 4) ? ck : reinterpret_cast<const float4*>(buf)[c];
-            // columns 4c..4c+3 that lie right of k
-            if (4 * c > k)
-                pfma2(a4[c].x, a4[c].y, u.x, u.y, nl, upd);
-            else if (4 * c + 1 > k)
-                pfma1(a4[c].y, u.y, nl, upd);
-            if (4 * c + 2 > k && 4 * c + 2 < N)
-                pfma2(a4[c].z, a4[c].w, u.z, u.w, nl, upd);
-            else if (4 * c + 3 > k && 4 * c + 3 < N)
-                pfma1(a4[c].w, u.w, nl, upd);
+                for (int c = k / 4; c < NC; c++) {
+                    const float4 u = (c == k / 4) ? ck : reinterpret_cast<const float4*>(buf)[c];
+                    // columns 4c..4c+3 that lie right of k
+                    if (4 * c > k) {
+                        ffma2_lo(a4[c], u.x, u.y, nl);
+                    } else if (4 * c + 1 > k) {
+                        a4[c].y = fmaf(-l, u.y, a4[c].y);
+                    }
+                    if (4 * c + 2 > k && 4 * c + 2 < N) {
+                        ffma2_hi(a4[c], u.z, u.w, nl);
+                    } else if (4 * c + 3 > k && 4 * c + 3 < N) {
+                        a4[c].w = fmaf(-l, u.w, a4[c].w);
+                    }
+                }
+            }
         }
     }
 

@@ -3,7 +3,6 @@
 
 #include <cuda_runtime.h>
 
-#include "internal.h"
 #include "small_common.cuh"
 
 namespace opsblas {
@@ -95,16 +94,12 @@ struct RhsShape {
     static constexpr int MAT = N * NP + 4;       // floats of one staged matrix (16-byte stagger)
     static constexpr int SLOT = MAT + 64;        // + pivots and row map (32 ints each)
     static constexpr int BCOL = NP;              // staged right-hand-side column per lane
-    static constexpr int BUF_WORDS = MPW * SLOT + 32 * BCOL;
-    static constexpr int WARP_WORDS = 2 * BUF_WORDS;  // double buffered
-    static constexpr int W0 = 18432 / WARP_WORDS;     // about 72 KiB per CTA
+    static constexpr int WARP_WORDS = MPW * SLOT + 32 * BCOL;
+    static constexpr int W0 = 9216 / WARP_WORDS;  // about 36 KiB per CTA: several CTAs per SM
     static constexpr int WARPS = W0 < 1 ? 1 : (W0 > 8 ? 8 : W0);
     static constexpr size_t SMEM = (size_t)WARPS * WARP_WORDS * 4;
 };
 
-// Persistent: warp w of CTA b handles matrix groups g = b*WARPS + w, + gridDim.x*WARPS, ...
-// While group g is solved from one buffer, the next group's LU, pivots and first right-hand
-// sides are in flight into the other (cp.async groups), so HBM stays busy during the solves.
 template <int N, int LPM, bool TRANS>
 __global__ void __launch_bounds__(RhsShape<N, LPM>::WARPS * 32)
 getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __restrict__ ipiv,
@@ -118,19 +113,31 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
     const int warp = threadIdx.x >> 5;
     const int seg = lane / LPM;
     const int q = lane % LPM;
-    const long long ngroups = (batch + R::MPW - 1) / R::MPW;
-    const long long gstride = (long long)gridDim.x * R::WARPS;
+    const long long m = ((long long)blockIdx.x * R::WARPS + warp) * R::MPW + seg;
+    const bool mvalid = m < batch;
     float* wbase = dsm + warp * R::WARP_WORDS;
+    float* sm = wbase + seg * R::SLOT;
+    int* pv = reinterpret_cast<int*>(sm + R::MAT);
+    int* map = pv + 32;
+    float* bs = wbase + R::MPW * R::SLOT + lane * R::BCOL;  // this lane's right-hand side
 
-    // Issue the copies of group g into buffer `buf`: LU, pivots, and this lane's first
-    // right-hand side.
-    auto stage = [&](long long g, int buf) {
-        const long long m = g * R::MPW + seg;
-        if (m >= batch) return;
-        float* sm = wbase + buf * R::BUF_WORDS + seg * R::SLOT;
-        int* pv = reinterpret_cast<int*>(sm + R::MAT);
-        float* bs = wbase + buf * R::BUF_WORDS + R::MPW * R::SLOT + lane * R::BCOL;
-        const float* A = Aarray[m];
+    const float* A = mvalid ? Aarray[m] : nullptr;
+    float* B = mvalid ? Barray[m] : nullptr;
+    const bool bvec = N % 4 == 0 && (ldb & 3) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0;
+
+    // Issue every global read of the first right-hand side up front: LU and B by cp.async,
+    // the pivots as plain loads; the row map is built while the copies are in flight.
+    auto stage_rhs = [&](int c) {
+        const float* Bc = B + (long long)c * ldb;
+        if (bvec) {
+#pragma unroll
+            for (int t = 0; t < NC; t++) cp_async16(bs + 4 * t, Bc + 4 * t);
+        } else {
+#pragma unroll
+            for (int i = 0; i < N; i++) cp_async4(bs + i, Bc + i);
+        }
+    };
+    if (mvalid) {
         if (N % 4 == 0 && (lda & 3) == 0 && (reinterpret_cast<uintptr_t>(A) & 15) == 0) {
             for (int e = q; e < N * NC; e += LPM) {
                 const int c = e % NC, j = e / NC;
@@ -142,175 +149,141 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
                 cp_async4(sm + i + j * NP, A + i + (long long)j * lda);
             }
         }
-        if (ipiv != nullptr)
-            for (int k = q; k < N; k += LPM) cp_async4(pv + k, ipiv + m * N + k);
-        if (q < nrhs) {
-            const float* Bc = Barray[m] + (long long)q * ldb;
-            if (N % 4 == 0 && (ldb & 3) == 0 && (reinterpret_cast<uintptr_t>(Bc) & 15) == 0) {
-#pragma unroll
-                for (int t = 0; t < NC; t++) cp_async16(bs + 4 * t, Bc + 4 * t);
-            } else {
-#pragma unroll
-                for (int i = 0; i < N; i++) cp_async4(bs + i, Bc + i);
+        if (q < nrhs) stage_rhs(q);
+        for (int k = q; k < N; k += LPM) {
+            pv[k] = ipiv != nullptr ? ipiv[m * N + k] : k + 1;
+            map[k] = k;
+        }
+    }
+    __syncwarp();
+    if (mvalid && q == 0 && ipiv != nullptr) {
+        // The interchanges k = 0..n-1 applied to the identity row map.
+        for (int k = 0; k < N; k++) {
+            const int p = pv[k] - 1;
+            if ((unsigned)p < (unsigned)N && p != k) {
+                const int t = map[k];
+                map[k] = map[p];
+                map[p] = t;
             }
         }
-    };
-
-    long long g = (long long)blockIdx.x * R::WARPS + warp;
-    int buf = 0;
-    if (g < ngroups) stage(g, 0);
-    cp_async_commit();
-    for (; g < ngroups; g += gstride, buf ^= 1) {
-        if (g + gstride < ngroups) stage(g + gstride, buf ^ 1);
-        cp_async_commit();
-        cp_async_wait_group<1>();  // everything but the prefetch just issued
-        __syncwarp();
-
-        const long long m = g * R::MPW + seg;
-        const bool mvalid = m < batch;
-        float* sm = wbase + buf * R::BUF_WORDS + seg * R::SLOT;
-        int* pv = reinterpret_cast<int*>(sm + R::MAT);
-        int* map = pv + 32;
-        float* bs = wbase + buf * R::BUF_WORDS + R::MPW * R::SLOT + lane * R::BCOL;
-        for (int k = q; k < N; k += LPM) map[k] = k;
-        __syncwarp();
-        if (mvalid && q == 0 && ipiv != nullptr) {
-            // The interchanges k = 0..n-1 applied to the identity row map.
-            for (int k = 0; k < N; k++) {
-                const int p = pv[k] - 1;
-                if ((unsigned)p < (unsigned)N && p != k) {
-                    const int t = map[k];
-                    map[k] = map[p];
-                    map[p] = t;
-                }
-            }
-        }
-        __syncwarp();
-        float* B = mvalid ? Barray[m] : nullptr;
-        const bool bvec = N % 4 == 0 && (ldb & 3) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0;
-        for (int c = q; mvalid && c < nrhs; c += LPM) {
-            float* Bc = B + (long long)c * ldb;
-            if (c != q) {  // further right-hand sides of this lane (nrhs > LPM): synchronous
-                if (bvec) {
-#pragma unroll
-                    for (int t = 0; t < NC; t++)
-                        *reinterpret_cast<float4*>(bs + 4 * t) = *reinterpret_cast<const float4*>(Bc + 4 * t);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < N; i++) bs[i] = Bc[i];
-                }
-            }
-            float2 x2[NPAIR];
-#pragma unroll
-            for (int p = 0; p < NPAIR; p++) x2[p] = make_float2(0.0f, 0.0f);
-            if (!TRANS) {
-#pragma unroll
-                for (int t = 0; t < NC; t++) {
-                    const int4 mp = reinterpret_cast<const int4*>(map)[t];
-                    if (4 * t + 0 < N) x2[2 * t].x = bs[mp.x];
-                    if (4 * t + 1 < N) x2[2 * t].y = bs[mp.y];
-                    if (4 * t + 2 < N) x2[2 * t + 1].x = bs[mp.z];
-                    if (4 * t + 3 < N) x2[2 * t + 1].y = bs[mp.w];
-                }
-                // unit-L forward: x[i] -= L[i][j] * x[j], i > j
-#pragma unroll
-                for (int j = 0; j < N - 1; j++) {
-                    const float xj = pget(x2, j);
-                    const float2 nx = make_float2(-xj, -xj);
-                    const float* lj = sm + j * NP;
-#pragma unroll
-                    for (int t = j / 4; t < NC; t++) {
-                        const float4 l4 = *reinterpret_cast<const float4*>(lj + 4 * t);
-                        if (4 * t > j)
-                            x2[2 * t] = __ffma2_rn(make_float2(l4.x, l4.y), nx, x2[2 * t]);
-                        else if (4 * t + 1 > j)
-                            x2[2 * t].y = fmaf(l4.y, -xj, x2[2 * t].y);
-                        if (4 * t + 2 > j && 4 * t + 2 < N)
-                            x2[2 * t + 1] = __ffma2_rn(make_float2(l4.z, l4.w), nx, x2[2 * t + 1]);
-                        else if (4 * t + 3 > j && 4 * t + 3 < N)
-                            x2[2 * t + 1].y = fmaf(l4.w, -xj, x2[2 * t + 1].y);
-                    }
-                }
-                // U backward: x[j] /= U[j][j]; x[i] -= U[i][j] * x[j], i < j
-#pragma unroll
-                for (int j = N - 1; j >= 0; j--) {
-                    const float* uj = sm + j * NP;
-                    const float4 dj = *reinterpret_cast<const float4*>(uj + 4 * (j / 4));
-                    const float xj = pget(x2, j) / f4get(dj, j % 4);
-                    pset(x2, j, xj);
-                    const float2 nx = make_float2(-xj, -xj);
-#pragma unroll
-                    for (int t = 0; t <= j / 4; t++) {
-                        const float4 u4 = (t == j / 4) ? dj : *reinterpret_cast<const float4*>(uj + 4 * t);
-                        if (4 * t + 1 < j)
-                            x2[2 * t] = __ffma2_rn(make_float2(u4.x, u4.y), nx, x2[2 * t]);
-                        else if (4 * t < j)
-                            x2[2 * t].x = fmaf(u4.x, -xj, x2[2 * t].x);
-                        if (4 * t + 3 < j)
-                            x2[2 * t + 1] = __ffma2_rn(make_float2(u4.z, u4.w), nx, x2[2 * t + 1]);
-                        else if (4 * t + 2 < j)
-                            x2[2 * t + 1].x = fmaf(u4.z, -xj, x2[2 * t + 1].x);
-                    }
-                }
-                if (bvec) {
-#pragma unroll
-                    for (int t = 0; t < NC; t++)
-                        *reinterpret_cast<float4*>(Bc + 4 * t) = make_float4(x2[2 * t].x, x2[2 * t].y,
-                                                                             x2[2 * t + 1].x, x2[2 * t + 1].y);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < N; i++) Bc[i] = pget(x2, i);
-                }
-            } else {
-#pragma unroll
-                for (int t = 0; t < NC; t++) {
-                    const float4 v = *reinterpret_cast<const float4*>(bs + 4 * t);
-                    x2[2 * t] = make_float2(v.x, v.y);
-                    x2[2 * t + 1] = make_float2(v.z, v.w);
-                }
-                // U^T forward: x[i] = (x[i] - sum_{j<i} U[j][i] x[j]) / U[i][i], j ascending
-#pragma unroll
-                for (int i = 0; i < N; i++) {
-                    const float* ui = sm + i * NP;
-                    float sacc = pget(x2, i);
-#pragma unroll
-                    for (int t = 0; t <= i / 4; t++) {
-                        const float4 u4 = *reinterpret_cast<const float4*>(ui + 4 * t);
-#pragma unroll
-                        for (int e = 0; e < 4; e++)
-                            if (4 * t + e < i) sacc = fmaf(-f4get(u4, e), pget(x2, 4 * t + e), sacc);
-                        if (t == i / 4) sacc = sacc / f4get(u4, i % 4);
-                    }
-                    pset(x2, i, sacc);
-                }
-                // L^T backward: x[j] -= sum_{i>j} L[i][j] x[i], i ascending
-#pragma unroll
-                for (int j = N - 2; j >= 0; j--) {
-                    const float* lj = sm + j * NP;
-                    float sacc = pget(x2, j);
-#pragma unroll
-                    for (int t = j / 4; t < NC; t++) {
-                        const float4 l4 = *reinterpret_cast<const float4*>(lj + 4 * t);
-#pragma unroll
-                        for (int e = 0; e < 4; e++)
-                            if (4 * t + e > j && 4 * t + e < N)
-                                sacc = fmaf(-f4get(l4, e), pget(x2, 4 * t + e), sacc);
-                    }
-                    pset(x2, j, sacc);
-                }
-#pragma unroll
-                for (int t = 0; t < NC; t++) {
-                    const int4 mp = reinterpret_cast<const int4*>(map)[t];
-                    if (4 * t + 0 < N) Bc[mp.x] = x2[2 * t].x;
-                    if (4 * t + 1 < N) Bc[mp.y] = x2[2 * t].y;
-                    if (4 * t + 2 < N) Bc[mp.z] = x2[2 * t + 1].x;
-                    if (4 * t + 3 < N) Bc[mp.w] = x2[2 * t + 1].y;
-                }
-            }
-        }
-        __syncwarp();  // the buffer is refilled two iterations later
     }
     cp_async_wait_all();
+    __syncwarp();
+    if (!mvalid) return;
+
+    for (int c = q; c < nrhs; c += LPM) {
+        float* Bc = B + (long long)c * ldb;
+        if (c != q) {  // later right-hand sides of this lane (nrhs > LPM)
+            stage_rhs(c);
+            cp_async_wait_all();
+        }
+        float2 x2[NPAIR];
+#pragma unroll
+        for (int p = 0; p < NPAIR; p++) x2[p] = make_float2(0.0f, 0.0f);
+        if (!TRANS) {
+#pragma unroll
+            for (int t = 0; t < NC; t++) {
+                const int4 mp = reinterpret_cast<const int4*>(map)[t];
+                if (4 * t + 0 < N) x2[2 * t].x = bs[mp.x];
+                if (4 * t + 1 < N) x2[2 * t].y = bs[mp.y];
+                if (4 * t + 2 < N) x2[2 * t + 1].x = bs[mp.z];
+                if (4 * t + 3 < N) x2[2 * t + 1].y = bs[mp.w];
+            }
+            // unit-L forward: x[i] -= L[i][j] * x[j], i > j
+#pragma unroll
+            for (int j = 0; j < N - 1; j++) {
+                const float xj = pget(x2, j);
+                const float2 nx = make_float2(-xj, -xj);
+                const float* lj = sm + j * NP;
+#pragma unroll
+                for (int t = j / 4; t < NC; t++) {
+                    const float4 l4 = *reinterpret_cast<const float4*>(lj + 4 * t);
+                    if (4 * t > j)
+                        x2[2 * t] = __ffma2_rn(make_float2(l4.x, l4.y), nx, x2[2 * t]);
+                    else if (4 * t + 1 > j)
+                        x2[2 * t].y = fmaf(l4.y, -xj, x2[2 * t].y);
+                    if (4 * t + 2 > j && 4 * t + 2 < N)
+                        x2[2 * t + 1] = __ffma2_rn(make_float2(l4.z, l4.w), nx, x2[2 * t + 1]);
+                    else if (4 * t + 3 > j && 4 * t + 3 < N)
+                        x2[2 * t + 1].y = fmaf(l4.w, -xj, x2[2 * t + 1].y);
+                }
+            }
+            // U backward: x[j] /= U[j][j]; x[i] -= U[i][j] * x[j], i < j
+#pragma unroll
+            for (int j = N - 1; j >= 0; j--) {
+                const float* uj = sm + j * NP;
+                const float4 dj = *reinterpret_cast<const float4*>(uj + 4 * (j / 4));
+                const float xj = pget(x2, j) / f4get(dj, j % 4);
+                pset(x2, j, xj);
+                const float2 nx = make_float2(-xj, -xj);
+#pragma unroll
+                for (int t = 0; t <= j / 4; t++) {
+                    const float4 u4 = (t == j / 4) ? dj : *reinterpret_cast<const float4*>(uj + 4 * t);
+                    if (4 * t + 1 < j)
+                        x2[2 * t] = __ffma2_rn(make_float2(u4.x, u4.y), nx, x2[2 * t]);
+                    else if (4 * t < j)
+                        x2[2 * t].x = fmaf(u4.x, -xj, x2[2 * t].x);
+                    if (4 * t + 3 < j)
+                        x2[2 * t + 1] = __ffma2_rn(make_float2(u4.z, u4.w), nx, x2[2 * t + 1]);
+                    else if (4 * t + 2 < j)
+                        x2[2 * t + 1].x = fmaf(u4.z, -xj, x2[2 * t + 1].x);
+                }
+            }
+            if (bvec) {
+#pragma unroll
+                for (int t = 0; t < NC; t++)
+                    *reinterpret_cast<float4*>(Bc + 4 * t) = make_float4(x2[2 * t].x, x2[2 * t].y, x2[2 * t + 1].x,
+                                                                         x2[2 * t + 1].y);
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; i++) Bc[i] = pget(x2, i);
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < NC; t++) {
+                const float4 v = *reinterpret_cast<const float4*>(bs + 4 * t);
+                x2[2 * t] = make_float2(v.x, v.y);
+                x2[2 * t + 1] = make_float2(v.z, v.w);
+            }
+            // U^T forward: x[i] = (x[i] - sum_{j<i} U[j][i] x[j]) / U[i][i], j ascending
+#pragma unroll
+            for (int i = 0; i < N; i++) {
+                const float* ui = sm + i * NP;
+                float sacc = pget(x2, i);
+#pragma unroll
+                for (int t = 0; t <= i / 4; t++) {
+                    const float4 u4 = *reinterpret_cast<const float4*>(ui + 4 * t);
+#pragma unroll
+                    for (int e = 0; e < 4; e++)
+                        if (4 * t + e < i) sacc = fmaf(-f4get(u4, e), pget(x2, 4 * t + e), sacc);
+                    if (t == i / 4) sacc = sacc / f4get(u4, i % 4);
+                }
+                pset(x2, i, sacc);
+            }
+            // L^T backward: x[j] -= sum_{i>j} L[i][j] x[i], i ascending
+#pragma unroll
+            for (int j = N - 2; j >= 0; j--) {
+                const float* lj = sm + j * NP;
+                float sacc = pget(x2, j);
+#pragma unroll
+                for (int t = j / 4; t < NC; t++) {
+                    const float4 l4 = *reinterpret_cast<const float4*>(lj + 4 * t);
+#pragma unroll
+                    for (int e = 0; e < 4; e++)
+                        if (4 * t + e > j && 4 * t + e < N) sacc = fmaf(-f4get(l4, e), pget(x2, 4 * t + e), sacc);
+                }
+                pset(x2, j, sacc);
+            }
+#pragma unroll
+            for (int t = 0; t < NC; t++) {
+                const int4 mp = reinterpret_cast<const int4*>(map)[t];
+                if (4 * t + 0 < N) Bc[mp.x] = x2[2 * t].x;
+                if (4 * t + 1 < N) Bc[mp.y] = x2[2 * t].y;
+                if (4 * t + 2 < N) Bc[mp.z] = x2[2 * t + 1].x;
+                if (4 * t + 3 < N) Bc[mp.w] = x2[2 * t + 1].y;
+            }
+        }
+    }
 }
 
 template <int N, int LPM, bool TRANS>
@@ -318,18 +291,14 @@ inline void launch_getrs_rhs(cudaStream_t st, const float* const* Aarray, int ld
                              float* const* Barray, int ldb, int nrhs, int batch)
 {
     using R = RhsShape<N, LPM>;
-    static int ctas_per_sm = 0;
-    if (ctas_per_sm == 0) {
+    static bool configured = false;
+    if (!configured) {
         cudaFuncSetAttribute(getrs_rhs_kernel<N, LPM, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)R::SMEM);
-        int v = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, getrs_rhs_kernel<N, LPM, TRANS>, R::WARPS * 32, R::SMEM);
-        ctas_per_sm = v > 0 ? v : 1;
+        configured = true;
     }
-    const long long groups = (batch + R::MPW - 1) / R::MPW;
-    const long long need = (groups + R::WARPS - 1) / R::WARPS;
-    const long long cap = (long long)ctas_per_sm * sm_count();
-    const unsigned grid = (unsigned)(need < cap ? need : cap);
+    constexpr int per_cta = R::WARPS * R::MPW;
+    const unsigned grid = (unsigned)((batch + per_cta - 1) / per_cta);
     getrs_rhs_kernel<N, LPM, TRANS><<<grid, R::WARPS * 32, R::SMEM, st>>>(Aarray, lda, ipiv, Barray, ldb, nrhs,
                                                                          batch);
 }
