@@ -108,6 +108,48 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetriBatched(
     aclblasHandle_t handle, int n, const float* const Aarray[], int lda, const int* PivotArray,
     float* const Carray[], int ldc, int* infoArray, int batchSize);
 
+/* Replaces aclblasGemmBatchedEx (include/cann_ops_blas.h:409;
+ * blas/gemm_batched_ex/arch35/gemm_batched_ex_host.cpp:156-581). C[i] = alpha*op(A[i])*op(B[i]) +
+ * beta*C[i]; alpha and beta are HOST pointers to float. Validation order: handle, alpha/beta
+ * (INVALID_VALUE), m/n/k/trans/batchCount (INVALID_VALUE), lda/ldb/ldc (INVALID_VALUE), algo !=
+ * DEFAULT (NOT_SUPPORTED), dtype combination (NOT_SUPPORTED), NULL arrays when batchCount > 0
+ * (INVALID_VALUE). Dtype combinations: the reference's FP16/BF16/FP8 table
+ * (gemm_batched_ex_host.cpp:87-118) plus FP32/FP32/FP32 with ACLBLAS_COMPUTE_32F_PEDANTIC (plain
+ * FP32), ACLBLAS_COMPUTE_32F_FAST_TF32 or ACLBLAS_COMPUTE_32F_FAST_16BF (FP32 under
+ * ACLBLAS_COMPUTE_32F stays NOT_SUPPORTED, as in the reference). No workspace, no host copy. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasGemmBatchedEx(
+    aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m, int n, int k,
+    const void* alpha, const void* const Aarray[], aclDataType Atype, int lda, const void* const Barray[],
+    aclDataType Btype, int ldb, const void* beta, void* const Carray[], aclDataType Ctype, int ldc, int batchCount,
+    aclblasComputeType_t computeType, aclblasGemmAlgo_t algo);
+
+/* ------------------------------------------------------------------------ extensions --- */
+
+/* Factor, solve and refine in one call; no counterpart in the reference. Aarray (kept
+ * unchanged) is copied to LUarray and factored (PivotArray, infoArray as for
+ * aclblasSgetrfBatched); computeType ACLBLAS_COMPUTE_32F factors in plain FP32,
+ * ACLBLAS_COMPUTE_32F_FAST_TF32 / _FAST_16BF use a split (hi + lo) TF32 / BF16 trailing update.
+ * X = LU \ B, then up to maxIter refinement steps: r = B - A X and the normwise backward error
+ * max_c ||r_c||inf / (||A||inf ||x_c||inf + ||b_c||inf) are computed in FP64 on the GPU;
+ * matrices whose error is <= tol stop, the others add LU \ r to X. berrArray (double),
+ * iterArray (refinement steps used; maxIter if not converged) and infoArray are device arrays.
+ * Needs n*nrhs*4 (rounded up to 256) + 12 bytes per matrix of handle workspace
+ * (aclblasSetWorkspace); EXECUTION_FAILED if it is smaller. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
+    aclblasHandle_t handle, int n, int nrhs, const float* const Aarray[], int lda, float* const LUarray[], int ldlu,
+    int* PivotArray, const float* const Barray[], int ldb, float* const Xarray[], int ldx,
+    aclblasComputeType_t computeType, int maxIter, double tol, double* berrArray, int* iterArray, int* infoArray,
+    int batchCount);
+
+/* Adjoint of the batched solve X = A^{-1} B; no counterpart in the reference. With the LU
+ * factors / pivots of aclblasSgetrfBatched, the solution X and the upstream gradient dX:
+ * dX is overwritten by dB = A^{-T} dX (transposed solve on the stored factors) and, when
+ * dAarray is not NULL, dA = -dB X^T is written (overwritten, not accumulated). nrhs <= 256. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrsAdjointBatched(
+    aclblasHandle_t handle, int n, int nrhs, const float* const LUarray[], int lda, const int* devIpiv,
+    const float* const Xarray[], int ldx, float* const dXarray[], int lddx, float* const dAarray[], int ldda,
+    int batchCount);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,7 +50,18 @@ SIGNATURES = {
     "aclblasSgetrsBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip,
                                        C.c_int]),
     "aclblasSgetriBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int]),
+    "aclblasGemmBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int,
+                                       _vp, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "aclblasSgetrfsRefineBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp,
+                                                C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp,
+                                                _vp, C.c_int]),
+    "aclblasSgetrsAdjointBatched": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp,
+                                              C.c_int, _vp, C.c_int, C.c_int]),
 }
+
+# aclDataType (include/acl/acl.h) and aclblasComputeType_t (include/cann_ops_blas_common.h)
+ACL_FLOAT, ACL_FLOAT16, ACL_BF16, ACL_FLOAT8_E5M2, ACL_FLOAT8_E4M3FN = 0, 1, 27, 35, 36
+COMPUTE_16F, COMPUTE_32F, COMPUTE_32F_PEDANTIC, COMPUTE_32F_FAST_16BF, COMPUTE_32F_FAST_TF32 = 0, 2, 3, 5, 6
 
 _lib = None
 
@@ -106,6 +117,7 @@ class Handle:
     """aclblasHandle_t bound to the current torch stream at creation (re-bind with set_stream)."""
 
     def __init__(self, stream=None):
+        self._ws = None
         self.h = _vp()
         check("aclblasCreate", lib().aclblasCreate(C.byref(self.h)))
         self.set_stream(stream)
@@ -120,6 +132,7 @@ class Handle:
         if self.h:
             check("aclblasDestroy", lib().aclblasDestroy(self.h))
             self.h = _vp()
+        self._ws = None
 
     def __enter__(self):
         return self
@@ -158,6 +171,50 @@ class Handle:
             C.byref(info), LU.shape[0]))
         return info.value
 
+    def gemm_batched_ex(self, transa, transb, m, n, k, alpha, A, atype, lda, B, btype, ldb, beta, Cm, ctype, ldc,
+                        compute=COMPUTE_32F, aptr=None, bptr=None, cptr=None):
+        """aclblasGemmBatchedEx on batch tensors; alpha/beta are Python floats."""
+        a = C.c_float(alpha)
+        b = C.c_float(beta)
+        aptr = ptr_array(A) if aptr is None else aptr
+        bptr = ptr_array(B) if bptr is None else bptr
+        cptr = ptr_array(Cm) if cptr is None else cptr
+        check("aclblasGemmBatchedEx", lib().aclblasGemmBatchedEx(
+            self.h, TRANS[transa], TRANS[transb], m, n, k, C.byref(a), aptr.data_ptr(), atype, lda,
+            bptr.data_ptr(), btype, ldb, C.byref(b), cptr.data_ptr(), ctype, ldc, Cm.shape[0], compute, 0))
+
+    def refine(self, A, B, n, nrhs, compute=COMPUTE_32F_FAST_TF32, max_iter=10, tol=1e-6):
+        """Factor + solve + iterative refinement (aclblasSgetrfsRefineBatchedEx).
+        A (batch, n, n) and B (batch, nrhs, n) are left unchanged. Returns
+        (X, LU, piv, info, berr, iters)."""
+        torch = _torch()
+        batch = A.shape[0]
+        dev = A.device
+        LU = torch.empty_like(A)
+        X = torch.empty_like(B)
+        piv = torch.empty((batch, n), dtype=torch.int32, device=dev)
+        info = torch.empty(batch, dtype=torch.int32, device=dev)
+        berr = torch.empty(batch, dtype=torch.float64, device=dev)
+        iters = torch.empty(batch, dtype=torch.int32, device=dev)
+        need = (((n * nrhs * 4 + 255) // 256) * 256 + 12) * batch + 512
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = torch.empty(max(need, 32 << 20), dtype=torch.uint8, device=dev)
+            check("aclblasSetWorkspace", lib().aclblasSetWorkspace(self.h, _vp(self._ws.data_ptr()),
+                                                                   self._ws.numel()))
+        check("aclblasSgetrfsRefineBatchedEx", lib().aclblasSgetrfsRefineBatchedEx(
+            self.h, n, nrhs, ptr_array(A).data_ptr(), n, ptr_array(LU).data_ptr(), n, piv.data_ptr(),
+            ptr_array(B).data_ptr(), n, ptr_array(X).data_ptr(), n, compute, max_iter, tol, berr.data_ptr(),
+            iters.data_ptr(), info.data_ptr(), batch))
+        return X, LU, piv, info, berr, iters
+
+    def adjoint(self, LU, n, lda, piv, X, ldx, dX, lddx, dA=None, ldda=None):
+        """dX <- A^{-T} dX (= dB); dA <- -dB X^T when dA is given (aclblasSgetrsAdjointBatched)."""
+        nrhs = X.shape[1]
+        check("aclblasSgetrsAdjointBatched", lib().aclblasSgetrsAdjointBatched(
+            self.h, n, nrhs, ptr_array(LU).data_ptr(), lda, _addr(piv), ptr_array(X).data_ptr(), ldx,
+            ptr_array(dX).data_ptr(), lddx, None if dA is None else ptr_array(dA).data_ptr(),
+            ldda if ldda is not None else n, LU.shape[0]))
+
     def getri(self, LU, n, lda, piv, Cinv, ldc, info=None, aptr=None, cptr=None):
         """Cinv = inverse from the LU factors; returns the info tensor."""
         torch = _torch()
@@ -168,3 +225,61 @@ class Handle:
         check("aclblasSgetriBatched", lib().aclblasSgetriBatched(
             self.h, n, aptr.data_ptr(), lda, _addr(piv), cptr.data_ptr(), ldc, info.data_ptr(), LU.shape[0]))
         return info
+
+
+# ------------------------------------------------------------------ differentiable solve --
+
+_default_handle = None
+
+
+def default_handle():
+    global _default_handle
+    if _default_handle is None:
+        _default_handle = Handle()
+    else:
+        _default_handle.set_stream()
+    return _default_handle
+
+
+def _solve_function():
+    torch = _torch()
+
+    class BatchedSolve(torch.autograd.Function):
+        """X = A^{-1} B for a batch. A: (batch, n, n), B: (batch, nrhs, n), both in the
+        column-major batch convention of this module (element (i, j) of A[b] is A[b, j, i]).
+        Forward: getrf + getrs (N). Backward: aclblasSgetrsAdjointBatched on the saved LU
+        factors and pivots -- dB = A^{-T} dX, dA = -dB X^T."""
+
+        @staticmethod
+        def forward(ctx, A, B):
+            h = default_handle()
+            n = A.shape[1]
+            LU = A.detach().contiguous().clone()
+            X = B.detach().contiguous().clone()
+            piv, info = h.getrf(LU, n, n)
+            h.getrs("N", LU, n, n, piv, X, X.shape[1], n)
+            ctx.save_for_backward(LU, piv, X)
+            return X
+
+        @staticmethod
+        def backward(ctx, dX):
+            LU, piv, X = ctx.saved_tensors
+            h = default_handle()
+            n = LU.shape[1]
+            dB = dX.detach().contiguous().clone()
+            dA = torch.empty_like(LU) if ctx.needs_input_grad[0] else None
+            h.adjoint(LU, n, n, piv, X, n, dB, n, dA, n)
+            return dA, (dB if ctx.needs_input_grad[1] else None)
+
+    return BatchedSolve
+
+
+_BatchedSolve = None
+
+
+def batched_solve(A, B):
+    """Differentiable batched solve through the C ABI (see _solve_function)."""
+    global _BatchedSolve
+    if _BatchedSolve is None:
+        _BatchedSolve = _solve_function()
+    return _BatchedSolve.apply(A, B)

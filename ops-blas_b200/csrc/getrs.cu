@@ -113,6 +113,25 @@ getrs_generic_kernel(const float* const* __restrict__ Aarray, int n, int lda, co
 
 }  // namespace opsblas
 
+namespace opsblas {
+
+cudaError_t getrs_launch(cudaStream_t st, bool tr, int n, int nrhs, const float* const* Aarray, int lda,
+                         const int* devIpiv, float* const* Barray, int ldb, int batchCount)
+{
+    if (n <= 32) {
+        if (tr)
+            getrs_small_dispatch_t(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
+        else
+            getrs_small_dispatch_n(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
+    } else {
+        getrs_generic_kernel<<<(unsigned)batchCount, kGenericThreads, 0, st>>>(Aarray, n, lda, devIpiv, Barray, ldb,
+                                                                               nrhs, tr ? 1 : 0);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace opsblas
+
 using namespace opsblas;
 
 namespace {
@@ -182,16 +201,6 @@ extern "C" aclblasStatus_t aclblasSgetrsBatched(
     set_info(info, 0);
     if (n == 0 || nrhs == 0 || batchCount == 0) return ACLBLAS_STATUS_SUCCESS;
 
-    cudaStream_t st = handle->stream;
-    const bool tr = trans != ACLBLAS_OP_N;
-    if (n <= 32) {
-        if (tr)
-            getrs_small_dispatch_t(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
-        else
-            getrs_small_dispatch_n(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
-    } else {
-        getrs_generic_kernel<<<(unsigned)batchCount, kGenericThreads, 0, st>>>(Aarray, n, lda, devIpiv, Barray, ldb,
-                                                                               nrhs, tr ? 1 : 0);
-    }
-    return launch_status(kApi, cudaGetLastError());
+    return launch_status(kApi, getrs_launch(handle->stream, trans != ACLBLAS_OP_N, n, nrhs, Aarray, lda, devIpiv,
+                                            Barray, ldb, batchCount));
 }

@@ -40,4 +40,23 @@ aclblasStatus_t launch_status(const char* api, cudaError_t err);
 
 inline int max1(int n) { return n > 1 ? n : 1; }
 
+// Validation-free launchers shared by the entry points (getrs.cu, gemm_batched_ex.cu).
+cudaError_t getrs_launch(cudaStream_t st, bool trans, int n, int nrhs, const float* const* Aarray, int lda,
+                         const int* devIpiv, float* const* Barray, int ldb, int batchCount);
+// C = alpha * op(A) * op(B) + beta * C, FP32 operands; round: 0 none, 1 TF32, 2 BF16.
+cudaError_t gemm_f32_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
+                            const float* const* A, int lda, const float* const* B, int ldb, float beta,
+                            float* const* C, int ldc, int batch, int round);
+
+// getrf_large.cu: 32 < n <= 640, matrix in global memory; mode 0 plain FP32 (reference
+// operation order), 1 = TF32 split trailing update, 2 = BF16 split trailing update.
+bool getrf_large_supported(int n);
+cudaError_t getrf_large_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch,
+                               int mode);
+
+// getrf_medium.cu: 32 < n <= 128, matrix resident in shared memory.
+bool getrf_medium_supported(int n);
+cudaError_t getrf_medium_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info,
+                                int batch);
+
 }  // namespace opsblas

@@ -1,0 +1,248 @@
+// aclblasSgetrfsRefineBatchedEx: factor + solve + iterative refinement, one call.
+//
+// No counterpart in the reference (an extension next to the drop-in chain). Per matrix:
+//   LU = A (copy; A is kept for the residual), P*LU = A factored by aclblasSgetrfBatched's
+//   kernels -- plain FP32 for ACLBLAS_COMPUTE_32F, or with the split TF32 / BF16 trailing
+//   update for ACLBLAS_COMPUTE_32F_FAST_TF32 / _FAST_16BF (getrf_large.cu);
+//   X = LU \ B (aclblasSgetrsBatched's kernels);
+//   repeat up to maxIter times: r = B - A X in FP64 on the GPU, backward error
+//     berr = max_c ||r_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf) in FP64;
+//     matrices with berr <= tol stop; the others solve LU d = r (FP32) and set X += d.
+// Convergence is tracked on the device (no host synchronisation inside the call), so the
+// call can be captured in a CUDA graph. berrArray / iterArray / infoArray are device arrays.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace opsblas {
+
+__global__ void init_ptr_array_kernel(float** out, float* base, long long stride, int count)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
+        out[i] = base + i * stride;
+}
+
+// dst[b](i, j) = src[b](i, j), i < rows, j < cols
+__global__ void copy_batched_kernel(const float* const* src, int lds, float* const* dst, int ldd, int rows, int cols)
+{
+    const float* s = src[blockIdx.x];  // one CTA per matrix
+    float* d = dst[blockIdx.x];
+    for (long long e = threadIdx.x; e < (long long)rows * cols; e += blockDim.x) {
+        const long long i = e % rows, j = e / rows;
+        d[i + j * ldd] = s[i + j * lds];
+    }
+}
+
+constexpr int kResThreads = 256;
+constexpr int kResMaxRhs = 16;  // right-hand sides per pass
+
+// One CTA per matrix. FP64 residual r = b - A x and normwise backward error; on the last check
+// (final != 0) only the error is recorded. d receives r in FP32 (or zeros when converged).
+__global__ void __launch_bounds__(kResThreads)
+refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, const float* const* Barray, int ldb,
+                       const float* const* Xarray, int ldx, float* const* Darray, int ldd, double tol, int it,
+                       int final_check, int* __restrict__ done, double* __restrict__ berr, int* __restrict__ iters)
+{
+    extern __shared__ double xs[];  // [n][kResMaxRhs]
+    __shared__ double red[kResThreads / 32];
+    __shared__ double s_anorm;
+    __shared__ double s_berr;
+    const long long m = blockIdx.x;
+    const float* A = Aarray[m];
+    const float* B = Barray[m];
+    const float* X = Xarray[m];
+    float* D = Darray[m];
+    const int tid = threadIdx.x;
+    const bool was_done = done[m] != 0;
+    if (was_done && !final_check) {
+        for (long long e = tid; e < (long long)n * nrhs; e += kResThreads) D[e % n + (e / n) * ldd] = 0.0f;
+        return;
+    }
+    auto block_max = [&](double v) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+        if ((tid & 31) == 0) red[tid >> 5] = v;
+        __syncthreads();
+        double r = red[0];
+        for (int q = 1; q < kResThreads / 32; q++) r = fmax(r, red[q]);
+        __syncthreads();
+        return r;
+    };
+    // ||A||_inf (max row sum)
+    double rowmax = 0.0;
+    for (int i = tid; i < n; i += kResThreads) {
+        double s = 0.0;
+        for (int j = 0; j < n; j++) s += fabs((double)A[i + (long long)j * lda]);
+        rowmax = fmax(rowmax, s);
+    }
+    const double anorm = block_max(rowmax);
+    if (tid == 0) {
+        s_anorm = anorm;
+        s_berr = 0.0;
+    }
+    double worst = 0.0;
+    for (int c0 = 0; c0 < nrhs; c0 += kResMaxRhs) {
+        const int cw = min(kResMaxRhs, nrhs - c0);
+        __syncthreads();
+        for (int e = tid; e < n * cw; e += kResThreads) {
+            const int i = e % n, c = e / n;
+            xs[i * kResMaxRhs + c] = (double)X[i + (long long)(c0 + c) * ldx];
+        }
+        __syncthreads();
+        double rmax[kResMaxRhs], xmax[kResMaxRhs], bmax[kResMaxRhs];
+#pragma unroll
+        for (int c = 0; c < kResMaxRhs; c++) rmax[c] = xmax[c] = bmax[c] = 0.0;
+        for (int i = tid; i < n; i += kResThreads) {
+            double r[kResMaxRhs];
+#pragma unroll
+            for (int c = 0; c < kResMaxRhs; c++) {
+                const double b = c < cw ? (double)B[i + (long long)(c0 + c) * ldb] : 0.0;
+                r[c] = b;
+                bmax[c] = fmax(bmax[c], fabs(b));
+            }
+            for (int j = 0; j < n; j++) {
+                const double a = (double)A[i + (long long)j * lda];
+#pragma unroll
+                for (int c = 0; c < kResMaxRhs; c++) r[c] = fma(-a, xs[j * kResMaxRhs + c], r[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < kResMaxRhs; c++) {
+                if (c < cw) {
+                    rmax[c] = fmax(rmax[c], fabs(r[c]));
+                    xmax[c] = fmax(xmax[c], fabs(xs[i * kResMaxRhs + c]));
+                    if (!final_check) D[i + (long long)(c0 + c) * ldd] = (float)r[c];
+                }
+            }
+        }
+        for (int c = 0; c < cw; c++) {
+            const double rn = block_max(rmax[c]);
+            const double xn = block_max(xmax[c]);
+            const double bn = block_max(bmax[c]);
+            const double den = s_anorm * xn + bn;
+            const double e = den > 0.0 ? rn / den : (rn > 0.0 ? INFINITY : 0.0);
+            worst = fmax(worst, e);
+        }
+    }
+    __syncthreads();
+    const bool conv = worst <= tol;
+    if (tid == 0) {
+        berr[m] = worst;
+        if (!was_done && (conv || final_check)) {
+            done[m] = conv ? 1 : 0;
+            iters[m] = it;
+        }
+        if (conv && !final_check) done[m] = 1;
+    }
+    if (conv && !final_check) {
+        __syncthreads();
+        for (long long e = tid; e < (long long)n * nrhs; e += kResThreads) D[e % n + (e / n) * ldd] = 0.0f;
+    }
+}
+
+__global__ void axpy_batched_kernel(int n, int nrhs, const float* const* Darray, int ldd, float* const* Xarray, int ldx)
+{
+    const float* D = Darray[blockIdx.x];  // one CTA per matrix
+    float* X = Xarray[blockIdx.x];
+    for (long long e = threadIdx.x; e < (long long)n * nrhs; e += blockDim.x) {
+        const long long i = e % n, c = e / n;
+        X[i + c * ldx] += D[i + c * ldd];
+    }
+}
+
+__global__ void fill_int_kernel(int* p, int v, int count)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
+}  // namespace opsblas
+
+using namespace opsblas;
+
+extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
+    aclblasHandle_t handle, int n, int nrhs, const float* const Aarray[], int lda, float* const LUarray[], int ldlu,
+    int* PivotArray, const float* const Barray[], int ldb, float* const Xarray[], int ldx,
+    aclblasComputeType_t computeType, int maxIter, double tol, double* berrArray, int* iterArray, int* infoArray,
+    int batchCount)
+{
+    static const char* kApi = "aclblasSgetrfsRefineBatchedEx";
+    if (handle == nullptr) {
+        log_error(kApi, "handle is nullptr");
+        return ACLBLAS_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (n < 0 || nrhs < 0 || batchCount < 0 || maxIter < 0 || !(tol >= 0.0)) {
+        log_error(kApi, "invalid size or control argument (n=%d nrhs=%d batch=%d maxIter=%d)", n, nrhs, batchCount,
+                  maxIter);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (lda < max1(n) || ldlu < max1(n) || ldb < max1(n) || ldx < max1(n)) {
+        log_error(kApi, "leading dimensions must be >= max(1, n)");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    int mode;
+    switch (computeType) {
+        case ACLBLAS_COMPUTE_32F: mode = 0; break;
+        case ACLBLAS_COMPUTE_32F_FAST_TF32: mode = 1; break;
+        case ACLBLAS_COMPUTE_32F_FAST_16BF: mode = 2; break;
+        default:
+            log_error(kApi, "computeType must be 32F, 32F_FAST_TF32 or 32F_FAST_16BF, got %d", (int)computeType);
+            return ACLBLAS_STATUS_NOT_SUPPORTED;
+    }
+    if (n == 0 || batchCount == 0) return ACLBLAS_STATUS_SUCCESS;
+    if (!Aarray || !LUarray || !PivotArray || !Barray || !Xarray || !berrArray || !iterArray || !infoArray) {
+        log_error(kApi, "array arguments must not be nullptr");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    // workspace: correction block D (n x nrhs per matrix), its pointer array, done flags
+    const size_t dbytes = ((size_t)n * nrhs * 4 + 255) / 256 * 256;
+    const size_t need = dbytes * batchCount + (size_t)batchCount * 8 + (size_t)batchCount * 4 + 512;
+    if (handle->workspace_size < need) {
+        log_error(kApi, "workspace required %zu bytes, but only %zu available; call aclblasSetWorkspace", need,
+                  handle->workspace_size);
+        return ACLBLAS_STATUS_EXECUTION_FAILED;
+    }
+    char* ws = static_cast<char*>(handle->workspace);
+    float* dbase = reinterpret_cast<float*>(ws);
+    float** dptr = reinterpret_cast<float**>(ws + dbytes * batchCount);
+    int* done = reinterpret_cast<int*>(reinterpret_cast<char*>(dptr) + (size_t)batchCount * 8);
+    cudaStream_t st = handle->stream;
+    const unsigned bgrid = (unsigned)((batchCount + 255) / 256 < 4096 ? (batchCount + 255) / 256 : 4096);
+
+    init_ptr_array_kernel<<<bgrid, 256, 0, st>>>(dptr, dbase, (long long)(dbytes / 4), batchCount);
+    fill_int_kernel<<<bgrid, 256, 0, st>>>(done, 0, batchCount);
+    fill_int_kernel<<<bgrid, 256, 0, st>>>(iterArray, maxIter, batchCount);
+    copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return launch_status(kApi, err);
+    if (n > 32 && getrf_large_supported(n) && (mode != 0 || n > 128)) {
+        err = getrf_large_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
+    } else {
+        aclblasStatus_t s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
+        if (s != ACLBLAS_STATUS_SUCCESS) return s;
+    }
+    if (err != cudaSuccess || nrhs == 0) return launch_status(kApi, err);
+    copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Barray, ldb, Xarray, ldx, n, nrhs);
+    err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, Xarray, ldx, batchCount);
+    if (err != cudaSuccess) return launch_status(kApi, err);
+    const int rhs_chunk = nrhs < kResMaxRhs ? nrhs : kResMaxRhs;
+    (void)rhs_chunk;
+    const size_t rsm = (size_t)n * kResMaxRhs * 8;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(refine_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        configured = true;
+    }
+    if (rsm > 200 * 1024) {
+        log_error(kApi, "n=%d exceeds the residual kernel's shared-memory limit", n);
+        return ACLBLAS_STATUS_NOT_SUPPORTED;
+    }
+    for (int it = 0; it < maxIter; it++) {
+        refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
+            n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, it, 0, done, berrArray, iterArray);
+        err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, dptr, n, batchCount);
+        if (err != cudaSuccess) return launch_status(kApi, err);
+        axpy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(n, nrhs, dptr, n, Xarray, ldx);
+    }
+    refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
+        n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, maxIter, 1, done, berrArray, iterArray);
+    return launch_status(kApi, cudaGetLastError());
+}

@@ -187,3 +187,33 @@ GETRI_ERRORS = [
 def work(case) -> int:
     """Rough n^3 * batch size, to keep the slowest CPU-side checks optional."""
     return max(case.n, 0) ** 3 * max(case.batch, 0)
+
+# GemmBatchedEx error rows (test/gemm_batched_ex/arch35/gemm_batched_ex_test.csv, expect != SUCCESS):
+# (name, transA, transB, m, n, k, Atype, Btype, Ctype, lda, ldb, ldc, batch, compute, algo,
+#  alpha_null, beta_null, a_null, b_null, c_null, null_handle, status)
+GEMM_ERRORS = [
+    ("L0_24", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 1, HN),
+    ("L0_25", "N", "N", -1, 128, 128, "F16", "F16", "F16", 1, 128, 1, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L0_26", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 1, 0, 0, 0, 0, 0, IV),
+    ("L0_27", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 1, 0, 0, 0, 0, IV),
+    ("L0_28", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, -1, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L0_29", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 1, 0, 0, 0, IV),
+    ("L0_30", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 1, 0, 0, IV),
+    ("L0_31", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 1, 0, IV),
+    ("L0_32", "N", "N", 128, 128, 128, "F16", "F16", "F16", 64, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L0_33", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 64, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L0_34", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 64, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L0_35", "T", "N", 128, 128, 128, "F16", "F16", "F16", 64, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L0_36", "N", "N", 128, 128, 128, "F32", "F32", "F32", 128, 128, 128, 4, "32F", 0, 0, 0, 0, 0, 0, 0, "NOT_SUPPORTED"),
+    ("L0_37", "N", "N", 128, 128, 128, "E4M3", "E4M3", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0,
+     "NOT_SUPPORTED"),
+    ("L1_36", "N", "N", 128, -1, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L1_37", "N", "N", 128, 128, -1, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L1_38", "INVALID", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L1_39", "N", "INVALID", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 0, 0, IV),
+    ("L1_40", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 0, 0, 0, 0, 0, 1, 0, IV),
+    ("L1_41", "N", "N", 128, 128, 128, "F16", "F32", "F16", 128, 128, 128, 4, "32F", 0, 0, 0, 0, 0, 0, 0,
+     "NOT_SUPPORTED"),
+    ("L1_42", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 1, 0, 0, 0, 0, 0, 0,
+     "NOT_SUPPORTED"),
+]

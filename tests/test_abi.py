@@ -175,3 +175,49 @@ def test_logger_file_sink(ob, tmp_path):
         L.aclblasLoggerConfigure(0, 0, 0, None)
     text = open(path.decode()).read()
     assert "lda must be >= max(1, n)" in text
+
+
+from cases import GEMM_ERRORS  # noqa: E402
+
+DT = {"F32": 0, "F16": 1, "BF16": 27, "E5M2": 35, "E4M3": 36}
+CT = {"16F": 0, "32F": 2}
+
+
+@pytest.mark.parametrize("row", GEMM_ERRORS, ids=lambda r: r[0])
+def test_gemm_batched_ex_error_rows(ob, row):
+    (name, ta, tb, m, n, k, at, bt, ct, lda, ldb, ldc, batch, comp, algo, an, bn, a0, b0, c0, hn, status) = row
+    one = C.c_float(1.0)
+    zero = C.c_float(0.0)
+    tr = lambda t: 999 if t == "INVALID" else ob.TRANS[t]  # noqa: E731
+    st = ob.lib().aclblasGemmBatchedEx(
+        None if hn else H, tr(ta), tr(tb), m, n, k, None if an else C.byref(one), None if a0 else P, DT[at], lda,
+        None if b0 else P, DT[bt], ldb, None if bn else C.byref(zero), None if c0 else P, DT[ct], ldc, batch,
+        CT[comp], algo)
+    assert ob.STATUS[st] == status
+
+
+def test_gemm_batched_ex_fp32_extension_and_noop(ob):
+    L = ob.lib()
+    one, zero = C.c_float(1.0), C.c_float(0.0)
+    # FP32 operands accepted with the PEDANTIC and FAST compute types (no-op sizes: nothing touched)
+    for comp in (3, 5, 6):
+        assert L.aclblasGemmBatchedEx(H, ob.OP_N, ob.OP_N, 0, 4, 4, C.byref(one), P, 0, 4, P, 0, 4, C.byref(zero),
+                                      P, 0, 4, 2, comp, 0) == ob.SUCCESS
+    assert L.aclblasGemmBatchedEx(H, ob.OP_N, ob.OP_N, 4, 4, 4, C.byref(one), P, 0, 4, P, 0, 4, C.byref(zero), P,
+                                  0, 4, 0, 6, 0) == ob.SUCCESS
+
+
+def test_refine_and_adjoint_validation(ob):
+    L = ob.lib()
+    assert L.aclblasSgetrfsRefineBatchedEx(None, 4, 1, P, 4, P, 4, P, P, 4, P, 4, 6, 5, 1e-6, P, P, P, 2) == \
+        ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSgetrfsRefineBatchedEx(H, 4, 1, P, 3, P, 4, P, P, 4, P, 4, 6, 5, 1e-6, P, P, P, 2) == \
+        ob.INVALID_VALUE
+    assert L.aclblasSgetrfsRefineBatchedEx(H, 4, 1, P, 4, P, 4, P, P, 4, P, 4, 0, 5, 1e-6, P, P, P, 2) == \
+        ob.NOT_SUPPORTED
+    assert L.aclblasSgetrfsRefineBatchedEx(H, 0, 1, None, 1, None, 1, None, None, 1, None, 1, 6, 5, 1e-6, None,
+                                           None, None, 2) == ob.SUCCESS
+    assert L.aclblasSgetrsAdjointBatched(None, 4, 1, P, 4, P, P, 4, P, 4, P, 4, 2) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSgetrsAdjointBatched(H, 4, 257, P, 4, P, P, 4, P, 4, P, 4, 2) == ob.INVALID_VALUE
+    assert L.aclblasSgetrsAdjointBatched(H, 4, 2, P, 4, P, P, 3, P, 4, P, 4, 2) == ob.INVALID_VALUE
+    assert L.aclblasSgetrsAdjointBatched(H, 4, 0, None, 4, None, None, 4, None, 4, None, 4, 2) == ob.SUCCESS

@@ -142,7 +142,7 @@ def test_getri_csv(handle, c):
 
 # -------------------------------------------------------------------------- edge cases --
 
-@pytest.mark.parametrize("n", list(range(1, 33)) + [33, 40, 64, 100])
+@pytest.mark.parametrize("n", list(range(1, 33)) + [33, 40, 64, 100, 128, 129, 160, 300])
 def test_getrf_every_small_n_with_tail_and_padding(handle, n):
     """Every register-kernel size, a batch that is not a multiple of the per-CTA matrix count,
     lda > n with sentinel padding that must survive untouched."""
@@ -159,7 +159,7 @@ def test_getrf_every_small_n_with_tail_and_padding(handle, n):
     assert np.all(lu[:, :, n:] == 12345.0)
 
 
-@pytest.mark.parametrize("n", [1, 3, 8, 16, 31, 32, 48])
+@pytest.mark.parametrize("n", [1, 3, 8, 16, 31, 32, 48, 150])
 def test_singular_nan_and_zero_pivots(handle, n):
     """Zero columns (info, zeroed trailing pivots), a NaN entry (never chosen as pivot), and
     exact ties (lowest row wins), bit-exact against the oracle."""
