@@ -201,19 +201,22 @@ class Handle:
             self._ws = torch.empty(max(need, 32 << 20), dtype=torch.uint8, device=dev)
             check("aclblasSetWorkspace", lib().aclblasSetWorkspace(self.h, _vp(self._ws.data_ptr()),
                                                                    self._ws.numel()))
+        # the pointer arrays must stay referenced until the call has been enqueued: a temporary
+        # freed inside the argument list would hand its memory to the next one
+        pa, plu, pb, px = ptr_array(A), ptr_array(LU), ptr_array(B), ptr_array(X)
         check("aclblasSgetrfsRefineBatchedEx", lib().aclblasSgetrfsRefineBatchedEx(
-            self.h, n, nrhs, ptr_array(A).data_ptr(), n, ptr_array(LU).data_ptr(), n, piv.data_ptr(),
-            ptr_array(B).data_ptr(), n, ptr_array(X).data_ptr(), n, compute, max_iter, tol, berr.data_ptr(),
-            iters.data_ptr(), info.data_ptr(), batch))
+            self.h, n, nrhs, pa.data_ptr(), n, plu.data_ptr(), n, piv.data_ptr(), pb.data_ptr(), n, px.data_ptr(), n,
+            compute, max_iter, tol, berr.data_ptr(), iters.data_ptr(), info.data_ptr(), batch))
         return X, LU, piv, info, berr, iters
 
     def adjoint(self, LU, n, lda, piv, X, ldx, dX, lddx, dA=None, ldda=None):
         """dX <- A^{-T} dX (= dB); dA <- -dB X^T when dA is given (aclblasSgetrsAdjointBatched)."""
         nrhs = X.shape[1]
+        plu, px, pdx = ptr_array(LU), ptr_array(X), ptr_array(dX)
+        pda = None if dA is None else ptr_array(dA)
         check("aclblasSgetrsAdjointBatched", lib().aclblasSgetrsAdjointBatched(
-            self.h, n, nrhs, ptr_array(LU).data_ptr(), lda, _addr(piv), ptr_array(X).data_ptr(), ldx,
-            ptr_array(dX).data_ptr(), lddx, None if dA is None else ptr_array(dA).data_ptr(),
-            ldda if ldda is not None else n, LU.shape[0]))
+            self.h, n, nrhs, plu.data_ptr(), lda, _addr(piv), px.data_ptr(), ldx, pdx.data_ptr(), lddx,
+            None if pda is None else pda.data_ptr(), ldda if ldda is not None else n, LU.shape[0]))
 
     def getri(self, LU, n, lda, piv, Cinv, ldc, info=None, aptr=None, cptr=None):
         """Cinv = inverse from the LU factors; returns the info tensor."""

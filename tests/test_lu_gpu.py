@@ -188,7 +188,8 @@ def test_no_pivot_without_info(handle, n, ob):
     rng = np.random.default_rng(7)
     a = (rng.standard_normal((9, n, n)) + 4 * n * np.eye(n)).astype(np.float32)
     A = to_dev(a, "cuda")
-    st = ob.lib().aclblasSgetrfBatched(handle.h, n, ob.ptr_array(A).data_ptr(), n, None, None, 9)
+    aptr = ob.ptr_array(A)  # kept referenced until the launch is enqueued
+    st = ob.lib().aclblasSgetrfBatched(handle.h, n, aptr.data_ptr(), n, None, None, 9)
     assert st == ob.SUCCESS
     torch.cuda.synchronize()
     olu = a.copy()
