@@ -141,6 +141,26 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     aclblasComputeType_t computeType, int maxIter, double tol, double* berrArray, int* iterArray, int* infoArray,
     int batchCount);
 
+/* Bytes of device scratch that aclblasSgetrfsRefineBatchedStaticScratch can use. */
+#define ACLBLAS_REFINE_STATIC_SCRATCH_BYTES ((size_t)8 << 20)
+
+/* aclblasSgetrfsRefineBatchedEx without a workspace; no counterpart in the reference. For callers
+ * that cannot give the library device memory (the host application owns it all, or must not
+ * call cudaMalloc/cudaFree, which synchronise the device): the call allocates nothing and
+ * leaves the handle workspace alone. Its scratch is a fixed array of
+ * ACLBLAS_REFINE_STATIC_SCRATCH_BYTES in the library's device image, one per device; a call
+ * needs (n*nrhs*4 rounded up to 256 + 12) * batchCount + 512 bytes of it, and a larger request
+ * returns ACLBLAS_STATUS_INVALID_VALUE without launching anything. The first call on each device
+ * (with the handle's device current) sets up the scratch address; make it before any stream
+ * capture. The scratch is shared by all handles and streams of the process: calls that overlap
+ * in time on one device race on it; calls one after another on one stream are safe. Arguments,
+ * results and status codes are otherwise those of aclblasSgetrfsRefineBatchedEx. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
+    aclblasHandle_t handle, int n, int nrhs, const float* const Aarray[], int lda, float* const LUarray[], int ldlu,
+    int* PivotArray, const float* const Barray[], int ldb, float* const Xarray[], int ldx,
+    aclblasComputeType_t computeType, int maxIter, double tol, double* berrArray, int* iterArray, int* infoArray,
+    int batchCount);
+
 /* Adjoint of the batched solve X = A^{-1} B; no counterpart in the reference. With the LU
  * factors / pivots of aclblasSgetrfBatched, the solution X and the upstream gradient dX:
  * dX is overwritten by dB = A^{-T} dX (transposed solve on the stored factors) and, when

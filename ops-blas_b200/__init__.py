@@ -55,6 +55,9 @@ SIGNATURES = {
     "aclblasSgetrfsRefineBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp,
                                                 C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp,
                                                 _vp, C.c_int]),
+    "aclblasSgetrfsRefineBatchedStaticScratch": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp,
+                                                           _vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_double,
+                                                           _vp, _vp, _vp, C.c_int]),
     "aclblasSgetrsAdjointBatched": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp,
                                               C.c_int, _vp, C.c_int, C.c_int]),
 }

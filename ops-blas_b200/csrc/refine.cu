@@ -12,6 +12,8 @@
 // call can be captured in a CUDA graph. berrArray / iterArray / infoArray are device arrays.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "internal.h"
 
 namespace opsblas {
@@ -235,6 +237,161 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
         log_error(kApi, "n=%d exceeds the residual kernel's shared-memory limit", n);
         return ACLBLAS_STATUS_NOT_SUPPORTED;
     }
+    for (int it = 0; it < maxIter; it++) {
+        refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
+            n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, it, 0, done, berrArray, iterArray);
+        err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, dptr, n, batchCount);
+        if (err != cudaSuccess) return launch_status(kApi, err);
+        axpy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(n, nrhs, dptr, n, Xarray, ldx);
+    }
+    refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
+        n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, maxIter, 1, done, berrArray, iterArray);
+    return launch_status(kApi, cudaGetLastError());
+}
+
+// ----------------------------------------------------------------------------------------------
+// aclblasSgetrfsRefineBatchedStaticScratch: aclblasSgetrfsRefineBatchedEx with its scratch taken
+// from a fixed array in the library's device image instead of the handle workspace.
+//
+// Some callers cannot hand the library device memory: a plugin inside a host application that
+// owns every device allocation (a caching allocator with all memory reserved, or a hard memory
+// budget), or code that must not call cudaMalloc/cudaFree because those synchronise the device.
+// This entry point needs no workspace and allocates nothing. Its scratch (correction blocks D,
+// their pointer array, per-matrix convergence flags; the same layout as the workspace of
+// aclblasSgetrfsRefineBatchedEx) is kRefineStaticScratchBytes of static device memory; a request
+// that needs more is rejected with ACLBLAS_STATUS_INVALID_VALUE before anything is launched.
+//
+// Set-up: the first call on each device (with that device current) looks up the scratch address
+// with cudaGetSymbolAddress and sets the residual kernel's shared-memory limit; later calls reuse
+// the cached address. Make that first call before any stream capture.
+//
+// Only the convergence flags must start at zero; every call clears them on its stream before use,
+// so the scratch may hold anything a previous call left there. There is one scratch array per
+// device, shared by every handle and stream in the process: calls that overlap in time on the
+// same device (different streams, or different host threads) race on it and give wrong results.
+// Calls issued one after another on the same stream are safe.
+namespace opsblas {
+
+constexpr size_t kRefineStaticScratchBytes = ACLBLAS_REFINE_STATIC_SCRATCH_BYTES;
+constexpr int kStaticMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_refine_static_scratch[kRefineStaticScratchBytes];
+
+static std::mutex g_static_mu;
+static char* g_static_base[kStaticMaxDevices];  // per device ordinal, nullptr until set up
+
+// The scratch address on the current device; the first call per device does the set-up.
+static aclblasStatus_t static_scratch_base(const char* api, int device, char** base)
+{
+    if (device < 0 || device >= kStaticMaxDevices) {
+        log_error(api, "device ordinal %d is beyond the %d devices this entry point supports", device,
+                  kStaticMaxDevices);
+        return ACLBLAS_STATUS_NOT_SUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (g_static_base[device] == nullptr) {
+        void* p = nullptr;
+        cudaError_t err = cudaGetSymbolAddress(&p, g_refine_static_scratch);
+        if (err != cudaSuccess || p == nullptr) {
+            log_error(api, "cannot resolve the static scratch on device %d: %s", device, cudaGetErrorString(err));
+            return launch_status(api, err != cudaSuccess ? err : cudaErrorInvalidSymbol);
+        }
+        err = cudaFuncSetAttribute(refine_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (err != cudaSuccess) return launch_status(api, err);
+        g_static_base[device] = static_cast<char*>(p);
+    }
+    *base = g_static_base[device];
+    return ACLBLAS_STATUS_SUCCESS;
+}
+
+}  // namespace opsblas
+
+extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
+    aclblasHandle_t handle, int n, int nrhs, const float* const Aarray[], int lda, float* const LUarray[], int ldlu,
+    int* PivotArray, const float* const Barray[], int ldb, float* const Xarray[], int ldx,
+    aclblasComputeType_t computeType, int maxIter, double tol, double* berrArray, int* iterArray, int* infoArray,
+    int batchCount)
+{
+    static const char* kApi = "aclblasSgetrfsRefineBatchedStaticScratch";
+    if (handle == nullptr) {
+        log_error(kApi, "handle is nullptr");
+        return ACLBLAS_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (n < 0 || nrhs < 0 || batchCount < 0 || maxIter < 0 || !(tol >= 0.0)) {
+        log_error(kApi, "invalid size or control argument (n=%d nrhs=%d batch=%d maxIter=%d)", n, nrhs, batchCount,
+                  maxIter);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (lda < max1(n) || ldlu < max1(n) || ldb < max1(n) || ldx < max1(n)) {
+        log_error(kApi, "leading dimensions must be >= max(1, n)");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    int mode;
+    switch (computeType) {
+        case ACLBLAS_COMPUTE_32F: mode = 0; break;
+        case ACLBLAS_COMPUTE_32F_FAST_TF32: mode = 1; break;
+        case ACLBLAS_COMPUTE_32F_FAST_16BF: mode = 2; break;
+        default:
+            log_error(kApi, "computeType must be 32F, 32F_FAST_TF32 or 32F_FAST_16BF, got %d", (int)computeType);
+            return ACLBLAS_STATUS_NOT_SUPPORTED;
+    }
+    if (n == 0 || batchCount == 0) return ACLBLAS_STATUS_SUCCESS;
+    if (!Aarray || !LUarray || !PivotArray || !Barray || !Xarray || !berrArray || !iterArray || !infoArray) {
+        log_error(kApi, "array arguments must not be nullptr");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    // scratch: correction block D (n x nrhs per matrix, 256-byte rounded), its pointer array, flags
+    const size_t cap = kRefineStaticScratchBytes;
+    if ((size_t)n * (size_t)nrhs > cap / 4) {
+        log_error(kApi, "n*nrhs=%zu needs more than the %zu bytes of static scratch", (size_t)n * nrhs, cap);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    const size_t dbytes = ((size_t)n * nrhs * 4 + 255) / 256 * 256;
+    if ((size_t)batchCount > (cap - 512) / (dbytes + 12)) {
+        log_error(kApi,
+                  "scratch required %zu bytes, but the static scratch holds %zu; split the batch or use "
+                  "aclblasSgetrfsRefineBatchedEx with a workspace",
+                  (dbytes + 12) * (size_t)batchCount + 512, cap);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    const size_t rsm = (size_t)n * kResMaxRhs * 8;
+    if (rsm > 200 * 1024) {
+        log_error(kApi, "n=%d exceeds the residual kernel's shared-memory limit", n);
+        return ACLBLAS_STATUS_NOT_SUPPORTED;
+    }
+    int device = -1;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) return launch_status(kApi, err);
+    if (device != handle->device) {
+        log_error(kApi, "the handle belongs to device %d but device %d is current", handle->device, device);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    char* ws = nullptr;
+    aclblasStatus_t s = static_scratch_base(kApi, device, &ws);
+    if (s != ACLBLAS_STATUS_SUCCESS) return s;
+
+    float* dbase = reinterpret_cast<float*>(ws);
+    float** dptr = reinterpret_cast<float**>(ws + dbytes * batchCount);
+    int* done = reinterpret_cast<int*>(reinterpret_cast<char*>(dptr) + (size_t)batchCount * 8);
+    cudaStream_t st = handle->stream;
+    const unsigned bgrid = (unsigned)((batchCount + 255) / 256 < 4096 ? (batchCount + 255) / 256 : 4096);
+
+    init_ptr_array_kernel<<<bgrid, 256, 0, st>>>(dptr, dbase, (long long)(dbytes / 4), batchCount);
+    fill_int_kernel<<<bgrid, 256, 0, st>>>(done, 0, batchCount);
+    fill_int_kernel<<<bgrid, 256, 0, st>>>(iterArray, maxIter, batchCount);
+    copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
+    err = cudaGetLastError();
+    if (err != cudaSuccess) return launch_status(kApi, err);
+    if (n > 32 && getrf_large_supported(n) && (mode != 0 || n > 128)) {
+        err = getrf_large_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
+    } else {
+        s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
+        if (s != ACLBLAS_STATUS_SUCCESS) return s;
+    }
+    if (err != cudaSuccess || nrhs == 0) return launch_status(kApi, err);
+    copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Barray, ldb, Xarray, ldx, n, nrhs);
+    err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, Xarray, ldx, batchCount);
+    if (err != cudaSuccess) return launch_status(kApi, err);
     for (int it = 0; it < maxIter; it++) {
         refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
             n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, it, 0, done, berrArray, iterArray);
