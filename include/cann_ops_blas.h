@@ -170,6 +170,36 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrsAdjointBatched(
     const float* const Xarray[], int ldx, float* const dXarray[], int lddx, float* const dAarray[], int ldda,
     int batchCount);
 
+/* Grouped factor + solve of matrices of different orders; no counterpart in the reference.
+ * A plan describes groupCount groups (host arrays): group g has groupSizeArray[g] instances of
+ * order nArray[g], nrhsArray[g] right-hand sides (0: factor only), leading dimensions
+ * ldaArray[g] / ldbArray[g]. Instances are numbered group by group. configArray is NULL or holds
+ * 3 ints per group {lanes per matrix (n <= 32: 4/8/16/32), warps per matrix (n > 32: 2 or 4),
+ * panel width (n > 32: 8 or 16)}, 0 = take the tuning table's choice; the table is the file
+ * named by OPSBLAS_GROUPED_TUNING, else grouped_tuning.txt beside the library, else built-in
+ * defaults. Invalid choices are replaced; aclblasSgetrfGetrsGroupedPlanGetConfig returns the
+ * ones in use. Creating a plan allocates and uploads its task lists (synchronously). */
+typedef struct _aclblas_grouped_plan* aclblasGroupedPlan_t;
+
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(
+    aclblasHandle_t handle, int groupCount, const int nArray[], const int nrhsArray[], const int ldaArray[],
+    const int ldbArray[], const int groupSizeArray[], const int* configArray, aclblasGroupedPlan_t* plan);
+
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfGetrsGroupedPlanGetConfig(aclblasGroupedPlan_t plan, int* configArray);
+
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfGetrsGroupedPlanDestroy(aclblasGroupedPlan_t plan);
+
+/* Executes a plan on the handle's stream: for every instance i, Aarray[i] is factored in place
+ * (P*A = L*U, pivots at PivotArray + sum of the orders of the instances before i, infoArray[i]
+ * as aclblasSgetrfBatched) and Barray[i] (n x nrhs) is overwritten by the solution X of A X = B
+ * (as aclblasSgetrsBatched with trans N); the results equal those two calls bit for bit.
+ * Instances with n <= 128 run in one persistent launch; larger ones use the batched kernels.
+ * No allocation and no host synchronisation. Executions of one plan must not overlap in time
+ * (they share the plan's work counters). */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfGetrsGroupedBatched(
+    aclblasHandle_t handle, aclblasGroupedPlan_t plan, float* const Aarray[], int* PivotArray, int* infoArray,
+    float* const Barray[]);
+
 #ifdef __cplusplus
 }
 #endif

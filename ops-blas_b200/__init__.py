@@ -58,6 +58,11 @@ SIGNATURES = {
     "aclblasSgetrfsRefineBatchedStaticScratch": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp,
                                                            _vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_double,
                                                            _vp, _vp, _vp, C.c_int]),
+    "aclblasSgetrfGetrsGroupedPlanCreate": (C.c_int, [_vp, C.c_int, _ip, _ip, _ip, _ip, _ip, _ip,
+                                                      C.POINTER(_vp)]),
+    "aclblasSgetrfGetrsGroupedPlanGetConfig": (C.c_int, [_vp, _ip]),
+    "aclblasSgetrfGetrsGroupedPlanDestroy": (C.c_int, [_vp]),
+    "aclblasSgetrfGetrsGroupedBatched": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "aclblasSgetrsAdjointBatched": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp,
                                               C.c_int, _vp, C.c_int, C.c_int]),
 }
@@ -231,6 +236,97 @@ class Handle:
         check("aclblasSgetriBatched", lib().aclblasSgetriBatched(
             self.h, n, aptr.data_ptr(), lda, _addr(piv), cptr.data_ptr(), ldc, info.data_ptr(), LU.shape[0]))
         return info
+
+
+# ------------------------------------------------------------------- grouped factor+solve --
+
+def _int_array(vals):
+    vals = [int(v) for v in vals]
+    return (C.c_int * max(len(vals), 1))(*vals)
+
+
+class GroupedPlan:
+    """aclblasGroupedPlan_t for groups of instances sharing (n, nrhs, lda, ldb).
+
+    ``ns``, ``nrhss``, ``sizes`` (and optionally ``ldas``, ``ldbs``, default n) are per group;
+    ``config`` is None or one (lanes, warps, panel) triple per group, 0 = the tuning table's
+    choice. Instances are numbered group by group."""
+
+    def __init__(self, handle, ns, nrhss, sizes, ldas=None, ldbs=None, config=None):
+        self.ns = [int(v) for v in ns]
+        self.nrhss = [int(v) for v in nrhss]
+        self.sizes = [int(v) for v in sizes]
+        self.ldas = [max(1, v) for v in self.ns] if ldas is None else [int(v) for v in ldas]
+        self.ldbs = [max(1, v) for v in self.ns] if ldbs is None else [int(v) for v in ldbs]
+        cfg = None if config is None else _int_array([x for t in config for x in t])
+        self.p = _vp()
+        check("aclblasSgetrfGetrsGroupedPlanCreate", lib().aclblasSgetrfGetrsGroupedPlanCreate(
+            handle.h, len(self.ns), _int_array(self.ns), _int_array(self.nrhss), _int_array(self.ldas),
+            _int_array(self.ldbs), _int_array(self.sizes), cfg, C.byref(self.p)))
+
+    def config(self):
+        out = (C.c_int * max(3 * len(self.ns), 1))()
+        check("aclblasSgetrfGetrsGroupedPlanGetConfig", lib().aclblasSgetrfGetrsGroupedPlanGetConfig(self.p, out))
+        return [tuple(out[3 * g:3 * g + 3]) for g in range(len(self.ns))]
+
+    def run(self, handle, aptr, piv, info, bptr=None):
+        """Executes the plan: aptr / bptr are device pointer arrays (int64 tensors) in instance
+        order, piv the concatenated pivots, info one int per instance."""
+        check("aclblasSgetrfGetrsGroupedBatched", lib().aclblasSgetrfGetrsGroupedBatched(
+            handle.h, self.p, aptr.data_ptr(), piv.data_ptr(), info.data_ptr(),
+            None if bptr is None else bptr.data_ptr()))
+
+    def close(self):
+        if self.p:
+            check("aclblasSgetrfGetrsGroupedPlanDestroy", lib().aclblasSgetrfGetrsGroupedPlanDestroy(self.p))
+            self.p = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def grouped_offsets(ns, cols, lds, sizes, align=64):
+    """Offsets (in floats) of the instances of a grouped batch packed in one slab: instance i of
+    group g takes lds[g] * cols[g] floats, each starting on an ``align``-float boundary.
+    Returns (offsets list, total floats)."""
+    offs, cur = [], 0
+    for n, c, ld, sz in zip(ns, cols, lds, sizes):
+        span = ld * c
+        for _ in range(sz):
+            offs.append(cur)
+            cur += (span + align - 1) // align * align
+    return offs, max(cur, 1)
+
+
+def slab_ptrs(slab, offsets):
+    """Device int64 tensor of slab.data_ptr() + 4 * offset for each offset."""
+    torch = _torch()
+    off = torch.tensor(offsets, dtype=torch.int64, device=slab.device)
+    return (off * slab.element_size() + slab.data_ptr()).contiguous()
+
+
+def grouped_plain(handle, ns, nrhss, sizes, ldas, ldbs, aptr, piv, info, bptr=None):
+    """The same work as GroupedPlan.run through the plain entry points: per group one
+    aclblasSgetrfBatched and one aclblasSgetrsBatched (trans N) on the group's slice of the
+    pointer arrays. This is the plain FP32 path the grouped launch is compared with."""
+    L = lib()
+    first = poff = 0
+    info_h = C.c_int(0)
+    for n, nrhs, sz, lda, ldb in zip(ns, nrhss, sizes, ldas, ldbs):
+        if sz > 0 and n > 0:
+            a = aptr.data_ptr() + 8 * first
+            p = piv.data_ptr() + 4 * poff
+            check("aclblasSgetrfBatched", L.aclblasSgetrfBatched(handle.h, n, a, lda, p, info.data_ptr() + 4 * first,
+                                                                 sz))
+            if nrhs > 0:
+                check("aclblasSgetrsBatched", L.aclblasSgetrsBatched(handle.h, OP_N, n, nrhs, a, lda, p,
+                                                                     bptr.data_ptr() + 8 * first, ldb,
+                                                                     C.byref(info_h), sz))
+        first += sz
+        poff += n * sz
 
 
 # ------------------------------------------------------------------ differentiable solve --

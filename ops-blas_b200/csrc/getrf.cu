@@ -13,54 +13,16 @@
 #include <cuda_runtime.h>
 
 #include "internal.h"
+#include "lu_core.cuh"
 #include "small_common.cuh"
 
 namespace opsblas {
 
 // ---------------------------------------------------------------------------------------
-// n <= 32. Lane r of a segment holds row r of its matrix in registers a[0..n-1].
-// Pivoting is implicit: rows never move between lanes during the factorisation; `pos` is
-// the row index the lane's row currently has in the reference's in-place matrix, and rows
-// are stored at `pos` at the end. Per column k:
-//   1. argmax of |a[k]| over lanes with pos >= k (redux.sync), ties to the lowest pos --
-//      identical to the reference's first-maximum rule, zero/NaN never chosen;
-//   2. the pivot lane publishes its row (from column k on) in shared memory; every lane
-//      reads it back with broadcast 16-byte loads;
-//   3. lanes below the pivot form l = a[k] / pivot and update a[j] -= l * u[j], j > k.
-// Arithmetic per element is the reference's, in its order, one fmaf per update.
+// n <= 32: one warp segment per matrix, rows in registers (small_getrf_core, lu_core.cuh).
+// The lane of row r loads it with coalesced column-wise loads and stores it at its final
+// position.
 // ---------------------------------------------------------------------------------------
-template <int N>
-__device__ __forceinline__ float qget(const float4 (&v)[(N + 3) / 4], int j)
-{
-    return f4get(v[j >> 2], j & 3);
-}
-
-template <int N>
-__device__ __forceinline__ void qset(float4 (&v)[(N + 3) / 4], int j, float x)
-{
-    float4& c = v[j >> 2];
-    if ((j & 3) == 0) c.x = x;
-    else if ((j & 3) == 1) c.y = x;
-    else if ((j & 3) == 2) c.z = x;
-    else c.w = x;
-}
-
-// a[j] -= l * u[j] on the pairs (x, y) / (z, w) of a float4 chunk, one packed fma per pair;
-// fma(u, -l, a) == fma(-l, u, a) exactly.
-__device__ __forceinline__ void ffma2_lo(float4& a, float ux, float uy, float2 nl)
-{
-    const float2 r = __ffma2_rn(make_float2(ux, uy), nl, make_float2(a.x, a.y));
-    a.x = r.x;
-    a.y = r.y;
-}
-
-__device__ __forceinline__ void ffma2_hi(float4& a, float uz, float uw, float2 nl)
-{
-    const float2 r = __ffma2_rn(make_float2(uz, uw), nl, make_float2(a.z, a.w));
-    a.z = r.x;
-    a.w = r.y;
-}
-
 template <int N, bool PIVOT>
 __global__ void __launch_bounds__(kSmallWarps * 32, N > 16 ? 4 : (N > 8 ? 5 : 6))
 getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__ piv, int* __restrict__ info,
@@ -68,7 +30,6 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
 {
     using S = SmallShape<N>;
     constexpr int NC = S::NC;
-    constexpr bool UNIFORM = S::MPW == 1;  // one matrix per warp: segment state is warp-uniform
     __shared__ __align__(16) float rowbuf[kSmallWarps][2][32];
 
     const int lane = threadIdx.x & 31;
@@ -91,70 +52,8 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
         for (int j = 0; j < N; j++) qset<N>(a4, j, Ar[(long long)j * lda]);
     }
 
-    int pos = r;
-    int mypiv = 0;
-    int inf = 0;  // uniform within a segment
-#pragma unroll
-    for (int k = 0; k < N; k++) {
-        float* buf = &rowbuf[warp][k & 1][seg * S::SEG];
-        const bool live = UNIFORM ? rvalid : (rvalid && inf == 0);
-        const float ak = qget<N>(a4, k);
-        int prow = k;
-        bool ispiv;
-        if (PIVOT) {
-            const bool elig = live && pos >= k;
-            const float v = fabsf(ak);
-            const unsigned key = (elig && v > 0.0f) ? __float_as_uint(v) : 0u;
-            prow = (int)seg_argmax<S::SEG>(key, elig ? (unsigned)pos : 0xffffffffu, seg);
-            ispiv = elig && pos == prow;
-        } else {
-            ispiv = live && pos == k;
-        }
-        if (ispiv) {
-#pragma unroll
-            for (int c = k / 4; c < NC; c++) reinterpret_cast<float4*>(buf)[c] = a4[c];
-        }
-        __syncwarp();
-        const float4 ck = reinterpret_cast<const float4*>(buf)[k / 4];
-        const float pv = f4get(ck, k % 4);
-        if (UNIFORM) {
-            if (PIVOT && r == k) mypiv = prow + 1;
-            if (pv == 0.0f) {  // warp-uniform: every lane read the same pivot
-                inf = k + 1;
-                break;
-            }
-        } else if (mvalid && inf == 0) {
-            if (PIVOT && r == k) mypiv = prow + 1;
-            if (pv == 0.0f) inf = k + 1;
-        }
-        if (UNIFORM ? live : (live && inf == 0)) {
-            if (ispiv)
-                pos = k;
-            else if (pos == k)
-                pos = prow;
-            if (pos > k) {
-                // Multiplier by true division, then a[j] -= l * u[j] for j > k, one fma each.
-                const float l = ak / pv;
-                qset<N>(a4, k, l);
-                const float2 nl = make_float2(-l, -l);
-#pragma unroll
-                for (int c = k / 4; c < NC; c++) {
-                    const float4 u = (c == k / 4) ? ck : reinterpret_cast<const float4*>(buf)[c];
-                    // columns 4c..4c+3 that lie right of k
-                    if (4 * c > k) {
-                        ffma2_lo(a4[c], u.x, u.y, nl);
-                    } else if (4 * c + 1 > k) {
-                        a4[c].y = fmaf(-l, u.y, a4[c].y);
-                    }
-                    if (4 * c + 2 > k && 4 * c + 2 < N) {
-                        ffma2_hi(a4[c], u.z, u.w, nl);
-                    } else if (4 * c + 3 > k && 4 * c + 3 < N) {
-                        a4[c].w = fmaf(-l, u.w, a4[c].w);
-                    }
-                }
-            }
-        }
-    }
+    int pos, mypiv, inf;
+    small_getrf_core<N, PIVOT, S::SEG>(a4, pos, mypiv, inf, &rowbuf[warp][0][0], seg, r, mvalid, rvalid);
 
     if (rvalid) {
         float* Ap = A + pos;

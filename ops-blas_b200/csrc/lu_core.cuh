@@ -1,0 +1,448 @@
+// LU building blocks shared by the batched kernels (getrf.cu, getrf_medium.cu) and the grouped
+// persistent kernel (grouped.cu). Each block restates the reference's unblocked right-looking
+// LU (sgetrf_batched_kernel.cpp:106-150): first-maximum pivot, whole-row interchange,
+// multipliers by true division, one fmaf per update in column order, stop at the first
+// exactly-zero pivot. Whatever kernel runs them, the factors are the same bits.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "small_common.cuh"
+
+namespace opsblas {
+
+// =============================================================================================
+// Register LU for n <= 32: one warp segment per matrix (SEG lanes, 32/SEG matrices per warp).
+// Lane r of a segment holds row r of its matrix in registers a4 (float4 chunks, zero padded).
+// Pivoting is implicit: rows never move between lanes; `pos` is the row index the lane's row
+// has in the reference's in-place matrix at the current step. Per column k:
+//   1. argmax of |a[k]| over lanes with pos >= k (redux.sync), ties to the lowest pos --
+//      the reference's first-maximum rule; zero and NaN are never chosen;
+//   2. the pivot lane publishes its row (from column k on) in shared memory; every lane
+//      reads it back with broadcast 16-byte loads;
+//   3. lanes below the pivot form l = a[k] / pivot and update a[j] -= l * u[j], j > k.
+// =============================================================================================
+template <int N>
+__device__ __forceinline__ float qget(const float4 (&v)[(N + 3) / 4], int j)
+{
+    return f4get(v[j >> 2], j & 3);
+}
+
+template <int N>
+__device__ __forceinline__ void qset(float4 (&v)[(N + 3) / 4], int j, float x)
+{
+    float4& c = v[j >> 2];
+    if ((j & 3) == 0) c.x = x;
+    else if ((j & 3) == 1) c.y = x;
+    else if ((j & 3) == 2) c.z = x;
+    else c.w = x;
+}
+
+// a[j] -= l * u[j] on the pairs (x, y) / (z, w) of a float4 chunk, one packed fma per pair;
+// fma(u, -l, a) == fma(-l, u, a) exactly.
+__device__ __forceinline__ void ffma2_lo(float4& a, float ux, float uy, float2 nl)
+{
+    const float2 r = __ffma2_rn(make_float2(ux, uy), nl, make_float2(a.x, a.y));
+    a.x = r.x;
+    a.y = r.y;
+}
+
+__device__ __forceinline__ void ffma2_hi(float4& a, float uz, float uw, float2 nl)
+{
+    const float2 r = __ffma2_rn(make_float2(uz, uw), nl, make_float2(a.z, a.w));
+    a.z = r.x;
+    a.w = r.y;
+}
+
+// Factors the segment's matrix held in a4. rowbuf: this warp's 2 x 32 floats of shared memory
+// (16-byte aligned). On return: pos = the lane row's final row index, mypiv = 1-based pivot of
+// column r (0 when r >= info), inf = info (uniform within the segment).
+template <int N, bool PIVOT, int SEG>
+__device__ __forceinline__ void small_getrf_core(float4 (&a4)[(N + 3) / 4], int& pos, int& mypiv, int& inf,
+                                                 float* rowbuf, int seg, int r, bool mvalid, bool rvalid)
+{
+    constexpr int NC = (N + 3) / 4;
+    constexpr bool UNIFORM = SEG == 32;  // one matrix per warp: segment state is warp-uniform
+    pos = r;
+    mypiv = 0;
+    inf = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        float* buf = rowbuf + (k & 1) * 32 + seg * SEG;
+        const bool live = UNIFORM ? rvalid : (rvalid && inf == 0);
+        const float ak = qget<N>(a4, k);
+        int prow = k;
+        bool ispiv;
+        if (PIVOT) {
+            const bool elig = live && pos >= k;
+            const float v = fabsf(ak);
+            const unsigned key = (elig && v > 0.0f) ? __float_as_uint(v) : 0u;
+            prow = (int)seg_argmax<SEG>(key, elig ? (unsigned)pos : 0xffffffffu, seg);
+            ispiv = elig && pos == prow;
+        } else {
+            ispiv = live && pos == k;
+        }
+        if (ispiv) {
+#pragma unroll
+            for (int c = k / 4; c < NC; c++) reinterpret_cast<float4*>(buf)[c] = a4[c];
+        }
+        __syncwarp();
+        const float4 ck = reinterpret_cast<const float4*>(buf)[k / 4];
+        const float pv = f4get(ck, k % 4);
+        if (UNIFORM) {
+            if (PIVOT && r == k) mypiv = prow + 1;
+            if (pv == 0.0f) {  // warp-uniform: every lane read the same pivot
+                inf = k + 1;
+                break;
+            }
+        } else if (mvalid && inf == 0) {
+            if (PIVOT && r == k) mypiv = prow + 1;
+            if (pv == 0.0f) inf = k + 1;
+        }
+        if (UNIFORM ? live : (live && inf == 0)) {
+            if (ispiv)
+                pos = k;
+            else if (pos == k)
+                pos = prow;
+            if (pos > k) {
+                // Multiplier by true division, then a[j] -= l * u[j] for j > k, one fma each.
+                const float l = ak / pv;
+                qset<N>(a4, k, l);
+                const float2 nl = make_float2(-l, -l);
+#pragma unroll
+                for (int c = k / 4; c < NC; c++) {
+                    const float4 u = (c == k / 4) ? ck : reinterpret_cast<const float4*>(buf)[c];
+                    // columns 4c..4c+3 that lie right of k
+                    if (4 * c > k) {
+                        ffma2_lo(a4[c], u.x, u.y, nl);
+                    } else if (4 * c + 1 > k) {
+                        a4[c].y = fmaf(-l, u.y, a4[c].y);
+                    }
+                    if (4 * c + 2 > k && 4 * c + 2 < N) {
+                        ffma2_hi(a4[c], u.z, u.w, nl);
+                    } else if (4 * c + 3 > k && 4 * c + 3 < N) {
+                        a4[c].w = fmaf(-l, u.w, a4[c].w);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// Solves one right-hand side with the factors left in registers by small_getrf_core, in the
+// reference getrs's order (sgetrs_batched_kernel.cpp:83-200, trans N): b permuted by the row
+// interchanges, unit-L forward sweep j = 0..n-1, U backward sweep j = n-1..0 with x_j = y_j /
+// U(j,j), one fmaf per update. The lane of original row r enters with y = b[r] (b[r] sits at
+// position pos after the interchanges) and leaves with y = x[pos]. owner: this segment's SEG
+// ints of shared memory, filled here with the lane of each position. All 32 lanes call this.
+template <int N, int SEG>
+__device__ __forceinline__ float small_solve_core(const float4 (&a4)[(N + 3) / 4], int pos, bool rvalid, int seg,
+                                                  int r, int* owner, float y)
+{
+    if (rvalid) owner[pos] = r;
+    __syncwarp();
+    const int base = seg * SEG;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const float yk = __shfl_sync(0xffffffffu, y, base + owner[k]);
+        if (rvalid && pos > k) y = fmaf(-qget<N>(a4, k), yk, y);
+    }
+#pragma unroll
+    for (int k = N - 1; k >= 0; k--) {
+        const float t = (rvalid && pos == k) ? y / qget<N>(a4, k) : 0.0f;
+        const float xk = __shfl_sync(0xffffffffu, t, base + owner[k]);
+        if (rvalid) {
+            if (pos == k)
+                y = xk;
+            else if (pos < k)
+                y = fmaf(-qget<N>(a4, k), xk, y);
+        }
+    }
+    __syncwarp();
+    return y;
+}
+
+// =============================================================================================
+// Blocked LU of one matrix resident in shared memory (32 < n <= 128), run by a team of NT
+// threads (NT = 64 or 128; the team's first warp factors the panels). The reference's arithmetic
+// reorganised into panels of PB columns:
+//   1. panel: warp 0 factors columns k0..k0+PB-1 of the rows k0..n-1, up to 4 rows per lane
+//      in registers, first-maximum pivots by redux.sync, multipliers by division;
+//   2. U12: rows k0..k0+PB-1 right of the panel, forward substitution with the panel's unit
+//      L11 in order m = 0..PB-1 (what the reference's rank-1 updates do to those rows);
+//   3. A22 -= L21 * U12 with 4x4 register tiles whose accumulators start from A22 and add
+//      the PB products in order -- one fmaf per product, exactly the reference sequence.
+// Every element receives the same products in the same order for any PB, so PB and NT are free
+// tuning choices. Rows never move in shared memory: pivoting only updates a logical-to-physical
+// row map. On an exactly-zero pivot at column k the panel's columns before k are still applied
+// to the trailing columns (steps 2-3 with a narrower panel), so a singular matrix ends in the
+// reference's state too.
+// =============================================================================================
+constexpr int kMedMaxN = 128;
+constexpr int kMedRows = kMedMaxN / 32;  // panel rows per lane
+
+struct MedLayout {
+    int ld;       // column stride of the resident matrix (odd: conflict-free row access)
+    int ls_ld;    // row stride of the staged L21 / U12 blocks (multiple of 4)
+    int mat;      // floats reserved for the matrix (multiple of 4: 16-byte aligned staging)
+    size_t bytes;
+    __host__ __device__ MedLayout(int n, int pb)
+    {
+        ld = n | 1;
+        ls_ld = (n + 3) & ~3;
+        mat = (ld * n + 3) & ~3;
+        bytes = (size_t)mat * 4               // matrix
+                + (size_t)2 * pb * ls_ld * 4  // staged L21 (transposed) and U12
+                + (size_t)n * 4               // row map
+                + (size_t)2 * 32 * 4          // pivot row broadcast (double buffered)
+                + 64;                         // scalars
+        bytes = (bytes + 15) & ~(size_t)15;
+    }
+};
+
+// Views of a team's shared-memory region laid out by MedLayout.
+struct MedSmem {
+    float* sa;    // resident matrix, column-major, ld
+    float* l21;   // [PB][lsd]: l21[m*lsd + i'] = L(r0+i', k0+m)
+    float* u12;   // [PB][lsd]: u12[m*lsd + j'] = U(k0+m, j0+j')
+    int* rmap;    // logical row -> physical row
+    float* prow;  // 2 x 32 floats
+    int* sc;      // scalars: [0] info, [1] panel columns applied
+    __device__ MedSmem(float* base, const MedLayout& L, int n, int pb)
+    {
+        sa = base;
+        l21 = sa + L.mat;
+        u12 = l21 + pb * L.ls_ld;
+        rmap = reinterpret_cast<int*>(u12 + pb * L.ls_ld);
+        prow = reinterpret_cast<float*>(rmap + n);
+        sc = reinterpret_cast<int*>(prow + 64);
+    }
+};
+
+// Barrier over the team: bar < 0 means the team is the whole CTA.
+template <int NT>
+__device__ __forceinline__ void team_sync(int bar)
+{
+    if (bar < 0)
+        __syncthreads();
+    else
+        asm volatile("bar.sync %0, %1;\n" ::"r"(bar), "n"(NT) : "memory");
+}
+
+// Factors the matrix in S.sa (loaded by the caller, rmap = identity, sc[0] = 0, pm zeroed when
+// pivoting). Returns info. tid is the thread's index within the team.
+template <bool PIVOT, int NT, int PB>
+__device__ __forceinline__ int med_getrf_core(const MedSmem& S, int n, int ld, int lsd, int* pm, int tid, int bar)
+{
+    float* sa = S.sa;
+    float* l21 = S.l21;
+    float* u12 = S.u12;
+    int* rmap = S.rmap;
+    float* prow = S.prow;
+    int* sc = S.sc;
+    const int lane = tid & 31, warp = tid >> 5;
+
+    for (int k0 = 0; k0 < n; k0 += PB) {
+        const int pb = min(PB, n - k0);
+        // ---------------------------------------------------------------- 1. panel --
+        if (warp == 0) {
+            float pr[kMedRows][PB];
+            int pos[kMedRows], phys[kMedRows];
+#pragma unroll
+            for (int t = 0; t < kMedRows; t++) {
+                const int i = k0 + lane + 32 * t;
+                pos[t] = i;
+                phys[t] = i < n ? rmap[i] : 0;
+#pragma unroll
+                for (int c = 0; c < PB; c++) pr[t][c] = (i < n && c < pb) ? sa[phys[t] + (k0 + c) * ld] : 0.0f;
+            }
+            int done = pb;
+            int inf = 0;
+#pragma unroll
+            for (int c = 0; c < PB; c++) {
+                if (c >= pb) break;
+                const int k = k0 + c;
+                float* buf = prow + 32 * (c & 1);
+                int ppos = k;
+                if (PIVOT) {
+                    // lane-local first maximum (ties to the lowest logical row), then warp-wide
+                    unsigned bkey = 0, bpos = 0xffffffffu;
+#pragma unroll
+                    for (int t = 0; t < kMedRows; t++) {
+                        const bool elig = pos[t] < n && pos[t] >= k;
+                        const float v = fabsf(pr[t][c]);
+                        const unsigned key = (elig && v > 0.0f) ? __float_as_uint(v) : 0u;
+                        if (elig && (key > bkey || (key == bkey && (unsigned)pos[t] < bpos))) {
+                            bkey = key;
+                            bpos = (unsigned)pos[t];
+                        }
+                    }
+                    ppos = (int)seg_argmax<32>(bkey, bpos, 0);
+                }
+                // the pivot row's owner publishes it
+#pragma unroll
+                for (int t = 0; t < kMedRows; t++) {
+                    if (pos[t] == ppos) {
+#pragma unroll
+                        for (int cc = 0; cc < PB; cc++) buf[cc] = pr[t][cc];
+                    }
+                }
+                __syncwarp();
+                const float pv = buf[c];
+                if (PIVOT && lane == 0) pm[k] = ppos + 1;
+                if (pv == 0.0f) {
+                    inf = k + 1;
+                    done = c;
+                    break;
+                }
+#pragma unroll
+                for (int t = 0; t < kMedRows; t++) {
+                    if (pos[t] == ppos)
+                        pos[t] = k;
+                    else if (pos[t] == k)
+                        pos[t] = ppos;
+                }
+#pragma unroll
+                for (int t = 0; t < kMedRows; t++) {
+                    if (pos[t] < n && pos[t] > k) {
+                        const float l = pr[t][c] / pv;
+                        pr[t][c] = l;
+#pragma unroll
+                        for (int cc = c + 1; cc < PB; cc++) pr[t][cc] = fmaf(-l, buf[cc], pr[t][cc]);
+                    }
+                }
+            }
+            // write the panel back in place, record the new logical order
+#pragma unroll
+            for (int t = 0; t < kMedRows; t++) {
+                if (k0 + lane + 32 * t < n) {
+#pragma unroll
+                    for (int c = 0; c < PB; c++)
+                        if (c < pb) sa[phys[t] + (k0 + c) * ld] = pr[t][c];
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < kMedRows; t++)
+                if (k0 + lane + 32 * t < n) rmap[pos[t]] = phys[t];
+            if (lane == 0) {
+                sc[0] = inf;
+                sc[1] = done;
+            }
+        }
+        team_sync<NT>(bar);
+        const int w = sc[1];     // panel columns to apply (pb, or fewer after a zero pivot)
+        const int j0 = k0 + pb;  // first column right of the panel
+        const int r0 = k0 + w;   // first row of the trailing block
+        const int rest = n - j0;
+        if (w > 0 && rest > 0) {
+            // ------------------------------------------------ 2. U12 (+ staging) --
+            for (int jj = tid; jj < rest; jj += NT) {
+                const int j = j0 + jj;
+                float u[PB];
+#pragma unroll
+                for (int r = 0; r < PB; r++) u[r] = r < w ? sa[rmap[k0 + r] + j * ld] : 0.0f;
+#pragma unroll
+                for (int mm = 0; mm < PB; mm++) {
+                    if (mm < w) {
+#pragma unroll
+                        for (int r = mm + 1; r < PB; r++)
+                            if (r < w) u[r] = fmaf(-sa[rmap[k0 + r] + (k0 + mm) * ld], u[mm], u[r]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < PB; r++) {
+                    if (r < w) {
+                        sa[rmap[k0 + r] + j * ld] = u[r];
+                        u12[r * lsd + jj] = u[r];
+                    }
+                }
+            }
+            const int rows = n - r0;  // rows below the applied panel columns
+            for (int e = tid; e < rows * w; e += NT) {
+                const int ii = e % rows, mm = e / rows;
+                l21[mm * lsd + ii] = sa[rmap[r0 + ii] + (k0 + mm) * ld];
+            }
+            team_sync<NT>(bar);
+            // ------------------------------------------- 3. A22 -= L21 * U12 --
+            const int tr = (rows + 3) / 4, tc = (rest + 3) / 4;
+            for (int tile = tid; tile < tr * tc; tile += NT) {
+                const int bi = (tile % tr) * 4, bj = (tile / tr) * 4;
+                float acc[4][4];
+                int pr4[4];
+#pragma unroll
+                for (int a = 0; a < 4; a++) pr4[a] = (bi + a < rows) ? rmap[r0 + bi + a] : -1;
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        acc[a][b] = (pr4[a] >= 0 && bj + b < rest) ? sa[pr4[a] + (j0 + bj + b) * ld] : 0.0f;
+                for (int mm = 0; mm < w; mm++) {
+                    const float4 lv = *reinterpret_cast<const float4*>(l21 + mm * lsd + bi);
+                    const float4 uv = *reinterpret_cast<const float4*>(u12 + mm * lsd + bj);
+                    const float la[4] = {-lv.x, -lv.y, -lv.z, -lv.w};
+                    const float ub[4] = {uv.x, uv.y, uv.z, uv.w};
+#pragma unroll
+                    for (int a = 0; a < 4; a++)
+#pragma unroll
+                        for (int b = 0; b < 4; b++) acc[a][b] = fmaf(la[a], ub[b], acc[a][b]);
+                }
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int b = 0; b < 4; b++)
+                        if (pr4[a] >= 0 && bj + b < rest) sa[pr4[a] + (j0 + bj + b) * ld] = acc[a][b];
+            }
+        }
+        team_sync<NT>(bar);
+        if (sc[0] != 0) break;
+    }
+    return sc[0];
+}
+
+// Solves right-hand-side column y (n values, logical order after the interchanges: the lane's
+// rows i = lane + 32 t enter with y[t] = b[rmap[i]]) with the factors in S, in the reference
+// getrs's order (trans N): unit-L forward sweep, then U backward sweep with x_j = y_j / U(j,j).
+// Run by one warp; y[t] leaves as x[lane + 32 t].
+__device__ __forceinline__ void med_solve_core(const MedSmem& S, int n, int ld, int lane, float (&y)[kMedRows])
+{
+    const float* sa = S.sa;
+    const int* rmap = S.rmap;
+    int ph[kMedRows];
+#pragma unroll
+    for (int t = 0; t < kMedRows; t++) ph[t] = (lane + 32 * t < n) ? rmap[lane + 32 * t] : 0;
+#pragma unroll
+    for (int kq = 0; kq < kMedRows; kq++) {
+        for (int kl = 0; kl < 32; kl++) {
+            const int k = kq * 32 + kl;
+            if (k >= n) break;
+            const float yk = __shfl_sync(0xffffffffu, y[kq], kl);
+#pragma unroll
+            for (int t = 0; t < kMedRows; t++) {
+                const int i = lane + 32 * t;
+                if (t >= kq && i > k && i < n) y[t] = fmaf(-sa[ph[t] + k * ld], yk, y[t]);
+            }
+        }
+    }
+#pragma unroll
+    for (int kq = kMedRows - 1; kq >= 0; kq--) {
+        for (int kl = 31; kl >= 0; kl--) {
+            const int k = kq * 32 + kl;
+            if (k >= n) continue;
+            const float t0 = (lane == kl) ? y[kq] / sa[ph[kq] + k * ld] : 0.0f;
+            const float xk = __shfl_sync(0xffffffffu, t0, kl);
+#pragma unroll
+            for (int t = 0; t < kMedRows; t++) {
+                const int i = lane + 32 * t;
+                if (t <= kq) {
+                    if (i == k)
+                        y[t] = xk;
+                    else if (i < k)
+                        y[t] = fmaf(-sa[ph[t] + k * ld], xk, y[t]);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace opsblas

@@ -221,3 +221,26 @@ def test_refine_and_adjoint_validation(ob):
     assert L.aclblasSgetrsAdjointBatched(H, 4, 257, P, 4, P, P, 4, P, 4, P, 4, 2) == ob.INVALID_VALUE
     assert L.aclblasSgetrsAdjointBatched(H, 4, 2, P, 4, P, P, 3, P, 4, P, 4, 2) == ob.INVALID_VALUE
     assert L.aclblasSgetrsAdjointBatched(H, 4, 0, None, 4, None, None, 4, None, 4, None, 4, 2) == ob.SUCCESS
+
+
+def test_grouped_argument_checks(ob):
+    """Plan creation validates every group before touching the device."""
+    L = ob.lib()
+    ia = ob._int_array
+    plan = C.c_void_p()
+    args = lambda ns, nrhs, lda, ldb, sz: (len(ns), ia(ns), ia(nrhs), ia(lda), ia(ldb), ia(sz), None, C.byref(plan))
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(None, *args([4], [1], [4], [4], [2])) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, *args([-1], [1], [4], [4], [2])) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, *args([4], [-1], [4], [4], [2])) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, *args([4], [1], [3], [4], [2])) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, *args([4], [1], [4], [3], [2])) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, *args([4], [1], [4], [4], [-2])) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, 1, None, None, None, None, None, None,
+                                                 C.byref(plan)) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, -1, None, None, None, None, None, None,
+                                                 C.byref(plan)) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanCreate(H, 0, None, None, None, None, None, None, None) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanDestroy(None) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedPlanGetConfig(None, None) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfGetrsGroupedBatched(None, None, P, P, P, P) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSgetrfGetrsGroupedBatched(H, None, P, P, P, P) == ob.INVALID_VALUE
