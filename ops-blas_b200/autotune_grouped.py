@@ -4,13 +4,13 @@ For each size bucket it times every candidate configuration of the persistent ke
 synthetic batch whose orders are spread uniformly over the bucket (A ~ N(0,1), one right-hand
 side), keeps the fastest, and writes the table that aclblasSgetrfGetrsGroupedPlanCreate reads:
 
-    # n_lo n_hi lanes warps panel
+    # n_lo n_hi lanes warps rows
     1 4 4 0 0
     ...
 
 Candidates: n <= 16 -- lanes per matrix {natural segment, 32}; 33 <= n <= 128 -- warps per
-matrix {2, 4} x panel width {8, 16} (2-warp teams only where two matrices fit the shared-memory
-budget; the plan replaces the others). Every candidate computes the same bits, so only time
+matrix {4, 8} x rows per lane {ceil(n/32), ..., 4} (the instantiated register shapes; a 4-warp
+shape puts two matrices in one CTA). Every candidate computes the same bits, so only time
 decides. Usage (needs a B200):
 
     python ops-blas_b200/autotune_grouped.py [--out PATH] [--reps 7]
@@ -49,7 +49,8 @@ def _natural(n):
 def candidates(lo, hi):
     if hi <= 32:
         return [(_natural(hi), 0, 0)] + ([(32, 0, 0)] if hi <= 16 else [])
-    return [(0, w, p) for w in (2, 4) for p in (8, 16)]
+    rmin = (hi + 31) // 32
+    return [(0, w, r) for r in range(rmin, 5) for w in (4, 8) if not (r == 4 and w == 4)]
 
 
 def time_bucket(ob, handle, lo, hi, config, reps, seed=0, target_bytes=256 << 20, max_instances=400_000):
@@ -101,7 +102,7 @@ def main(argv=None):
     handle = ob.Handle()
     lines = ["# grouped getrf+getrs tuning table, written by autotune_grouped.py on "
              + torch.cuda.get_device_name(0),
-             "# n_lo n_hi lanes warps panel   (candidate: matrices/s)"]
+             "# n_lo n_hi lanes warps rows   (candidate: matrices/s)"]
     for lo, hi in SMALL_BUCKETS + MEDIUM_BUCKETS:
         results = {}
         for cfg in candidates(lo, hi):

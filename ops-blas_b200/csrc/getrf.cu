@@ -7,7 +7,7 @@
 // :93-104), rank-1 update (Rank1Update :38-50), stop at the first exactly-zero pivot
 // (:127-137). The B200 kernels are:
 //   n <= 32 : getrf_small_kernel, one warp segment per matrix, rows in registers;
-//   32 < n <= 128 : getrf_medium_kernel (getrf_medium.cu), blocked, matrix in shared memory;
+//   32 < n <= 128 : getrf_reg_kernel (getrf_reg.cu), matrix in registers across the CTA;
 //   128 < n <= 640 : getrf_large_kernel (getrf_large.cu), blocked, matrix in global memory;
 //   n  > 640 : getrf_generic_kernel, one CTA per matrix, unblocked in global memory.
 #include <cuda_runtime.h>
@@ -203,8 +203,11 @@ extern "C" aclblasStatus_t aclblasSgetrfBatched(
             default:
                 break;
         }
-    } else if (getrf_medium_supported(n)) {
-        return launch_status(kApi, getrf_medium_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize));
+    } else if (getrf_reg_supported(n)) {
+        int rows, warps;
+        reg_default_shape(n, rows, warps);
+        return launch_status(kApi, getrf_reg_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize, rows,
+                                                    warps));
     } else if (getrf_large_supported(n)) {
         return launch_status(kApi, getrf_large_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize, 0));
     } else {

@@ -5,15 +5,15 @@
 // blocks (lu_core.cuh) run here.
 //
 // A plan describes the batch: groups of instances that share n, nrhs, lda and ldb. Creating it
-// chooses, per group, the lanes per matrix (n <= 32) or the warps per matrix and the panel
-// width (32 < n <= 128) from a tuning table written by autotune_grouped.py (or from the
-// caller), orders the work largest first, and uploads the task lists to the device. Each
-// execution is then one launch of grouped_lu_kernel on the handle's stream (plus the regular
-// batched kernels for groups with n > 128): a grid of one wave of 128-thread CTAs that take
-// tasks from two device counters --
-//   phase 1, CTA tasks (n > 32): the CTA (or each 2-warp team of it) loads one matrix into
-//     shared memory, factors it (med_getrf_core), solves its right-hand sides from the
-//     resident factors (med_solve_core), and stores LU, pivots, info and X;
+// chooses, per group, the lanes per matrix (n <= 32) or the warps per matrix and rows per lane
+// (32 < n <= 128) from a tuning table written by autotune_grouped.py (or from the caller),
+// orders the work largest first, and uploads the task lists to the device. Each execution is
+// then one launch of grouped_lu_kernel on the handle's stream (plus the regular batched kernels
+// for groups with n > 128): a grid of one wave of 256-thread CTAs that take tasks from two
+// device counters --
+//   phase 1, CTA tasks (n > 32): the CTA (8 warps) or each 4-warp half of it factors one matrix
+//     held in registers (reg_getrf_core), stores LU, pivots and info, and solves the
+//     right-hand sides from the stored factors (reg_solve_global);
 //   phase 2, warp tasks (n <= 32): each warp takes 32/lanes matrices, factors them in
 //     registers (small_getrf_core) and solves from the registers (small_solve_core).
 // The last CTA to finish resets the counters, so consecutive executions on one stream need no
@@ -32,16 +32,17 @@
 
 namespace opsblas {
 
-constexpr int kGrpThreads = 128;
+constexpr int kGrpThreads = 256;
 constexpr int kGrpWarps = kGrpThreads / 32;
+constexpr int kGrpMaxN = 128;  // larger orders use the batched kernels
 
 struct GroupDev {
     int n, nrhs, lda, ldb;
     long long piv_off;  // first pivot of the group's first instance
     int first;          // index of the group's first instance in the pointer arrays
     int lanes;          // n <= 32: lanes per matrix (SEG)
-    int warps;          // n > 32: warps per matrix (2 or 4)
-    int panel;          // n > 32: panel width (8 or 16)
+    int warps;          // n > 32: warps per matrix (4 or 8)
+    int rows;           // n > 32: rows per lane (2, 3 or 4; 32 * rows >= n)
     int pad[2];
 };
 
@@ -53,56 +54,59 @@ struct GroupTask {
 };
 
 // ------------------------------------------------------------------------------ n > 32 --
-template <int NT, int PB>
-__device__ __forceinline__ void grouped_medium(const GroupDev& g, int li, float* const* Aarray, float* const* Barray,
-                                               int* piv, int* info, float* base, int ttid, int bar)
+// One matrix per team of NW warps: registers hold the matrix (reg_getrf_core); after the factors
+// are stored, the team's warps solve the right-hand-side columns from them (reg_solve_global,
+// L2-resident reads of what the team just wrote).
+template <int R, int NW>
+__device__ __forceinline__ void grouped_reg(const GroupDev& g, int li, float* const* Aarray, float* const* Barray,
+                                            int* piv, int* info, RegTeamSmem& S, int warp, int lane, int bar)
 {
+    constexpr int CW = RegShape<R, NW>::CW;
     const int n = g.n;
     const long long inst = (long long)g.first + li;
     float* A = Aarray[inst];
     int* pm = piv + g.piv_off + (long long)li * n;
-    const MedLayout L(n, PB);
-    const MedSmem S(base, L, n, PB);
-    const int ld = L.ld, lda = g.lda;
-    for (int e = ttid; e < n * n; e += NT) {
-        const int i = e % n, j = e / n;
-        S.sa[i + j * ld] = A[i + (long long)j * lda];
-    }
-    for (int i = ttid; i < n; i += NT) {
-        S.rmap[i] = i;
-        pm[i] = 0;
-    }
-    if (ttid == 0) S.sc[0] = 0;
-    team_sync<NT>(bar);
-
-    const int inf = med_getrf_core<true, NT, PB>(S, n, ld, L.ls_ld, pm, ttid, bar);
-
+    float a[R][CW];
+    int pos[R];
+    reg_load<R, NW>(a, A, g.lda, n, warp, lane);
+#pragma unroll
+    for (int t = 0; t < R; t++) pos[t] = lane + 32 * t;
+    for (int i = warp * 32 + lane; i < n; i += NW * 32) pm[i] = 0;
+    team_sync<NW * 32>(bar);
+    const int inf = reg_getrf_core<R, NW, true>(a, pos, n, S, pm, warp, lane, bar);
+    reg_store<R, NW>(a, pos, A, g.lda, n, warp, lane);
     if (g.nrhs > 0) {
-        float* Bm = Barray[inst];
-        const int lane = ttid & 31;
-        for (int c = ttid >> 5; c < g.nrhs; c += NT / 32) {
-            float* bc = Bm + (long long)c * g.ldb;
-            float y[kMedRows];
+        if (warp == 0) {
 #pragma unroll
-            for (int t = 0; t < kMedRows; t++) {
-                const int i = lane + 32 * t;
-                y[t] = i < n ? bc[S.rmap[i]] : 0.0f;
-            }
-            __syncwarp();  // every lane has read its b before any lane writes x
-            med_solve_core(S, n, ld, lane, y);
-            __syncwarp();
-#pragma unroll
-            for (int t = 0; t < kMedRows; t++) {
-                const int i = lane + 32 * t;
-                if (i < n) bc[i] = y[t];
-            }
+            for (int t = 0; t < R; t++)
+                if (lane + 32 * t < n) S.lmap[pos[t]] = lane + 32 * t;
         }
+        team_sync<NW * 32>(bar);  // the stored factors and the row map are visible to the team
+        float* Bm = Barray[inst];
+        for (int c = warp; c < g.nrhs; c += NW) reg_solve_global<R>(A, g.lda, n, Bm + (long long)c * g.ldb, S.lmap,
+                                                                    lane);
     }
-    for (int e = ttid; e < n * n; e += NT) {
-        const int i = e % n, j = e / n;
-        A[i + (long long)j * lda] = S.sa[S.rmap[i] + j * ld];
+    if (warp == 0 && lane == 0) info[inst] = inf;
+}
+
+template <int NW>
+__device__ __forceinline__ void grouped_reg_dispatch(const GroupDev& g, int li, float* const* Aarray,
+                                                     float* const* Barray, int* piv, int* info, RegTeamSmem& S,
+                                                     int warp, int lane, int bar)
+{
+    if (NW == 4) {
+        if (g.rows == 2)
+            grouped_reg<2, 4>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+        else
+            grouped_reg<3, 4>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+    } else {
+        if (g.rows == 2)
+            grouped_reg<2, 8>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+        else if (g.rows == 3)
+            grouped_reg<3, 8>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+        else
+            grouped_reg<4, 8>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
     }
-    if (ttid == 0) info[inst] = inf;
 }
 
 // ----------------------------------------------------------------------------- n <= 32 --
@@ -160,18 +164,18 @@ __device__ __forceinline__ void grouped_small_dispatch(const GroupDev& g, const 
         grouped_small<N, 32>(g, task, Aarray, Barray, piv, info, rowbuf, owner, lane);
 }
 
-__global__ void __launch_bounds__(kGrpThreads, 3)
+__global__ void __launch_bounds__(kGrpThreads, 2)
 grouped_lu_kernel(const GroupDev* __restrict__ groups, const GroupTask* __restrict__ cta_tasks, int n_cta,
                   const GroupTask* __restrict__ warp_tasks, int n_warp, int* __restrict__ counters,
-                  float* const* Aarray, float* const* Barray, int* piv, int* info, int team_floats)
+                  float* const* Aarray, float* const* Barray, int* piv, int* info)
 {
-    extern __shared__ __align__(16) float smem[];
+    __shared__ RegTeamSmem team[2];
     __shared__ int s_task;
     __shared__ __align__(16) float rowbuf[kGrpWarps][2][32];
     __shared__ int owner[kGrpWarps][32];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    // phase 1: one matrix per CTA (or per 2-warp team), largest first
+    // phase 1: one matrix per CTA (or per 4-warp team), largest first
     for (;;) {
         if (tid == 0) s_task = atomicAdd(&counters[0], 1);
         __syncthreads();
@@ -180,20 +184,13 @@ grouped_lu_kernel(const GroupDev* __restrict__ groups, const GroupTask* __restri
         if (t >= n_cta) break;
         const GroupTask task = cta_tasks[t];
         const GroupDev g = groups[task.group];
-        if (g.warps == 2) {
-            const int tm = warp >> 1;
-            if (tm < task.count) {
-                float* base = smem + (size_t)tm * team_floats;
-                if (g.panel == 8)
-                    grouped_medium<64, 8>(g, task.first + tm, Aarray, Barray, piv, info, base, tid & 63, 1 + tm);
-                else
-                    grouped_medium<64, 16>(g, task.first + tm, Aarray, Barray, piv, info, base, tid & 63, 1 + tm);
-            }
+        if (g.warps == 4) {
+            const int tm = warp >> 2;
+            if (tm < task.count)
+                grouped_reg_dispatch<4>(g, task.first + tm, Aarray, Barray, piv, info, team[tm], warp & 3, lane,
+                                        1 + tm);
         } else {
-            if (g.panel == 8)
-                grouped_medium<128, 8>(g, task.first, Aarray, Barray, piv, info, smem, tid, -1);
-            else
-                grouped_medium<128, 16>(g, task.first, Aarray, Barray, piv, info, smem, tid, -1);
+            grouped_reg_dispatch<8>(g, task.first, Aarray, Barray, piv, info, team[0], warp, lane, -1);
         }
     }
 
@@ -233,15 +230,20 @@ grouped_lu_kernel(const GroupDev* __restrict__ groups, const GroupTask* __restri
 
 // ------------------------------------------------------------------------- host side --
 struct TuneRow {
-    int lo, hi, lanes, warps, panel;
+    int lo, hi, lanes, warps, rows;
 };
 
-// Built-in choices, used when no tuning table is found: natural lanes, whole CTA, panel 16.
+// Built-in choices, used when no tuning table is found: natural lanes; 8 warps, ceil(n/32) rows.
 static void default_config(int n, int cfg[3])
 {
-    cfg[0] = n <= 4 ? 4 : (n <= 8 ? 8 : (n <= 16 ? 16 : 32));
-    cfg[1] = 4;
-    cfg[2] = 16;
+    if (n <= 32) {
+        cfg[0] = n <= 4 ? 4 : (n <= 8 ? 8 : (n <= 16 ? 16 : 32));
+        cfg[1] = 0;
+        cfg[2] = 0;
+    } else {
+        cfg[0] = 0;
+        reg_default_shape(n, cfg[2], cfg[1]);
+    }
 }
 
 static std::string tuning_path()
@@ -257,7 +259,7 @@ static std::string tuning_path()
     return "grouped_tuning.txt";
 }
 
-// Table rows "n_lo n_hi lanes warps panel"; '#' starts a comment.
+// Table rows "n_lo n_hi lanes warps rows"; '#' starts a comment.
 static std::vector<TuneRow> load_tuning()
 {
     std::vector<TuneRow> rows;
@@ -267,19 +269,14 @@ static std::vector<TuneRow> load_tuning()
     while (std::fgets(line, sizeof line, f)) {
         if (line[0] == '#') continue;
         TuneRow r;
-        if (std::sscanf(line, "%d %d %d %d %d", &r.lo, &r.hi, &r.lanes, &r.warps, &r.panel) == 5) rows.push_back(r);
+        if (std::sscanf(line, "%d %d %d %d %d", &r.lo, &r.hi, &r.lanes, &r.warps, &r.rows) == 5) rows.push_back(r);
     }
     std::fclose(f);
     return rows;
 }
 
-static size_t medium_team_bytes(int n, int panel) { return MedLayout(n, panel).bytes; }
-
-// Shared memory of the largest single-team matrix: 2-warp teams may use at most this for two.
-static size_t medium_budget() { return medium_team_bytes(kMedMaxN, 16); }
-
-// Makes cfg valid for n: lanes in {natural, 32} (n <= 32); warps in {2, 4} with two teams fitting
-// the budget, panel in {8, 16} (n > 32).
+// Makes cfg valid for n: lanes in {natural, 32} (n <= 32); an instantiated (rows, warps) shape
+// with 32 * rows >= n (n > 32).
 static void sanitize_config(int n, int cfg[3])
 {
     int def[3];
@@ -290,9 +287,10 @@ static void sanitize_config(int n, int cfg[3])
         cfg[2] = 0;
     } else {
         cfg[0] = 0;
-        if (cfg[2] != 8 && cfg[2] != 16) cfg[2] = def[2];
-        if (cfg[1] != 2 && cfg[1] != 4) cfg[1] = def[1];
-        if (cfg[1] == 2 && 2 * medium_team_bytes(n, cfg[2]) > medium_budget()) cfg[1] = 4;
+        if (!reg_shape_valid(n, cfg[2], cfg[1])) {
+            cfg[1] = def[1];
+            cfg[2] = def[2];
+        }
     }
 }
 
@@ -314,8 +312,6 @@ struct _aclblas_grouped_plan {
     opsblas::GroupTask* d_warp = nullptr;
     int* d_counters = nullptr;
     int n_cta = 0, n_warp = 0;
-    size_t smem = 0;
-    int team_floats = 0;
     int grid = 0;
     bool has_persistent = false;
 };
@@ -376,7 +372,7 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
             if (h.n >= r.lo && h.n <= r.hi) {
                 h.cfg[0] = r.lanes;
                 h.cfg[1] = r.warps;
-                h.cfg[2] = r.panel;
+                h.cfg[2] = r.rows;
             }
         if (configArray) {
             for (int q = 0; q < 3; q++)
@@ -394,15 +390,12 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
     for (int g = 0; g < groupCount; g++) order[g] = g;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p->groups[a].n > p->groups[b].n; });
     std::vector<GroupTask> cta, warp;
-    size_t smem = 0, team_bytes = 0;
     for (int g : order) {
         const GroupHost& h = p->groups[g];
-        if (h.n == 0 || h.size == 0 || h.n > kMedMaxN) continue;
+        if (h.n == 0 || h.size == 0 || h.n > kGrpMaxN) continue;
         if (h.n > 32) {
-            const int per = h.cfg[1] == 2 ? 2 : 1;
+            const int per = h.cfg[1] == 4 ? 2 : 1;
             for (int i = 0; i < h.size; i += per) cta.push_back({g, i, std::min(per, h.size - i), 0});
-            smem = std::max(smem, per * medium_team_bytes(h.n, h.cfg[2]));
-            if (per == 2) team_bytes = std::max(team_bytes, medium_team_bytes(h.n, h.cfg[2]));
         } else {
             const int per = 32 / h.cfg[0];
             for (int i = 0; i < h.size; i += per) warp.push_back({g, i, std::min(per, h.size - i), 0});
@@ -411,8 +404,6 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
     p->n_cta = (int)cta.size();
     p->n_warp = (int)warp.size();
     p->has_persistent = p->n_cta + p->n_warp > 0;
-    p->team_floats = (int)(team_bytes / 4);
-    p->smem = smem;
 
     std::vector<GroupDev> gd(std::max(groupCount, 1));
     for (int g = 0; g < groupCount; g++) {
@@ -440,12 +431,9 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
             err = cudaMemcpy(p->d_cta, cta.data(), cta.size() * sizeof(GroupTask), cudaMemcpyHostToDevice);
         if (err == cudaSuccess && !warp.empty())
             err = cudaMemcpy(p->d_warp, warp.data(), warp.size() * sizeof(GroupTask), cudaMemcpyHostToDevice);
-        if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(grouped_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)std::max<size_t>(p->smem, 1));
         int per_sm = 0;
         if (err == cudaSuccess)
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_lu_kernel, kGrpThreads, p->smem);
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_lu_kernel, kGrpThreads, 0);
         if (err != cudaSuccess || per_sm < 1) {
             log_error(kApi, "plan set-up failed: %s", cudaGetErrorString(err));
             cudaFree(p->dmem);
@@ -501,15 +489,15 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedBatched(aclblasHandle_t hand
     }
     cudaStream_t st = handle->stream;
     if (plan->has_persistent) {
-        grouped_lu_kernel<<<(unsigned)plan->grid, kGrpThreads, plan->smem, st>>>(
+        grouped_lu_kernel<<<(unsigned)plan->grid, kGrpThreads, 0, st>>>(
             plan->d_groups, plan->d_cta, plan->n_cta, plan->d_warp, plan->n_warp, plan->d_counters, Aarray, Barray,
-            PivotArray, infoArray, plan->team_floats);
+            PivotArray, infoArray);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return launch_status(kApi, err);
     }
     // groups beyond the persistent kernel's sizes: the regular batched kernels
     for (const GroupHost& h : plan->groups) {
-        if (h.n <= kMedMaxN || h.size == 0) continue;
+        if (h.n <= kGrpMaxN || h.size == 0) continue;
         aclblasStatus_t s = aclblasSgetrfBatched(handle, h.n, Aarray + h.first, h.lda, PivotArray + h.piv_off,
                                                  infoArray + h.first, h.size);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;

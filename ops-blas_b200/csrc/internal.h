@@ -54,6 +54,13 @@ bool getrf_large_supported(int n);
 cudaError_t getrf_large_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch,
                                int mode);
 
+// getrf_reg.cu: 32 < n <= 128, matrix in registers; shape = rows per lane x warps per matrix.
+bool getrf_reg_supported(int n);
+bool reg_shape_valid(int n, int rows, int warps);
+void reg_default_shape(int n, int& rows, int& warps);
+cudaError_t getrf_reg_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch,
+                             int rows, int warps);
+
 // getrf_medium.cu: 32 < n <= 128, matrix resident in shared memory.
 bool getrf_medium_supported(int n);
 cudaError_t getrf_medium_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info,

@@ -162,6 +162,245 @@ __device__ __forceinline__ float small_solve_core(const float4 (&a4)[(N + 3) / 4
     return y;
 }
 
+// Barrier over the team: bar < 0 means the team is the whole CTA.
+template <int NT>
+__device__ __forceinline__ void team_sync(int bar)
+{
+    if (bar < 0)
+        __syncthreads();
+    else
+        asm volatile("bar.sync %0, %1;\n" ::"r"(bar), "n"(NT) : "memory");
+}
+
+// =============================================================================================
+// Register LU for 32 < n <= 128, run by a team of NW warps. The matrix lives in registers:
+// lane l of every warp holds rows p = l + 32 t (t < R, R = ceil(n / 32)), and warp w holds the
+// columns j = s * NW + w (slot s < CW = 32 R / NW), so every warp sees every row and the columns
+// are dealt out cyclically (all warps stay busy until the last columns). Pivoting is implicit as
+// in small_getrf_core: `pos` (replicated in every warp) is the row's index in the reference's
+// in-place matrix; rows never move. Per column k (owner warp k % NW, slot k / NW):
+//   A. the owner warp finds the first-maximum pivot (lane-local over t, then redux.sync),
+//      forms l = a / pivot for the rows that end below the pivot (true division) and publishes
+//      the pivot position, the pivot value and the multipliers in shared memory;
+//   B. one team barrier; every warp applies the interchange to `pos`, broadcasts the pivot row's
+//      entries of its own columns through shared memory, and updates a(i, j) -= l_i * u_j for
+//      its columns j > k and rows below the pivot -- one fmaf per element, column order.
+// On an exactly-zero pivot every warp stops (the reference's early exit).
+// =============================================================================================
+template <int R, int NW>
+struct RegShape {
+    static constexpr int NMAX = 32 * R;
+    static constexpr int CW = NMAX / NW;  // column slots per warp
+    static_assert(NMAX % NW == 0, "columns must deal out evenly");
+};
+
+constexpr int kRegMaxCW = 24;  // largest CW of the instantiated shapes
+
+// Shared state of one team.
+struct RegTeamSmem {
+    float l[2][128];               // multipliers of the current column by physical row (double buffered)
+    float u[8][kRegMaxCW];         // per warp: the pivot row's entries in the warp's columns
+    int lmap[128];                 // after factoring: logical row -> physical row
+    int ppos[2];
+    float pv[2];
+};
+
+// Loads matrix A (n x n, leading dimension lda) into the team's registers.
+template <int R, int NW>
+__device__ __forceinline__ void reg_load(float (&a)[R][RegShape<R, NW>::CW], const float* A, int lda, int n,
+                                         int warp, int lane)
+{
+    constexpr int CW = RegShape<R, NW>::CW;
+#pragma unroll
+    for (int s = 0; s < CW; s++) {
+        const int j = s * NW + warp;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+            const int p = lane + 32 * t;
+            a[t][s] = (p < n && j < n) ? A[p + (long long)j * lda] : 0.0f;
+        }
+    }
+}
+
+// Stores the factors: row p goes to its final position pos.
+template <int R, int NW>
+__device__ __forceinline__ void reg_store(const float (&a)[R][RegShape<R, NW>::CW], const int (&pos)[R], float* A,
+                                          int lda, int n, int warp, int lane)
+{
+    constexpr int CW = RegShape<R, NW>::CW;
+#pragma unroll
+    for (int s = 0; s < CW; s++) {
+        const int j = s * NW + warp;
+#pragma unroll
+        for (int t = 0; t < R; t++) {
+            const int p = lane + 32 * t;
+            if (p < n && j < n) A[pos[t] + (long long)j * lda] = a[t][s];
+        }
+    }
+}
+
+// Factors the team's matrix. pos must start as the physical row (lane + 32 t); pm (when
+// pivoting) must be zero for the whole team before the call (a team barrier after zeroing).
+// Returns info.
+template <int R, int NW, bool PIVOT>
+__device__ __forceinline__ int reg_getrf_core(float (&a)[R][RegShape<R, NW>::CW], int (&pos)[R], int n,
+                                              RegTeamSmem& S, int* pm, int warp, int lane, int bar)
+{
+    constexpr int CW = RegShape<R, NW>::CW;
+    int info = 0;
+    bool stop = false;
+#pragma unroll
+    for (int c = 0; c < CW; c++) {
+        if (stop) break;
+        for (int w = 0; w < NW; w++) {
+            const int k = c * NW + w;
+            if (k >= n) {
+                stop = true;
+                break;
+            }
+            const int buf = k & 1;
+            if (warp == w) {
+                // ---- A: pivot, multipliers (owner warp) ----
+                int ppos = k;
+                if (PIVOT) {
+                    unsigned bkey = 0, bpos = 0xffffffffu;
+#pragma unroll
+                    for (int t = 0; t < R; t++) {
+                        const bool elig = pos[t] < n && pos[t] >= k;
+                        const float v = fabsf(a[t][c]);
+                        const unsigned key = (elig && v > 0.0f) ? __float_as_uint(v) : 0u;
+                        if (elig && (key > bkey || (key == bkey && (unsigned)pos[t] < bpos))) {
+                            bkey = key;
+                            bpos = (unsigned)pos[t];
+                        }
+                    }
+                    ppos = (int)seg_argmax<32>(bkey, bpos, 0);
+                }
+                float cand = 0.0f;
+                bool own = false;
+#pragma unroll
+                for (int t = 0; t < R; t++) {
+                    if (pos[t] == ppos) {
+                        cand = a[t][c];
+                        own = true;
+                    }
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, own);
+                const float pv = __shfl_sync(0xffffffffu, cand, __ffs(bal) - 1);
+                if (pv != 0.0f) {
+#pragma unroll
+                    for (int t = 0; t < R; t++) {
+                        const int np = pos[t] == ppos ? k : (pos[t] == k ? ppos : pos[t]);
+                        if (np > k && np < n) {
+                            const float l = a[t][c] / pv;
+                            a[t][c] = l;
+                            S.l[buf][lane + 32 * t] = l;
+                        }
+                    }
+                }
+                if (lane == 0) {
+                    S.ppos[buf] = ppos;
+                    S.pv[buf] = pv;
+                    if (PIVOT) pm[k] = ppos + 1;
+                }
+            }
+            team_sync<NW * 32>(bar);
+            // ---- B: interchange, pivot-row broadcast, update (every warp) ----
+            const int ppos = S.ppos[buf];
+            if (S.pv[buf] == 0.0f) {
+                info = k + 1;
+                stop = true;
+                break;
+            }
+#pragma unroll
+            for (int t = 0; t < R; t++) pos[t] = pos[t] == ppos ? k : (pos[t] == k ? ppos : pos[t]);
+            float l[R];
+            bool below[R];
+#pragma unroll
+            for (int t = 0; t < R; t++) {
+                below[t] = pos[t] > k && pos[t] < n;
+                l[t] = below[t] ? S.l[buf][lane + 32 * t] : 0.0f;
+            }
+            float* ub = S.u[warp];
+#pragma unroll
+            for (int t = 0; t < R; t++) {
+                if (pos[t] == k) {
+#pragma unroll
+                    for (int s = c; s < CW; s++) ub[s] = a[t][s];
+                }
+            }
+            __syncwarp();
+#pragma unroll
+            for (int s = c; s < CW; s++) {
+                if (s > c || warp > w) {
+                    const float u = ub[s];
+#pragma unroll
+                    for (int t = 0; t < R; t++)
+                        if (below[t]) a[t][s] = fmaf(-l[t], u, a[t][s]);
+                }
+            }
+        }
+    }
+    return info;
+}
+
+// Solves one right-hand side column bc (n values) with the factors already stored in logical
+// row order at A (leading dimension lda) and the team's lmap, in the reference getrs's order
+// (trans N): b permuted, unit-L forward sweep, U backward sweep with x_j = y_j / U(j,j), one
+// fmaf per update. Run by one warp; lane l handles logical rows l + 32 t.
+template <int R>
+__device__ __forceinline__ void reg_solve_global(const float* A, int lda, int n, float* bc, const int* lmap,
+                                                 int lane)
+{
+    float y[R];
+#pragma unroll
+    for (int t = 0; t < R; t++) {
+        const int i = lane + 32 * t;
+        y[t] = i < n ? bc[lmap[i]] : 0.0f;
+    }
+    __syncwarp();  // every lane has read its b before any lane writes x
+#pragma unroll
+    for (int kq = 0; kq < R; kq++) {
+#pragma unroll 4
+        for (int kl = 0; kl < 32; kl++) {
+            const int k = kq * 32 + kl;
+            if (k >= n) break;
+            const float yk = __shfl_sync(0xffffffffu, y[kq], kl);
+            const float* col = A + (long long)k * lda;
+#pragma unroll
+            for (int t = kq; t < R; t++) {
+                const int i = lane + 32 * t;
+                if (i > k && i < n) y[t] = fmaf(-col[i], yk, y[t]);
+            }
+        }
+    }
+#pragma unroll
+    for (int kq = R - 1; kq >= 0; kq--) {
+#pragma unroll 4
+        for (int kl = 31; kl >= 0; kl--) {
+            const int k = kq * 32 + kl;
+            if (k >= n) continue;
+            const float* col = A + (long long)k * lda;
+            const float t0 = (lane == kl) ? y[kq] / col[k] : 0.0f;
+            const float xk = __shfl_sync(0xffffffffu, t0, kl);
+#pragma unroll
+            for (int t = 0; t <= kq; t++) {
+                const int i = lane + 32 * t;
+                if (i == k)
+                    y[t] = xk;
+                else if (i < k)
+                    y[t] = fmaf(-col[i], xk, y[t]);
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < R; t++) {
+        const int i = lane + 32 * t;
+        if (i < n) bc[i] = y[t];
+    }
+}
+
 // =============================================================================================
 // Blocked LU of one matrix resident in shared memory (32 < n <= 128), run by a team of NT
 // threads (NT = 64 or 128; the team's first warp factors the panels). The reference's arithmetic
@@ -218,16 +457,6 @@ struct MedSmem {
         sc = reinterpret_cast<int*>(prow + 64);
     }
 };
-
-// Barrier over the team: bar < 0 means the team is the whole CTA.
-template <int NT>
-__device__ __forceinline__ void team_sync(int bar)
-{
-    if (bar < 0)
-        __syncthreads();
-    else
-        asm volatile("bar.sync %0, %1;\n" ::"r"(bar), "n"(NT) : "memory");
-}
 
 // Factors the matrix in S.sa (loaded by the caller, rmap = identity, sc[0] = 0, pm zeroed when
 // pivoting). Returns info. tid is the thread's index within the team.

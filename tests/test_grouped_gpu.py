@@ -2,7 +2,7 @@
 
 Every instance must come out bit-identical to aclblasSgetrfBatched followed by
 aclblasSgetrsBatched (trans N) on the same matrix -- LU, pivots, info and X -- whatever the
-per-group configuration (lanes per matrix, warps per matrix, panel width), over repeated
+per-group configuration (lanes per matrix, warps per matrix, rows per lane), over repeated
 executions (the persistent kernel resets its own work counters) and when replayed from a CUDA
 graph. The plain path itself is pinned to the oracle by test_lu_gpu.py; a sample is checked
 against the oracle here too.
@@ -97,21 +97,19 @@ def test_grouped_repeated_executions_reset_counters(ob, handle):
         _assert_same(o, ref)
 
 
-@pytest.mark.parametrize("config", [(32, 0, 0), (0, 2, 8), (0, 2, 16), (0, 4, 8), (0, 4, 16)])
+@pytest.mark.parametrize("config", [(32, 0, 0), (0, 4, 2), (0, 8, 2), (0, 4, 3), (0, 8, 3), (0, 8, 4)])
 def test_grouped_every_config_gives_the_same_bits(ob, handle, config):
     d = _setup(ob, **MIXED, seed=3, ldpad=3)
     cfgs = [config] * len(d["ns"])
     out, ref, used = _run_both(ob, handle, d, config=cfgs)
     _assert_same(out[0], ref)
-    for n, (lanes, warps, panel) in zip(d["ns"], used):
+    for n, (lanes, warps, rows) in zip(d["ns"], used):
         if n <= 32:
             assert lanes in (4, 8, 16, 32) and (config[0] != 32 or lanes == 32)
         else:
-            assert panel in (8, 16) and warps in (2, 4)
-            if config[2]:
-                assert panel == config[2]
-            if config[1] == 4:
-                assert warps == 4
+            assert 32 * rows >= n and warps in (4, 8) and not (rows == 4 and warps == 4)
+            if config[2] and 32 * config[2] >= n:
+                assert (warps, rows) == (config[1], config[2])
 
 
 def test_grouped_singular_and_factor_only(ob, handle):
@@ -187,8 +185,8 @@ def test_grouped_cuda_graph_replay(ob):
 
 def test_grouped_tuning_table_is_read(ob, handle, tmp_path, monkeypatch):
     table = tmp_path / "t.txt"
-    table.write_text("# n_lo n_hi lanes warps panel\n1 16 32 0 0\n33 64 0 2 8\n65 128 0 4 8\n")
+    table.write_text("# n_lo n_hi lanes warps rows\n1 16 32 0 0\n33 64 0 4 3\n65 128 0 8 4\n")
     monkeypatch.setenv("OPSBLAS_GROUPED_TUNING", str(table))
     plan = ob.GroupedPlan(handle, [8, 40, 100], [1, 1, 1], [2, 2, 2])
-    assert plan.config() == [(32, 0, 0), (0, 2, 8), (0, 4, 8)]
+    assert plan.config() == [(32, 0, 0), (0, 4, 3), (0, 8, 4)]
     plan.close()
