@@ -13,7 +13,7 @@
 // device counters --
 //   phase 1, CTA tasks (n > 32): the CTA (8 warps) or each 4-warp half of it factors one matrix
 //     held in registers (reg_getrf_core), stores LU, pivots and info, and solves the
-//     right-hand sides from the stored factors (reg_solve_global);
+//     right-hand sides from a copy of the factors in shared memory (med_solve_core);
 //   phase 2, warp tasks (n <= 32): each warp takes 32/lanes matrices, factors them in
 //     registers (small_getrf_core) and solves from the registers (small_solve_core).
 // The last CTA to finish resets the counters, so consecutive executions on one stream need no
@@ -54,12 +54,14 @@ struct GroupTask {
 };
 
 // ------------------------------------------------------------------------------ n > 32 --
-// One matrix per team of NW warps: registers hold the matrix (reg_getrf_core); after the factors
-// are stored, the team's warps solve the right-hand-side columns from them (reg_solve_global,
-// L2-resident reads of what the team just wrote).
+// One matrix per team of NW warps: registers hold the matrix (reg_getrf_core). With right-hand
+// sides, the factors are also staged in the team's shared memory (physical rows, odd column
+// stride) so that the team's warps solve their columns from there (med_solve_core) while the
+// factors go to global memory.
 template <int R, int NW>
 __device__ __forceinline__ void grouped_reg(const GroupDev& g, int li, float* const* Aarray, float* const* Barray,
-                                            int* piv, int* info, RegTeamSmem& S, int warp, int lane, int bar)
+                                            int* piv, int* info, RegTeamSmem& S, float* sa, int warp, int lane,
+                                            int bar)
 {
     constexpr int CW = RegShape<R, NW>::CW;
     const int n = g.n;
@@ -74,17 +76,44 @@ __device__ __forceinline__ void grouped_reg(const GroupDev& g, int li, float* co
     for (int i = warp * 32 + lane; i < n; i += NW * 32) pm[i] = 0;
     team_sync<NW * 32>(bar);
     const int inf = reg_getrf_core<R, NW, true>(a, pos, n, S, pm, warp, lane, bar);
-    reg_store<R, NW>(a, pos, A, g.lda, n, warp, lane);
+    const int ld = n | 1;
     if (g.nrhs > 0) {
+#pragma unroll
+        for (int s = 0; s < CW; s++) {
+            const int j = s * NW + warp;
+#pragma unroll
+            for (int t = 0; t < R; t++) {
+                const int p = lane + 32 * t;
+                if (p < n && j < n) sa[p + j * ld] = a[t][s];
+            }
+        }
         if (warp == 0) {
 #pragma unroll
             for (int t = 0; t < R; t++)
                 if (lane + 32 * t < n) S.lmap[pos[t]] = lane + 32 * t;
         }
-        team_sync<NW * 32>(bar);  // the stored factors and the row map are visible to the team
+    }
+    reg_store<R, NW>(a, pos, A, g.lda, n, warp, lane);
+    if (g.nrhs > 0) {
+        team_sync<NW * 32>(bar);  // staged factors and row map visible to the team
         float* Bm = Barray[inst];
-        for (int c = warp; c < g.nrhs; c += NW) reg_solve_global<R>(A, g.lda, n, Bm + (long long)c * g.ldb, S.lmap,
-                                                                    lane);
+        for (int c = warp; c < g.nrhs; c += NW) {
+            float* bc = Bm + (long long)c * g.ldb;
+            float y[kMedRows];
+#pragma unroll
+            for (int t = 0; t < kMedRows; t++) {
+                const int i = lane + 32 * t;
+                y[t] = i < n ? bc[S.lmap[i]] : 0.0f;
+            }
+            __syncwarp();  // every lane has read its b before any lane writes x
+            med_solve_core(sa, S.lmap, n, ld, lane, y);
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < kMedRows; t++) {
+                const int i = lane + 32 * t;
+                if (i < n) bc[i] = y[t];
+            }
+        }
     }
     if (warp == 0 && lane == 0) info[inst] = inf;
 }
@@ -92,20 +121,20 @@ __device__ __forceinline__ void grouped_reg(const GroupDev& g, int li, float* co
 template <int NW>
 __device__ __forceinline__ void grouped_reg_dispatch(const GroupDev& g, int li, float* const* Aarray,
                                                      float* const* Barray, int* piv, int* info, RegTeamSmem& S,
-                                                     int warp, int lane, int bar)
+                                                     float* sa, int warp, int lane, int bar)
 {
     if (NW == 4) {
         if (g.rows == 2)
-            grouped_reg<2, 4>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+            grouped_reg<2, 4>(g, li, Aarray, Barray, piv, info, S, sa, warp, lane, bar);
         else
-            grouped_reg<3, 4>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+            grouped_reg<3, 4>(g, li, Aarray, Barray, piv, info, S, sa, warp, lane, bar);
     } else {
         if (g.rows == 2)
-            grouped_reg<2, 8>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+            grouped_reg<2, 8>(g, li, Aarray, Barray, piv, info, S, sa, warp, lane, bar);
         else if (g.rows == 3)
-            grouped_reg<3, 8>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+            grouped_reg<3, 8>(g, li, Aarray, Barray, piv, info, S, sa, warp, lane, bar);
         else
-            grouped_reg<4, 8>(g, li, Aarray, Barray, piv, info, S, warp, lane, bar);
+            grouped_reg<4, 8>(g, li, Aarray, Barray, piv, info, S, sa, warp, lane, bar);
     }
 }
 
@@ -167,8 +196,9 @@ __device__ __forceinline__ void grouped_small_dispatch(const GroupDev& g, const 
 __global__ void __launch_bounds__(kGrpThreads, 2)
 grouped_lu_kernel(const GroupDev* __restrict__ groups, const GroupTask* __restrict__ cta_tasks, int n_cta,
                   const GroupTask* __restrict__ warp_tasks, int n_warp, int* __restrict__ counters,
-                  float* const* Aarray, float* const* Barray, int* piv, int* info)
+                  float* const* Aarray, float* const* Barray, int* piv, int* info, int team_floats)
 {
+    extern __shared__ __align__(16) float dyn[];  // per team: staged factors for the solve
     __shared__ RegTeamSmem team[2];
     __shared__ int s_task;
     __shared__ __align__(16) float rowbuf[kGrpWarps][2][32];
@@ -187,10 +217,11 @@ grouped_lu_kernel(const GroupDev* __restrict__ groups, const GroupTask* __restri
         if (g.warps == 4) {
             const int tm = warp >> 2;
             if (tm < task.count)
-                grouped_reg_dispatch<4>(g, task.first + tm, Aarray, Barray, piv, info, team[tm], warp & 3, lane,
+                grouped_reg_dispatch<4>(g, task.first + tm, Aarray, Barray, piv, info, team[tm],
+                                        dyn + (size_t)tm * team_floats, warp & 3, lane,
                                         1 + tm);
         } else {
-            grouped_reg_dispatch<8>(g, task.first, Aarray, Barray, piv, info, team[0], warp, lane, -1);
+            grouped_reg_dispatch<8>(g, task.first, Aarray, Barray, piv, info, team[0], dyn, warp, lane, -1);
         }
     }
 
@@ -313,6 +344,8 @@ struct _aclblas_grouped_plan {
     int* d_counters = nullptr;
     int n_cta = 0, n_warp = 0;
     int grid = 0;
+    int team_floats = 0;  // shared-memory floats per team for the staged factors
+    size_t smem = 0;      // dynamic shared memory per CTA
     bool has_persistent = false;
 };
 
@@ -390,12 +423,20 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
     for (int g = 0; g < groupCount; g++) order[g] = g;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p->groups[a].n > p->groups[b].n; });
     std::vector<GroupTask> cta, warp;
+    size_t team_floats = 0, smem = 0;
     for (int g : order) {
         const GroupHost& h = p->groups[g];
         if (h.n == 0 || h.size == 0 || h.n > kGrpMaxN) continue;
         if (h.n > 32) {
             const int per = h.cfg[1] == 4 ? 2 : 1;
             for (int i = 0; i < h.size; i += per) cta.push_back({g, i, std::min(per, h.size - i), 0});
+            if (h.nrhs > 0) {
+                const size_t f = ((size_t)(h.n | 1) * h.n + 3) & ~(size_t)3;  // staged factors, 16-byte rounded
+                if (per == 2)
+                    team_floats = std::max(team_floats, f);  // second team starts here
+                else
+                    smem = std::max(smem, f * 4);
+            }
         } else {
             const int per = 32 / h.cfg[0];
             for (int i = 0; i < h.size; i += per) warp.push_back({g, i, std::min(per, h.size - i), 0});
@@ -404,6 +445,8 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
     p->n_cta = (int)cta.size();
     p->n_warp = (int)warp.size();
     p->has_persistent = p->n_cta + p->n_warp > 0;
+    p->team_floats = (int)team_floats;
+    p->smem = std::max(smem, 2 * team_floats * 4);  // the two 4-warp teams of a CTA stage side by side
 
     std::vector<GroupDev> gd(std::max(groupCount, 1));
     for (int g = 0; g < groupCount; g++) {
@@ -431,9 +474,12 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
             err = cudaMemcpy(p->d_cta, cta.data(), cta.size() * sizeof(GroupTask), cudaMemcpyHostToDevice);
         if (err == cudaSuccess && !warp.empty())
             err = cudaMemcpy(p->d_warp, warp.data(), warp.size() * sizeof(GroupTask), cudaMemcpyHostToDevice);
+        if (err == cudaSuccess)
+            err = cudaFuncSetAttribute(grouped_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)std::max<size_t>(p->smem, 1));
         int per_sm = 0;
         if (err == cudaSuccess)
-            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_lu_kernel, kGrpThreads, 0);
+            err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_lu_kernel, kGrpThreads, p->smem);
         if (err != cudaSuccess || per_sm < 1) {
             log_error(kApi, "plan set-up failed: %s", cudaGetErrorString(err));
             cudaFree(p->dmem);
@@ -489,9 +535,9 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedBatched(aclblasHandle_t hand
     }
     cudaStream_t st = handle->stream;
     if (plan->has_persistent) {
-        grouped_lu_kernel<<<(unsigned)plan->grid, kGrpThreads, 0, st>>>(
+        grouped_lu_kernel<<<(unsigned)plan->grid, kGrpThreads, plan->smem, st>>>(
             plan->d_groups, plan->d_cta, plan->n_cta, plan->d_warp, plan->n_warp, plan->d_counters, Aarray, Barray,
-            PivotArray, infoArray);
+            PivotArray, infoArray, plan->team_floats);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return launch_status(kApi, err);
     }

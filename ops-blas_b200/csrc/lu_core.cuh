@@ -197,7 +197,7 @@ struct RegShape {
 constexpr int kRegMaxCW = 24;  // largest CW of the instantiated shapes
 
 // Shared state of one team.
-struct RegTeamSmem {
+struct __align__(16) RegTeamSmem {
     float l[2][128];               // multipliers of the current column by physical row (double buffered)
     float u[8][kRegMaxCW];         // per warp: the pivot row's entries in the warp's columns
     int lmap[128];                 // after factoring: logical row -> physical row
@@ -321,22 +321,49 @@ __device__ __forceinline__ int reg_getrf_core(float (&a)[R][RegShape<R, NW>::CW]
                 below[t] = pos[t] > k && pos[t] < n;
                 l[t] = below[t] ? S.l[buf][lane + 32 * t] : 0.0f;
             }
-            float* ub = S.u[warp];
+            // the lane holding logical row k publishes its slots (from chunk c/4 on) as float4s
+            float4* ub4 = reinterpret_cast<float4*>(S.u[warp]);
 #pragma unroll
             for (int t = 0; t < R; t++) {
                 if (pos[t] == k) {
 #pragma unroll
-                    for (int s = c; s < CW; s++) ub[s] = a[t][s];
+                    for (int q = c / 4; q < CW / 4; q++)
+                        ub4[q] = make_float4(a[t][4 * q], a[t][4 * q + 1], a[t][4 * q + 2], a[t][4 * q + 3]);
                 }
             }
             __syncwarp();
+            float u[CW];
 #pragma unroll
-            for (int s = c; s < CW; s++) {
-                if (s > c || warp > w) {
-                    const float u = ub[s];
+            for (int q = c / 4; q < CW / 4; q++) {
+                const float4 v = ub4[q];
+                u[4 * q] = v.x;
+                u[4 * q + 1] = v.y;
+                u[4 * q + 2] = v.z;
+                u[4 * q + 3] = v.w;
+            }
+            // slot c holds column k itself (owner warp) or a column right of k (later warps)
+            if (warp > w) {
+#pragma unroll
+                for (int t = 0; t < R; t++)
+                    if (below[t]) a[t][c] = fmaf(-l[t], u[c], a[t][c]);
+            }
+            // slots c+1.. : two columns per packed fma, fma(u, -l, a) == fma(-l, u, a) exactly
+#pragma unroll
+            for (int s2 = c + 1; s2 < CW; s2 += 2) {
+                if (s2 + 1 < CW) {
+#pragma unroll
+                    for (int t = 0; t < R; t++) {
+                        if (below[t]) {
+                            const float2 r2 = __ffma2_rn(make_float2(u[s2], u[s2 + 1]), make_float2(-l[t], -l[t]),
+                                                         make_float2(a[t][s2], a[t][s2 + 1]));
+                            a[t][s2] = r2.x;
+                            a[t][s2 + 1] = r2.y;
+                        }
+                    }
+                } else {
 #pragma unroll
                     for (int t = 0; t < R; t++)
-                        if (below[t]) a[t][s] = fmaf(-l[t], u, a[t][s]);
+                        if (below[t]) a[t][s2] = fmaf(-l[t], u[s2], a[t][s2]);
                 }
             }
         }
@@ -630,13 +657,13 @@ __device__ __forceinline__ int med_getrf_core(const MedSmem& S, int n, int ld, i
 }
 
 // Solves right-hand-side column y (n values, logical order after the interchanges: the lane's
-// rows i = lane + 32 t enter with y[t] = b[rmap[i]]) with the factors in S, in the reference
+// rows i = lane + 32 t enter with y[t] = b[rmap[i]]) with the factors held in shared memory at
+// sa (physical row p, column j at sa[p + j * ld]; logical row i is physical row rmap[i]), in the reference
 // getrs's order (trans N): unit-L forward sweep, then U backward sweep with x_j = y_j / U(j,j).
 // Run by one warp; y[t] leaves as x[lane + 32 t].
-__device__ __forceinline__ void med_solve_core(const MedSmem& S, int n, int ld, int lane, float (&y)[kMedRows])
+__device__ __forceinline__ void med_solve_core(const float* sa, const int* rmap, int n, int ld, int lane,
+                                               float (&y)[kMedRows])
 {
-    const float* sa = S.sa;
-    const int* rmap = S.rmap;
     int ph[kMedRows];
 #pragma unroll
     for (int t = 0; t < kMedRows; t++) ph[t] = (lane + 32 * t < n) ? rmap[lane + 32 * t] : 0;
