@@ -133,7 +133,7 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasGemmBatchedEx(
  * max_c ||r_c||inf / (||A||inf ||x_c||inf + ||b_c||inf) are computed in FP64 on the GPU;
  * matrices whose error is <= tol stop, the others add LU \ r to X. berrArray (double),
  * iterArray (refinement steps used; maxIter if not converged) and infoArray are device arrays.
- * Needs n*nrhs*4 (rounded up to 256) + 12 bytes per matrix of handle workspace
+ * Needs n*nrhs*4 (rounded up to 256) + 20 bytes per matrix (+ 512) of handle workspace
  * (aclblasSetWorkspace); EXECUTION_FAILED if it is smaller. */
 ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     aclblasHandle_t handle, int n, int nrhs, const float* const Aarray[], int lda, float* const LUarray[], int ldlu,
@@ -149,7 +149,7 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
  * call cudaMalloc/cudaFree, which synchronise the device): the call allocates nothing and
  * leaves the handle workspace alone. Its scratch is a fixed array of
  * ACLBLAS_REFINE_STATIC_SCRATCH_BYTES in the library's device image, one per device; a call
- * needs (n*nrhs*4 rounded up to 256 + 12) * batchCount + 512 bytes of it, and a larger request
+ * needs (n*nrhs*4 rounded up to 256 + 20) * batchCount + 512 bytes of it, and a larger request
  * returns ACLBLAS_STATUS_INVALID_VALUE without launching anything. The first call on each device
  * (with the handle's device current) sets up the scratch address; make it before any stream
  * capture. The scratch is shared by all handles and streams of the process: calls that overlap

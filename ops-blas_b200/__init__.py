@@ -204,7 +204,7 @@ class Handle:
         info = torch.empty(batch, dtype=torch.int32, device=dev)
         berr = torch.empty(batch, dtype=torch.float64, device=dev)
         iters = torch.empty(batch, dtype=torch.int32, device=dev)
-        need = (((n * nrhs * 4 + 255) // 256) * 256 + 12) * batch + 512
+        need = (((n * nrhs * 4 + 255) // 256) * 256 + 20) * batch + 512
         if self._ws is None or self._ws.numel() < need:
             self._ws = torch.empty(max(need, 32 << 20), dtype=torch.uint8, device=dev)
             check("aclblasSetWorkspace", lib().aclblasSetWorkspace(self.h, _vp(self._ws.data_ptr()),

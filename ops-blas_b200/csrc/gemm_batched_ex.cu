@@ -286,9 +286,10 @@ extern "C" aclblasStatus_t aclblasGemmBatchedEx(
                                                              Carray, ldc, batchCount);
             break;
         case Combo::F32_F32_F32:
-            if (computeType == ACLBLAS_COMPUTE_32F_FAST_TF32)
-                err = run_gemm<E::F32, E::F32, E::F32, R::TF32>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                               Carray, ldc, batchCount);
+            if (computeType == ACLBLAS_COMPUTE_32F_FAST_TF32)  // tcgen05 tensor cores, TF32 operands
+                err = gemm_tc_launch(st, ta, tb, m, n, k, a, reinterpret_cast<const float* const*>(Aarray), 0, lda,
+                                     reinterpret_cast<const float* const*>(Barray), 0, ldb, b,
+                                     reinterpret_cast<float* const*>(Carray), 0, ldc, batchCount, 0);
             else if (computeType == ACLBLAS_COMPUTE_32F_FAST_16BF)
                 err = run_gemm<E::F32, E::F32, E::F32, R::BF16>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
                                                                Carray, ldc, batchCount);

@@ -141,6 +141,7 @@ getrf_large_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __res
                 w = c;
                 break;
             }
+            __syncthreads();  // every thread has read pv before the pivot row moves
             if (p != k && tid < kLgPB) {
                 const float t = pb_s[(k - k0) * kLgPS + tid];
                 pb_s[(k - k0) * kLgPS + tid] = pb_s[(p - k0) * kLgPS + tid];

@@ -28,6 +28,7 @@ getrs_generic_kernel(const float* const* __restrict__ Aarray, int n, int lda, co
     const long long m = blockIdx.x;
     const float* A = Aarray[m];
     float* B = Barray[m];
+    if (B == nullptr) return;  // a NULL right-hand side skips the matrix
     const int* p = ipiv ? ipiv + m * n : nullptr;
     const int tid = threadIdx.x;
     __shared__ float sx[256];

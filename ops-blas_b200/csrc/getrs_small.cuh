@@ -25,7 +25,7 @@ getrs_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* 
     const int seg = lane / S::SEG;
     const int r = lane % S::SEG;
     const long long m = ((long long)blockIdx.x * kSmallWarps + warp) * S::MPW + seg;
-    const bool mvalid = m < batch;
+    const bool mvalid = m < batch && Barray[m] != nullptr;  // a NULL right-hand side skips the matrix
     const bool rvalid = mvalid && r < N;
 
     const float* A = mvalid ? Aarray[m] : nullptr;
@@ -114,7 +114,7 @@ getrs_rhs_kernel(const float* const* __restrict__ Aarray, int lda, const int* __
     const int seg = lane / LPM;
     const int q = lane % LPM;
     const long long m = ((long long)blockIdx.x * R::WARPS + warp) * R::MPW + seg;
-    const bool mvalid = m < batch;
+    const bool mvalid = m < batch && Barray[m] != nullptr;  // a NULL right-hand side skips the matrix
     float* wbase = dsm + warp * R::WARP_WORDS;
     float* sm = wbase + seg * R::SLOT;
     int* pv = reinterpret_cast<int*>(sm + R::MAT);

@@ -41,12 +41,21 @@ aclblasStatus_t launch_status(const char* api, cudaError_t err);
 inline int max1(int n) { return n > 1 ? n : 1; }
 
 // Validation-free launchers shared by the entry points (getrs.cu, gemm_batched_ex.cu).
+// getrs_launch skips every matrix whose Barray entry is NULL (the refinement's correction solves
+// pass NULL for converged matrices).
 cudaError_t getrs_launch(cudaStream_t st, bool trans, int n, int nrhs, const float* const* Aarray, int lda,
                          const int* devIpiv, float* const* Barray, int ldb, int batchCount);
 // C = alpha * op(A) * op(B) + beta * C, FP32 operands; round: 0 none, 1 TF32, 2 BF16.
 cudaError_t gemm_f32_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                             const float* const* A, int lda, const float* const* B, int ldb, float beta,
                             float* const* C, int ldc, int batch, int round);
+
+// gemm_tc.cu: C = alpha * op(A) * op(B) + beta * C on the tcgen05 tensor cores (TF32 operands;
+// split = 1 adds the low-part products for about FP32 accuracy). *_off are element offsets added
+// to every matrix pointer.
+cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
+                           const float* const* A, long long a_off, int lda, const float* const* B, long long b_off,
+                           int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split);
 
 // getrf_large.cu: 32 < n <= 640, matrix in global memory; mode 0 plain FP32 (reference
 // operation order), 1 = TF32 split trailing update, 2 = BF16 split trailing update.

@@ -39,11 +39,13 @@ constexpr int kResThreads = 256;
 constexpr int kResMaxRhs = 16;  // right-hand sides per pass
 
 // One CTA per matrix. FP64 residual r = b - A x and normwise backward error; on the last check
-// (final != 0) only the error is recorded. d receives r in FP32 (or zeros when converged).
+// (final != 0) only the error is recorded. d receives r in FP32; Dact[m] is set to d, or to NULL
+// when the matrix has converged, so that the correction solve and update skip it.
 __global__ void __launch_bounds__(kResThreads)
 refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, const float* const* Barray, int ldb,
-                       const float* const* Xarray, int ldx, float* const* Darray, int ldd, double tol, int it,
-                       int final_check, int* __restrict__ done, double* __restrict__ berr, int* __restrict__ iters)
+                       const float* const* Xarray, int ldx, float* const* Darray, int ldd, float** Dact, double tol,
+                       int it, int final_check, int* __restrict__ done, double* __restrict__ berr,
+                       int* __restrict__ iters)
 {
     extern __shared__ double xs[];  // [n][kResMaxRhs]
     __shared__ double red[kResThreads / 32];
@@ -57,7 +59,7 @@ refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, con
     const int tid = threadIdx.x;
     const bool was_done = done[m] != 0;
     if (was_done && !final_check) {
-        for (long long e = tid; e < (long long)n * nrhs; e += kResThreads) D[e % n + (e / n) * ldd] = 0.0f;
+        if (tid == 0) Dact[m] = nullptr;  // no correction for a converged matrix
         return;
     }
     auto block_max = [&](double v) {
@@ -134,16 +136,14 @@ refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, con
             iters[m] = it;
         }
         if (conv && !final_check) done[m] = 1;
-    }
-    if (conv && !final_check) {
-        __syncthreads();
-        for (long long e = tid; e < (long long)n * nrhs; e += kResThreads) D[e % n + (e / n) * ldd] = 0.0f;
+        if (!final_check) Dact[m] = conv ? nullptr : D;
     }
 }
 
 __global__ void axpy_batched_kernel(int n, int nrhs, const float* const* Darray, int ldd, float* const* Xarray, int ldx)
 {
-    const float* D = Darray[blockIdx.x];  // one CTA per matrix
+    const float* D = Darray[blockIdx.x];  // one CTA per matrix; NULL: converged, nothing to add
+    if (D == nullptr) return;
     float* X = Xarray[blockIdx.x];
     for (long long e = threadIdx.x; e < (long long)n * nrhs; e += blockDim.x) {
         const long long i = e % n, c = e / n;
@@ -194,9 +194,9 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
         log_error(kApi, "array arguments must not be nullptr");
         return ACLBLAS_STATUS_INVALID_VALUE;
     }
-    // workspace: correction block D (n x nrhs per matrix), its pointer array, done flags
+    // workspace: correction block D (n x nrhs per matrix), its two pointer arrays, done flags
     const size_t dbytes = ((size_t)n * nrhs * 4 + 255) / 256 * 256;
-    const size_t need = dbytes * batchCount + (size_t)batchCount * 8 + (size_t)batchCount * 4 + 512;
+    const size_t need = dbytes * batchCount + (size_t)batchCount * 16 + (size_t)batchCount * 4 + 512;
     if (handle->workspace_size < need) {
         log_error(kApi, "workspace required %zu bytes, but only %zu available; call aclblasSetWorkspace", need,
                   handle->workspace_size);
@@ -205,7 +205,8 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     char* ws = static_cast<char*>(handle->workspace);
     float* dbase = reinterpret_cast<float*>(ws);
     float** dptr = reinterpret_cast<float**>(ws + dbytes * batchCount);
-    int* done = reinterpret_cast<int*>(reinterpret_cast<char*>(dptr) + (size_t)batchCount * 8);
+    float** dact = dptr + batchCount;  // dptr, or NULL for converged matrices
+    int* done = reinterpret_cast<int*>(reinterpret_cast<char*>(dact) + (size_t)batchCount * 8);
     cudaStream_t st = handle->stream;
     const unsigned bgrid = (unsigned)((batchCount + 255) / 256 < 4096 ? (batchCount + 255) / 256 : 4096);
 
@@ -239,13 +240,13 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     }
     for (int it = 0; it < maxIter; it++) {
         refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
-            n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, it, 0, done, berrArray, iterArray);
-        err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, dptr, n, batchCount);
+            n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, dact, tol, it, 0, done, berrArray, iterArray);
+        err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, dact, n, batchCount);
         if (err != cudaSuccess) return launch_status(kApi, err);
-        axpy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(n, nrhs, dptr, n, Xarray, ldx);
+        axpy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(n, nrhs, dact, n, Xarray, ldx);
     }
     refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
-        n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, maxIter, 1, done, berrArray, iterArray);
+        n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, dact, tol, maxIter, 1, done, berrArray, iterArray);
     return launch_status(kApi, cudaGetLastError());
 }
 
@@ -340,18 +341,18 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
         log_error(kApi, "array arguments must not be nullptr");
         return ACLBLAS_STATUS_INVALID_VALUE;
     }
-    // scratch: correction block D (n x nrhs per matrix, 256-byte rounded), its pointer array, flags
+    // scratch: correction block D (n x nrhs per matrix, 256-byte rounded), its two pointer arrays, flags
     const size_t cap = kRefineStaticScratchBytes;
     if ((size_t)n * (size_t)nrhs > cap / 4) {
         log_error(kApi, "n*nrhs=%zu needs more than the %zu bytes of static scratch", (size_t)n * nrhs, cap);
         return ACLBLAS_STATUS_INVALID_VALUE;
     }
     const size_t dbytes = ((size_t)n * nrhs * 4 + 255) / 256 * 256;
-    if ((size_t)batchCount > (cap - 512) / (dbytes + 12)) {
+    if ((size_t)batchCount > (cap - 512) / (dbytes + 20)) {
         log_error(kApi,
                   "scratch required %zu bytes, but the static scratch holds %zu; split the batch or use "
                   "aclblasSgetrfsRefineBatchedEx with a workspace",
-                  (dbytes + 12) * (size_t)batchCount + 512, cap);
+                  (dbytes + 20) * (size_t)batchCount + 512, cap);
         return ACLBLAS_STATUS_INVALID_VALUE;
     }
     const size_t rsm = (size_t)n * kResMaxRhs * 8;
@@ -372,7 +373,8 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
 
     float* dbase = reinterpret_cast<float*>(ws);
     float** dptr = reinterpret_cast<float**>(ws + dbytes * batchCount);
-    int* done = reinterpret_cast<int*>(reinterpret_cast<char*>(dptr) + (size_t)batchCount * 8);
+    float** dact = dptr + batchCount;  // dptr, or NULL for converged matrices
+    int* done = reinterpret_cast<int*>(reinterpret_cast<char*>(dact) + (size_t)batchCount * 8);
     cudaStream_t st = handle->stream;
     const unsigned bgrid = (unsigned)((batchCount + 255) / 256 < 4096 ? (batchCount + 255) / 256 : 4096);
 
@@ -394,12 +396,12 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
     if (err != cudaSuccess) return launch_status(kApi, err);
     for (int it = 0; it < maxIter; it++) {
         refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
-            n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, it, 0, done, berrArray, iterArray);
-        err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, dptr, n, batchCount);
+            n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, dact, tol, it, 0, done, berrArray, iterArray);
+        err = getrs_launch(st, false, n, nrhs, LUarray, ldlu, PivotArray, dact, n, batchCount);
         if (err != cudaSuccess) return launch_status(kApi, err);
-        axpy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(n, nrhs, dptr, n, Xarray, ldx);
+        axpy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(n, nrhs, dact, n, Xarray, ldx);
     }
     refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
-        n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, tol, maxIter, 1, done, berrArray, iterArray);
+        n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, dact, tol, maxIter, 1, done, berrArray, iterArray);
     return launch_status(kApi, cudaGetLastError());
 }

@@ -44,7 +44,7 @@ def _static_call(ob, handle, A, B, n, nrhs, compute, max_iter, tol):
 def test_oversize_request_is_rejected(ob, handle):
     """A batch whose scratch exceeds the static array fails before any launch."""
     n, nrhs = 64, 64
-    per = ((n * nrhs * 4 + 255) // 256) * 256 + 12
+    per = ((n * nrhs * 4 + 255) // 256) * 256 + 20
     batch = (8 << 20) // per + 1
     P = C.c_void_p(0x1000)  # never dereferenced: the size check comes first
     st = ob.lib().aclblasSgetrfsRefineBatchedStaticScratch(
