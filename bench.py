@@ -201,6 +201,153 @@ def run_reference_arm(args, rank):
     return line
 
 
+def _events_ms(fn, reps, prep=None):
+    """Median device time (ms) of fn() over reps runs, prep() outside the timed region."""
+    import torch
+
+    ts = []
+    for r in range(reps + 1):
+        if prep:
+            prep()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        if r:
+            ts.append(e0.elapsed_time(e1))
+    return statistics.median(ts)
+
+
+def _fp64_berr(A, X, B):
+    """max over matrices and columns of ||b - A x||inf / (||A||inf ||x||inf + ||b||inf), FP64 on the GPU;
+    A (batch, n, n), X/B (batch, nrhs, n) in the column-major batch convention."""
+    a = A.double().transpose(1, 2)
+    x = X.double().transpose(1, 2)
+    b = B.double().transpose(1, 2)
+    r = b - a @ x
+    an = a.abs().sum(2).amax(1)
+    return float((r.abs().amax(1) / (an[:, None] * x.abs().amax(1) + b.abs().amax(1))).amax())
+
+
+def section_grouped(ob, h, dev, peak, reps=5):
+    """Configuration 3: 50000 instances, n ~ U{4..128}, nrhs = 1, one persistent launch (direct and
+    replayed from a CUDA graph) against the plain path (per-n getrf + getrs launches)."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(0)
+    nv = rng.integers(4, 129, size=50000)
+    ns = sorted(set(int(v) for v in nv), reverse=True)
+    sizes = [int((nv == n).sum()) for n in ns]
+    nrhss = [1] * len(ns)
+    a_offs, a_tot = ob.grouped_offsets(ns, ns, ns, sizes)
+    b_offs, b_tot = ob.grouped_offsets(ns, nrhss, ns, sizes)
+    g = torch.Generator(device=dev).manual_seed(3)
+    A0 = torch.randn(a_tot, device=dev, generator=g)
+    B0 = torch.randn(b_tot, device=dev, generator=g)
+    A, B = A0.clone(), B0.clone()
+    ap, bp = ob.slab_ptrs(A, a_offs), ob.slab_ptrs(B, b_offs)
+    piv = torch.empty(sum(n * s for n, s in zip(ns, sizes)), dtype=torch.int32, device=dev)
+    info = torch.empty(sum(sizes), dtype=torch.int32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    hs = ob.Handle(stream=s)
+    plan = ob.GroupedPlan(hs, ns, nrhss, sizes)
+    prep = lambda: (A.copy_(A0), B.copy_(B0))
+    with torch.cuda.stream(s):
+        t_grp = _events_ms(lambda: plan.run(hs, ap, piv, info, bp), reps, prep)
+        assert int(info.max()) == 0
+        t_plain = _events_ms(lambda: ob.grouped_plain(hs, ns, nrhss, sizes, ns, ns, ap, piv, info, bp), reps, prep)
+        graph = torch.cuda.CUDAGraph()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(graph, stream=s):
+            plan.run(hs, ap, piv, info, bp)
+        t_graph = _events_ms(graph.replay, reps, prep)
+    del graph
+    plan.close()
+    hs.close()
+    total = sum(sizes)
+    alg = sum(sz * (12 * n * n + 16 * n + 28) for n, sz in zip(ns, sizes))
+    return {"workload": "grouped_50000_n4-128_nrhs1", "instances": total,
+            "grouped_matrices_s": total / (t_grp * 1e-3), "grouped_graph_matrices_s": total / (t_graph * 1e-3),
+            "plain_matrices_s": total / (t_plain * 1e-3), "speedup_vs_plain": t_plain / min(t_grp, t_graph),
+            "ms": {"grouped": t_grp, "grouped_graph": t_graph, "plain": t_plain},
+            "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved_GB_s": alg / (min(t_grp, t_graph) * 1e-3) / 1e9,
+                         "frac": alg / (min(t_grp, t_graph) * 1e-3) / 1e9 / peak},
+            "plain_path": "per-n aclblasSgetrfBatched + aclblasSgetrsBatched"}
+
+def section_mixed(ob, h, dev, reps=3):
+    """Configuration 4: kappa = 1e4 (A = Q1 diag(logspace(0,4)) Q2^T in FP64, stored FP32), B ~ N(0,1),
+    nrhs = 16. Plain FP32 getrf + getrs against factor + solve + FP64-residual refinement with the
+    TF32 and BF16 split trailing updates; every result's backward error is measured in FP64."""
+    import torch
+
+    out = {}
+    for n, batch in ((256, 2048), (512, 256)):
+        g = torch.Generator(device=dev).manual_seed(n)
+        q1, _ = torch.linalg.qr(torch.randn(batch, n, n, device=dev, dtype=torch.float64, generator=g))
+        q2, _ = torch.linalg.qr(torch.randn(batch, n, n, device=dev, dtype=torch.float64, generator=g))
+        sv = torch.logspace(0, 4, n, device=dev, dtype=torch.float64)
+        A32 = ((q1 * sv) @ q2.transpose(1, 2)).transpose(1, 2).contiguous().float()
+        del q1, q2
+        B = torch.randn(batch, 16, n, device=dev, generator=g)
+        LU, X = torch.empty_like(A32), torch.empty_like(B)
+        pa, px = ob.ptr_array(LU), ob.ptr_array(X)
+        piv = torch.empty((batch, n), dtype=torch.int32, device=dev)
+        info = torch.empty(batch, dtype=torch.int32, device=dev)
+
+        def plain():
+            LU.copy_(A32)
+            X.copy_(B)
+            h.getrf(LU, n, n, piv=piv, info=info, aptr=pa)
+            h.getrs("N", LU, n, n, piv, X, 16, n, aptr=pa, bptr=px)
+
+        t_plain = _events_ms(plain, reps)
+        res = {"plain": {"matrices_s": batch / (t_plain * 1e-3), "ms": t_plain, "berr_max": _fp64_berr(A32, X, B)}}
+        for name, comp in (("tf32", ob.COMPUTE_32F_FAST_TF32), ("bf16", ob.COMPUTE_32F_FAST_16BF)):
+            box = {}
+            t = _events_ms(lambda: box.update(r=h.refine(A32, B, n, 16, compute=comp, max_iter=10, tol=1e-6)), reps)
+            Xm, _, _, _, _, it = box["r"]
+            res[name] = {"matrices_s": batch / (t * 1e-3), "ms": t, "berr_max": _fp64_berr(A32, Xm, B),
+                         "iters_max": int(it.max()), "vs_plain": t_plain / t}
+        out[f"n{n}_b{batch}"] = res
+        del A32, B, LU, X
+        torch.cuda.empty_cache()
+    return out
+
+
+def section_adjoint(ob, h, dev, reps=3):
+    """Configuration 5: X = A^{-1} B with A = G + 8 I, n = 64, nrhs = 8, 65536 matrices; forward
+    getrf + getrs and the adjoint (dB = A^{-T} dX by the transposed solve on the stored factors,
+    dA = -dB X^T by the batched GEMM)."""
+    import torch
+
+    n, nrhs, batch = 64, 8, 65536
+    g = torch.Generator(device=dev).manual_seed(5)
+    A = torch.randn(batch, n, n, device=dev, generator=g) + 8 * torch.eye(n, device=dev)
+    B = torch.randn(batch, nrhs, n, device=dev, generator=g)
+    dX0 = torch.randn(batch, nrhs, n, device=dev, generator=g)
+    LU, X, dX, dA = torch.empty_like(A), torch.empty_like(B), torch.empty_like(dX0), torch.empty_like(A)
+    pa, px = ob.ptr_array(LU), ob.ptr_array(X)
+    piv = torch.empty((batch, n), dtype=torch.int32, device=dev)
+    info = torch.empty(batch, dtype=torch.int32, device=dev)
+
+    def fwd():
+        LU.copy_(A)
+        X.copy_(B)
+        h.getrf(LU, n, n, piv=piv, info=info, aptr=pa)
+        h.getrs("N", LU, n, n, piv, X, nrhs, n, aptr=pa, bptr=px)
+
+    def bwd():
+        dX.copy_(dX0)
+        h.adjoint(LU, n, n, piv, X, n, dX, n, dA, n)
+
+    t_f = _events_ms(fwd, reps)
+    t_b = _events_ms(bwd, reps)
+    return {"workload": "adjoint_n64_nrhs8_b65536", "forward_matrices_s": batch / (t_f * 1e-3),
+            "backward_matrices_s": batch / (t_b * 1e-3), "fwd_bwd_matrices_s": batch / ((t_f + t_b) * 1e-3),
+            "ms": {"forward": t_f, "backward": t_b}}
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -209,6 +356,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sections", action="store_true", help="skip the grouped / mixed / adjoint measurements")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("OPSBLAS_BENCH_ALLOW_SHORT"), \
         "at least 3 warm-up steps"
@@ -365,6 +513,9 @@ def main():
             "gpu_launches": 3 * args.steps,
             "clocks": clocks.summary(),
         }
+        if world == 1 and not args.no_sections:
+            line["sections"] = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
+                                "adjoint": section_adjoint(ob, h, dev)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline()

@@ -1,0 +1,177 @@
+// aclblasSgetrsBatched, trans N, n > 32: one CTA per matrix, blocked substitution with the
+// right-hand sides resident in shared memory.
+//
+// The reference solve (sgetrs_batched_kernel.cpp:83-200) is laswp, then the unit-L forward sweep
+// x_i -= L(i,j) x_j for j = 0..n-1, then the U backward sweep x_j /= U(j,j), x_i -= U(i,j) x_j
+// for j = n-1..0. Every element x_i receives its updates in j order, so the sweeps can be blocked
+// by 32 rows without changing a bit:
+//   * interchanges: the swap sequence is applied to an index array once, then B is gathered;
+//   * forward, per 32-row block: the diagonal block is solved by warps (one right-hand side per
+//     warp at a time, lane = row, shuffles), then every row below subtracts the block's
+//     contributions in j order (one thread per row, 16 right-hand sides in registers);
+//   * backward, per block from the bottom: diagonal solve with true division, then the rows above
+//     subtract the block's contributions in descending j order.
+// Right-hand sides are processed 16 at a time.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace opsblas {
+
+constexpr int kBsThreads = 256;
+constexpr int kBsRC = 16;  // right-hand sides per pass
+constexpr int kBsB = 32;   // block rows
+constexpr int kBsLd = 33;  // padded row stride of the staged diagonal block
+
+size_t getrs_blk_smem(int n) { return (size_t)n * kBsRC * 4 + kBsB * kBsLd * 4 + (size_t)n * 4 * 2 + 16; }
+
+__global__ void __launch_bounds__(kBsThreads)
+getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const int* __restrict__ ipiv,
+                 float* const* __restrict__ Barray, int ldb, int nrhs)
+{
+    extern __shared__ __align__(16) float sm[];
+    float* xs = sm;                                          // [n][kBsRC]
+    float* blk = xs + (size_t)n * kBsRC;                     // [kBsB][kBsLd]: blk[j * kBsLd + i]
+    int* perm = reinterpret_cast<int*>(blk + kBsB * kBsLd);  // [n]: source row of position i
+    int* pv = perm + n;                                      // [n]: pivots
+    const long long m = blockIdx.x;
+    float* B = Barray[m];
+    if (B == nullptr) return;  // a NULL right-hand side skips the matrix
+    const float* A = Aarray[m];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    auto at = [&](int i, int j) { return A[i + (long long)j * lda]; };
+
+    // ---- interchanges (sgetrs_batched_kernel.cpp:94-100: out-of-range or zero pivots skipped) ----
+    for (int i = tid; i < n; i += kBsThreads) {
+        perm[i] = i;
+        pv[i] = ipiv ? ipiv[m * n + i] - 1 : i;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int k = 0; k < n; k++) {
+            const int p = pv[k];
+            if ((unsigned)p < (unsigned)n && p != k) {
+                const int t = perm[k];
+                perm[k] = perm[p];
+                perm[p] = t;
+            }
+        }
+    }
+    __syncthreads();
+
+    for (int c0 = 0; c0 < nrhs; c0 += kBsRC) {
+        const int cw = min(kBsRC, nrhs - c0);
+        for (int e = tid; e < n * kBsRC; e += kBsThreads) {
+            const int i = e % n, c = e / n;
+            xs[i * kBsRC + c] = c < cw ? B[perm[i] + (long long)(c0 + c) * ldb] : 0.0f;
+        }
+        __syncthreads();
+
+        // ------------------------------------------------------------ forward, unit L --
+        for (int r0 = 0; r0 < n; r0 += kBsB) {
+            const int bs = min(kBsB, n - r0);
+            for (int e = tid; e < kBsB * kBsB; e += kBsThreads) {
+                const int j = e / kBsB, i = e % kBsB;
+                blk[j * kBsLd + i] = (i < bs && j < bs) ? at(r0 + i, r0 + j) : 0.0f;
+            }
+            __syncthreads();
+            for (int c = warp; c < cw; c += kBsThreads / 32) {
+                float y = lane < bs ? xs[(r0 + lane) * kBsRC + c] : 0.0f;
+                for (int j = 0; j < bs; j++) {
+                    const float yj = __shfl_sync(0xffffffffu, y, j);
+                    if (lane > j && lane < bs) y = fmaf(-blk[j * kBsLd + lane], yj, y);
+                }
+                if (lane < bs) xs[(r0 + lane) * kBsRC + c] = y;
+            }
+            __syncthreads();
+            for (int i = r0 + bs + tid; i < n; i += kBsThreads) {
+                float4 acc[kBsRC / 4];
+#pragma unroll
+                for (int q = 0; q < kBsRC / 4; q++) acc[q] = reinterpret_cast<const float4*>(xs + i * kBsRC)[q];
+                for (int j = 0; j < bs; j++) {
+                    const float nl = -at(i, r0 + j);
+#pragma unroll
+                    for (int q = 0; q < kBsRC / 4; q++) {
+                        const float4 xj = reinterpret_cast<const float4*>(xs + (r0 + j) * kBsRC)[q];
+                        acc[q].x = fmaf(nl, xj.x, acc[q].x);
+                        acc[q].y = fmaf(nl, xj.y, acc[q].y);
+                        acc[q].z = fmaf(nl, xj.z, acc[q].z);
+                        acc[q].w = fmaf(nl, xj.w, acc[q].w);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kBsRC / 4; q++) reinterpret_cast<float4*>(xs + i * kBsRC)[q] = acc[q];
+            }
+            __syncthreads();
+        }
+
+        // ---------------------------------------------------------------- backward, U --
+        const int nblk = (n + kBsB - 1) / kBsB;
+        for (int kb = nblk - 1; kb >= 0; kb--) {
+            const int r0 = kb * kBsB;
+            const int bs = min(kBsB, n - r0);
+            for (int e = tid; e < kBsB * kBsB; e += kBsThreads) {
+                const int j = e / kBsB, i = e % kBsB;
+                blk[j * kBsLd + i] = (i < bs && j < bs) ? at(r0 + i, r0 + j) : 0.0f;
+            }
+            __syncthreads();
+            for (int c = warp; c < cw; c += kBsThreads / 32) {
+                float y = lane < bs ? xs[(r0 + lane) * kBsRC + c] : 0.0f;
+                for (int j = bs - 1; j >= 0; j--) {
+                    const float t = (lane == j) ? y / blk[j * kBsLd + j] : 0.0f;
+                    const float xj = __shfl_sync(0xffffffffu, t, j);
+                    if (lane == j)
+                        y = xj;
+                    else if (lane < j)
+                        y = fmaf(-blk[j * kBsLd + lane], xj, y);
+                }
+                if (lane < bs) xs[(r0 + lane) * kBsRC + c] = y;
+            }
+            __syncthreads();
+            for (int i = tid; i < r0; i += kBsThreads) {
+                float4 acc[kBsRC / 4];
+#pragma unroll
+                for (int q = 0; q < kBsRC / 4; q++) acc[q] = reinterpret_cast<const float4*>(xs + i * kBsRC)[q];
+                for (int j = bs - 1; j >= 0; j--) {
+                    const float nu = -at(i, r0 + j);
+#pragma unroll
+                    for (int q = 0; q < kBsRC / 4; q++) {
+                        const float4 xj = reinterpret_cast<const float4*>(xs + (r0 + j) * kBsRC)[q];
+                        acc[q].x = fmaf(nu, xj.x, acc[q].x);
+                        acc[q].y = fmaf(nu, xj.y, acc[q].y);
+                        acc[q].z = fmaf(nu, xj.z, acc[q].z);
+                        acc[q].w = fmaf(nu, xj.w, acc[q].w);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kBsRC / 4; q++) reinterpret_cast<float4*>(xs + i * kBsRC)[q] = acc[q];
+            }
+            __syncthreads();
+        }
+
+        for (int e = tid; e < n * cw; e += kBsThreads) {
+            const int i = e % n, c = e / n;
+            B[i + (long long)(c0 + c) * ldb] = xs[i * kBsRC + c];
+        }
+        __syncthreads();
+    }
+}
+
+bool getrs_blk_supported(int n) { return n > 32 && getrs_blk_smem(n) <= 200 * 1024; }
+
+cudaError_t getrs_blk_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda, const int* ipiv,
+                             float* const* Barray, int ldb, int batch)
+{
+    static int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e = cudaFuncSetAttribute(getrs_blk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        configured_device = dev;
+    }
+    getrs_blk_kernel<<<(unsigned)batch, kBsThreads, getrs_blk_smem(n), st>>>(Aarray, n, lda, ipiv, Barray, ldb, nrhs);
+    return cudaGetLastError();
+}
+
+}  // namespace opsblas

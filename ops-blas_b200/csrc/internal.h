@@ -45,6 +45,10 @@ inline int max1(int n) { return n > 1 ? n : 1; }
 // pass NULL for converged matrices).
 cudaError_t getrs_launch(cudaStream_t st, bool trans, int n, int nrhs, const float* const* Aarray, int lda,
                          const int* devIpiv, float* const* Barray, int ldb, int batchCount);
+// getrs_blk.cu: trans N, n > 32, blocked substitution with the right-hand sides in shared memory.
+bool getrs_blk_supported(int n);
+cudaError_t getrs_blk_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda, const int* ipiv,
+                             float* const* Barray, int ldb, int batch);
 // C = alpha * op(A) * op(B) + beta * C, FP32 operands; round: 0 none, 1 TF32, 2 BF16.
 cudaError_t gemm_f32_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                             const float* const* A, int lda, const float* const* B, int ldb, float beta,
