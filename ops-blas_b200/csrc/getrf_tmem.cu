@@ -1,0 +1,333 @@
+// Mixed-precision batched LU for 32 < n <= 256 with the matrix resident in tensor memory (TMEM).
+//
+// Used by aclblasSgetrfsRefineBatchedEx with ACLBLAS_COMPUTE_32F_FAST_TF32. One CTA of 256 threads
+// per matrix; thread t owns physical row t. TMEM (all 512 columns of the SM) holds the matrix:
+// rows 0..127 in lanes 0..127 at columns 0..255, rows 128..255 in the same lanes at columns
+// 256..511, so warp w reaches its rows 32w..32w+31 through its lane quarter (w % 4). Rows never
+// move; `pos` (the row's index in the reference's in-place matrix) records the interchanges.
+// Per panel of 32 columns k0..k0+31:
+//   1. every thread reads its row's panel columns from TMEM and the CTA factors the panel in FP32
+//      exactly as the reference's unblocked LU does (first-maximum pivot, true division, one fmaf
+//      per update), one CTA barrier per column;
+//   2. the panel goes back to TMEM; the rows that became this panel's pivot rows publish their
+//      unit-lower L11 part, and the rows below publish -L21 split into TF32 high and low parts
+//      in the UMMA shared-memory layout (the MMA's A operand);
+//   3. the pivot rows' trailing entries are read from TMEM, U12 = L11^-1 * A12 is formed in FP32
+//      (one thread per column, reference order) and staged split into TF32 parts as the B operand;
+//      the final U12 rows are written to global memory while the MMAs of step 4 run;
+//   4. one thread issues A22 += (-L21) * U12 as tcgen05.mma (kind::tf32, hi*hi + hi*lo + lo*hi)
+//      accumulating straight into the TMEM-resident trailing matrix, and commits to an mbarrier
+//      that the CTA waits on (bounded) before the next panel reads TMEM.
+// At the end every row is written to global memory at its final position: the columns left of
+// and inside its pivot panel from TMEM, the rest was written in step 3. HBM traffic is one read
+// and one write of the matrix. Rows that are not below a panel get zero A-operand rows, so the MMA
+// leaves them unchanged. On an exactly-zero pivot the factorisation stops (info = column + 1) and
+// the trailing columns keep the state of the last completed panel.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+#include "small_common.cuh"
+#include "tc_common.cuh"
+
+namespace opsblas {
+
+constexpr int kTmThreads = 256;
+constexpr int kTmWarps = kTmThreads / 32;
+constexpr int kTmMaxN = 256;
+constexpr int kTmPB = 32;                // panel width = the MMA's K slice
+constexpr int kTmPart = 128 * kTmPB;     // floats of one 128-row operand part
+constexpr uint32_t kTmWaitLimit = 1u << 24;
+
+__device__ unsigned int g_tmem_lu_timeouts;
+
+struct TmSmem {
+    float a_hi[2][kTmPart];  // -L21, rows of block b (physical rows 128b..), K-major UMMA layout
+    float a_lo[2][kTmPart];
+    float b_hi[2 * kTmPart];  // U12^T: 256 trailing columns x 32, K-major
+    float b_lo[2 * kTmPart];
+    float u12[kTmPB][kTmMaxN + 1];  // pivot rows' trailing entries, then U12
+    float l11[kTmPB][kTmPB + 1];    // unit-lower L11 of the panel (row = position - k0)
+    float crow[2][kTmWarps][kTmPB]; // per column parity and warp: the warp's pivot candidate row
+    unsigned ckey[2][kTmWarps];     //   its |value| key
+    unsigned cpos[2][kTmWarps];     //   its position
+    int info;
+    uint64_t mbar;
+    uint32_t taddr;
+};
+
+__device__ __forceinline__ int tm_off(int r, int k)
+{
+    return (r >> 3) * (kTmPB * 8) + (k >> 2) * 32 + (r & 7) * 4 + (k & 3);
+}
+
+// Factors the panel held in p (this thread's row, 32 columns). Returns false when a zero pivot
+// stopped the factorisation (S.info set). One CTA barrier per column: every warp publishes its
+// best candidate (key, position and the whole panel row), double buffered by column parity, and
+// after the barrier every thread picks the same winner and reads the pivot row from there.
+__device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid, int n, int k0, int* pm, TmSmem& S,
+                                         int tid, int warp, int lane)
+{
+#pragma unroll
+    for (int c = 0; c < kTmPB; c++) {
+        const int k = k0 + c;
+        if (k >= n) break;
+        const int buf = c & 1;
+        // first maximum of |a(., k)| over the rows at positions >= k; ties to the lowest position
+        const bool elig = valid && pos >= k;
+        const float av = fabsf(p[c]);
+        const unsigned key = (elig && av > 0.0f) ? __float_as_uint(av) : 0u;
+        const unsigned wkey = __reduce_max_sync(0xffffffffu, key);
+        const unsigned wpos = __reduce_min_sync(0xffffffffu, (elig && key == wkey) ? (unsigned)pos : 0xffffffffu);
+        if (lane == 0) {
+            S.ckey[buf][warp] = wkey;
+            S.cpos[buf][warp] = wpos;
+        }
+        if (elig && (unsigned)pos == wpos) {
+            float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
+#pragma unroll
+            for (int q = 0; q < kTmPB / 4; q++) dst[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
+        }
+        __syncthreads();
+        unsigned bk = S.ckey[buf][0], bp = S.cpos[buf][0];
+        int bw = 0;
+#pragma unroll
+        for (int q = 1; q < kTmWarps; q++) {
+            const unsigned qk = S.ckey[buf][q], qp = S.cpos[buf][q];
+            if (qk > bk || (qk == bk && qp < bp)) {
+                bk = qk;
+                bp = qp;
+                bw = q;
+            }
+        }
+        const int ppos = (int)bp;
+        const float* prow = S.crow[buf][bw];
+        const float pv = prow[c];
+        if (tid == 0 && pm) pm[k] = ppos + 1;
+        if (pv == 0.0f) {
+            if (tid == 0) S.info = k + 1;
+            return false;
+        }
+        if (pos == ppos)
+            pos = k;
+        else if (pos == k)
+            pos = ppos;
+        if (valid && pos > k) {
+            const float l = p[c] / pv;
+            p[c] = l;
+#pragma unroll
+            for (int cc = c + 1; cc < kTmPB; cc++) p[cc] = fmaf(-l, prow[cc], p[cc]);
+        }
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kTmThreads, 1)
+getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* __restrict__ LUarr, int n, int ldlu,
+                  int* __restrict__ piv, int* __restrict__ info)
+{
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    TmSmem& S = *reinterpret_cast<TmSmem*>(smraw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long m = blockIdx.x;
+    const float* A = Ain[m];
+    float* LU = LUarr[m];
+    int* pm = piv ? piv + m * n : nullptr;
+    const int row = tid;  // physical row
+    const bool valid = row < n;
+
+    if (warp == 0) {
+        tmem_alloc(&S.taddr, 512);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(&S.mbar, 1);
+        fence_mbar_init();
+        S.info = 0;
+    }
+    if (pm)
+        for (int i = tid; i < n; i += kTmThreads) pm[i] = 0;
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const uint32_t tbase = S.taddr;
+    // this thread's row at column 0: lane quarter of the warp, column half of the row block
+    const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((row >> 7) * 256);
+
+    // ---- load: the whole row block, zeros outside the matrix ----
+    for (int j0 = 0; j0 < kTmMaxN; j0 += 16) {
+        float v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const int j = j0 + i;
+            v[i] = (valid && j < n) ? A[row + (long long)j * lda] : 0.0f;
+        }
+        tmem_st16(trow + j0, v);
+    }
+    tmem_wait_st();
+
+    int pos = row;
+    int upanel = -1;  // first column of the panel in which this row became a pivot row
+    uint32_t phase = 0;
+    for (int k0 = 0; k0 < n; k0 += kTmPB) {
+        // ---- 1. panel ----
+        float p[kTmPB];
+        {
+            float v[16];
+            tmem_ld16(trow + k0, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++) p[i] = v[i];
+            tmem_ld16(trow + k0 + 16, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++) p[16 + i] = v[i];
+        }
+        const bool go = tm_panel(p, pos, valid, n, k0, pm, S, tid, warp, lane);
+        // ---- 2. panel back to TMEM; L11 and -L21 operands ----
+        {
+            float v[16];
+#pragma unroll
+            for (int i = 0; i < 16; i++) v[i] = p[i];
+            tmem_st16(trow + k0, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++) v[i] = p[16 + i];
+            tmem_st16(trow + k0 + 16, v);
+            tmem_wait_st();
+        }
+        if (!go) break;  // zero pivot (uniform)
+        const int kend = min(k0 + kTmPB, n);
+        const int j0 = k0 + kTmPB;
+        const int rest = n - j0;
+        const bool pivot_row = valid && pos >= k0 && pos < kend;
+        if (pivot_row) {
+            upanel = k0;
+#pragma unroll
+            for (int cc = 0; cc < kTmPB; cc++) S.l11[pos - k0][cc] = p[cc];
+        }
+        if (rest <= 0) break;
+        {
+            const int b = row >> 7, r = row & 127;
+            const bool below = valid && pos >= kend;
+#pragma unroll
+            for (int cc = 0; cc < kTmPB; cc++) {
+                const float x = (below && k0 + cc < n) ? -p[cc] : 0.0f;
+                const float hi = tf32_rne(x);
+                S.a_hi[b][tm_off(r, cc)] = hi;
+                S.a_lo[b][tm_off(r, cc)] = tf32_rne(x - hi);
+            }
+        }
+        __syncthreads();
+        // ---- 3. U12 = L11^-1 * A12 ----
+        for (int jc = j0; jc < n; jc += 16) {
+            float v[16];
+            tmem_ld16(trow + jc, v);
+            if (pivot_row) {
+#pragma unroll
+                for (int i = 0; i < 16; i++)
+                    if (jc + i < n) S.u12[pos - k0][jc - j0 + i] = v[i];
+            }
+        }
+        __syncthreads();
+        const int nr = kend - k0;  // pivot rows of this panel
+        const int npad = (rest + 15) & ~15;
+        for (int jj = tid; jj < npad; jj += kTmThreads) {
+            float u[kTmPB];
+#pragma unroll
+            for (int r = 0; r < kTmPB; r++) u[r] = (jj < rest && r < nr) ? S.u12[r][jj] : 0.0f;
+#pragma unroll
+            for (int r = 1; r < kTmPB; r++) {
+                if (r < nr) {
+#pragma unroll
+                    for (int mm = 0; mm < r; mm++) u[r] = fmaf(-S.l11[r][mm], u[mm], u[r]);
+                }
+            }
+            if (jj < rest) {
+#pragma unroll
+                for (int r = 0; r < kTmPB; r++) S.u12[r][jj] = u[r];  // written out after the MMA issue
+            }
+#pragma unroll
+            for (int r = 0; r < kTmPB; r++) {
+                const float hi = tf32_rne(u[r]);
+                S.b_hi[tm_off(jj, r)] = hi;
+                S.b_lo[tm_off(jj, r)] = tf32_rne(u[r] - hi);
+            }
+        }
+        fence_async_smem();
+        tc_fence_before_sync();
+        __syncthreads();
+        // ---- 4. A22 += (-L21) * U12 on the tensor cores, into the resident matrix ----
+        if (tid == 0) {
+            tc_fence_after_sync();
+            const uint32_t idesc = umma_idesc(128, npad, 2);
+            const uint32_t sbo = kTmPB * 32;
+            for (int b = 0; b < 2; b++) {
+                if (128 * b >= n) break;
+                const uint32_t d = tbase + (uint32_t)(b * 256 + j0);
+#pragma unroll
+                for (int s = 0; s < kTmPB / 8; s++) {
+                    const uint32_t step = s * 256;
+                    const uint64_t ah = umma_smem_desc(smem_u32(S.a_hi[b]) + step, 128, sbo);
+                    const uint64_t al = umma_smem_desc(smem_u32(S.a_lo[b]) + step, 128, sbo);
+                    const uint64_t bh = umma_smem_desc(smem_u32(S.b_hi) + step, 128, sbo);
+                    const uint64_t bl = umma_smem_desc(smem_u32(S.b_lo) + step, 128, sbo);
+                    umma_tf32(d, ah, bl, idesc, 1);
+                    umma_tf32(d, al, bh, idesc, 1);
+                    umma_tf32(d, ah, bh, idesc, 1);
+                }
+            }
+            umma_commit(&S.mbar);
+        }
+        // the final U12 rows go to global memory while the tensor cores run (coalesced columns)
+        for (int jj = warp; jj < rest; jj += kTmWarps)
+            if (lane < nr) LU[(k0 + lane) + (long long)(j0 + jj) * ldlu] = S.u12[lane][jj];
+        const bool waited = mbar_wait_bounded(&S.mbar, phase, kTmWaitLimit);
+        phase ^= 1u;
+        tc_fence_after_sync();
+        if (__syncthreads_or(!waited)) {
+            if (tid == 0) {
+                atomicAdd(&g_tmem_lu_timeouts, 1u);
+                S.info = -1;
+            }
+            break;
+        }
+    }
+
+    // ---- store: row at its final position; columns right of its pivot panel were written as U12 ----
+    tc_fence_before_sync();
+    __syncthreads();
+    tc_fence_after_sync();
+    const int lim = upanel >= 0 ? upanel + kTmPB : n;
+    for (int jc = 0; jc < n; jc += 16) {
+        float v[16];
+        tmem_ld16(trow + jc, v);
+        if (valid) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int j = jc + i;
+                if (j < n && j < lim) LU[pos + (long long)j * ldlu] = v[i];
+            }
+        }
+    }
+    if (tid == 0 && info != nullptr) info[m] = S.info;
+    tc_fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tbase, 512);
+}
+
+bool getrf_tmem_supported(int n) { return n > 32 && n <= kTmMaxN; }
+
+cudaError_t getrf_tmem_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
+                              int ldlu, int* piv, int* info, int batch)
+{
+    static int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e =
+            cudaFuncSetAttribute(getrf_tmem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TmSmem));
+        if (e != cudaSuccess) return e;
+        configured_device = dev;
+    }
+    getrf_tmem_kernel<<<(unsigned)batch, kTmThreads, sizeof(TmSmem), st>>>(Aarray, lda, LUarray, n, ldlu, piv, info);
+    return cudaGetLastError();
+}
+
+}  // namespace opsblas

@@ -266,3 +266,56 @@ def test_refine_full_occupancy(handle, compute):
     e = (r.abs().amax(1) / (an[:, None] * x64.abs().amax(1) + b64.abs().amax(1))).amax(1)
     assert float(e.max()) <= 1e-6, float(e.max())
     assert int(iters.max()) < 40
+
+
+def _apply_pivots(a, piv):
+    """Rows of a (n x n, math orientation) interchanged as LAPACK laswp with 1-based pivots."""
+    a = a.copy()
+    for k, p in enumerate(piv):
+        p = int(p) - 1
+        if 0 <= p < a.shape[0] and p != k:
+            a[[k, p]] = a[[p, k]]
+    return a
+
+
+@pytest.mark.parametrize("n", [33, 48, 100, 128, 129, 200, 255, 256])
+def test_tmem_mixed_lu_reconstructs(handle, n):
+    """TF32 mode (factors resident in tensor memory, split-TF32 tcgen05 trailing update): the
+    factors reproduce P*A = L*U to near FP32 accuracy in FP64, pivots form a permutation."""
+    import torch
+
+    batch, nrhs = 12, 2
+    A64, a32 = conditioned_batch(n, batch, 1e3, seed=n)
+    b = np.random.default_rng(n).standard_normal((batch, nrhs, n)).astype(np.float32)
+    X, LU, piv, info, berr, iters = handle.refine(to_dev(a32, "cuda"), to_dev(b, "cuda"), n, nrhs,
+                                                  compute=6, max_iter=10, tol=1e-6)
+    torch.cuda.synchronize()
+    assert int(info.max()) == 0 and int(info.min()) == 0
+    lu, pv = to_host(LU), to_host(piv)
+    for q in range(batch):
+        assert sorted(_apply_pivots(np.arange(n)[:, None].astype(float), pv[q])[:, 0].astype(int)) == list(range(n))
+        F = lu[q].T.astype(np.float64)
+        L = np.tril(F, -1) + np.eye(n)
+        U = np.triu(F)
+        PA = _apply_pivots(a32[q].T.astype(np.float64), pv[q])
+        rel = np.linalg.norm(PA - L @ U) / np.linalg.norm(PA)
+        assert rel < 2e-6, (q, rel)
+    assert float(to_host(berr).max()) <= 1e-6
+
+
+def test_tmem_mixed_lu_singular(handle):
+    """A zero column stops the TF32-mode factorisation with info = that column + 1."""
+    import torch
+
+    n, batch = 96, 4
+    rng = np.random.default_rng(9)
+    a = rng.standard_normal((batch, n, n)).astype(np.float32)
+    for q, col in enumerate([0, 31, 32, 77]):
+        a[q, col, :] = 0.0  # column col (column-major batch convention)
+    b = rng.standard_normal((batch, 1, n)).astype(np.float32)
+    X, LU, piv, info, berr, iters = handle.refine(to_dev(a, "cuda"), to_dev(b, "cuda"), n, 1, compute=6,
+                                                  max_iter=2, tol=1e-6)
+    torch.cuda.synchronize()
+    inf = to_host(info)
+    assert inf[0] == 1 and inf[1] >= 1 and inf[2] >= 1 and inf[3] >= 1
+    assert all(i <= c + 1 for i, c in zip(inf, [0, 31, 32, 77]))
