@@ -230,14 +230,47 @@ def _fp64_berr(A, X, B):
     return float((r.abs().amax(1) / (an[:, None] * x.abs().amax(1) + b.abs().amax(1))).amax())
 
 
-def section_grouped(ob, h, dev, peak, reps=5):
+def cpu_solve_rate(ns, nrhs, seed=7):
+    """Matrices/s of the reference's CPU golden getrf + getrs (trans N) over the orders in ns (one
+    matrix per entry, grouped by order), all host threads; returns (rate, cores, seconds)."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    import oracle as O
+
+    rng = np.random.default_rng(seed)
+    groups = {}
+    for n in ns:
+        groups[n] = groups.get(n, 0) + 1
+    data = [(n, rng.standard_normal((c, n, n)).astype(np.float32), rng.standard_normal((c, nrhs, n)).astype(np.float32))
+            for n, c in groups.items()]
+    t0 = time.perf_counter()
+    for n, a, b in data:
+        piv, _ = O.ref_getrf(a, n, n, True, 0)
+        O.ref_getrs("N", a, n, n, piv, b, nrhs, n, 0)
+    dt = time.perf_counter() - t0
+    return len(ns) / dt, O.ref().ref_max_threads(), dt
+
+
+def cpu_section_baseline(ns, nrhs, what, target_s=3.0):
+    """cpu_solve_rate on a sample sized to about target_s seconds, as a cpu_baseline object."""
+    probe = list(ns[: max(1, min(len(ns), 16))])
+    rate, cores, dt = cpu_solve_rate(probe, nrhs)
+    k = int(max(1, min(len(ns), rate * target_s)))
+    rate, cores, dt = cpu_solve_rate(list(ns[:k]), nrhs)
+    return {"value": rate, "unit": "matrices/s", "cores": cores, "kind": "reference",
+            "sample": f"{k} matrices of {what}: reference golden getrf + getrs(N) (LAPACK through its test headers), "
+                      f"OpenMP over batch chunks, {dt:.1f} s"}
+
+
+def section_grouped(ob, h, dev, peak, reps=5, instances=50000):
     """Configuration 3: 50000 instances, n ~ U{4..128}, nrhs = 1, one persistent launch (direct and
     replayed from a CUDA graph) against the plain path (per-n getrf + getrs launches)."""
     import numpy as np
     import torch
 
     rng = np.random.default_rng(0)
-    nv = rng.integers(4, 129, size=50000)
+    nv = rng.integers(4, 129, size=instances)
     ns = sorted(set(int(v) for v in nv), reverse=True)
     sizes = [int((nv == n).sum()) for n in ns]
     nrhss = [1] * len(ns)
@@ -268,22 +301,24 @@ def section_grouped(ob, h, dev, peak, reps=5):
     hs.close()
     total = sum(sizes)
     alg = sum(sz * (12 * n * n + 16 * n + 28) for n, sz in zip(ns, sizes))
-    return {"workload": "grouped_50000_n4-128_nrhs1", "instances": total,
+    return {"workload": f"grouped_{instances}_n4-128_nrhs1", "instances": total,
             "grouped_matrices_s": total / (t_grp * 1e-3), "grouped_graph_matrices_s": total / (t_graph * 1e-3),
             "plain_matrices_s": total / (t_plain * 1e-3), "speedup_vs_plain": t_plain / min(t_grp, t_graph),
             "ms": {"grouped": t_grp, "grouped_graph": t_graph, "plain": t_plain},
             "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved_GB_s": alg / (min(t_grp, t_graph) * 1e-3) / 1e9,
                          "frac": alg / (min(t_grp, t_graph) * 1e-3) / 1e9 / peak},
-            "plain_path": "per-n aclblasSgetrfBatched + aclblasSgetrsBatched"}
+            "GFLOP_s": sum(sz * (2 * n ** 3 / 3 + 2 * n * n) for n, sz in zip(ns, sizes)) / (min(t_grp, t_graph) * 1e-3) / 1e9,
+            "plain_path": "per-n aclblasSgetrfBatched + aclblasSgetrsBatched",
+            "cpu_baseline": cpu_section_baseline([int(v) for v in nv], 1, "the same n ~ U{4..128} draw, nrhs = 1")}
 
-def section_mixed(ob, h, dev, reps=3):
+def section_mixed(ob, h, dev, reps=3, sizes=((256, 2048), (512, 256))):
     """Configuration 4: kappa = 1e4 (A = Q1 diag(logspace(0,4)) Q2^T in FP64, stored FP32), B ~ N(0,1),
     nrhs = 16. Plain FP32 getrf + getrs against factor + solve + FP64-residual refinement with the
     TF32 and BF16 split trailing updates; every result's backward error is measured in FP64."""
     import torch
 
     out = {}
-    for n, batch in ((256, 2048), (512, 256)):
+    for n, batch in sizes:
         g = torch.Generator(device=dev).manual_seed(n)
         q1, _ = torch.linalg.qr(torch.randn(batch, n, n, device=dev, dtype=torch.float64, generator=g))
         q2, _ = torch.linalg.qr(torch.randn(batch, n, n, device=dev, dtype=torch.float64, generator=g))
@@ -310,19 +345,24 @@ def section_mixed(ob, h, dev, reps=3):
             Xm, _, _, _, _, it = box["r"]
             res[name] = {"matrices_s": batch / (t * 1e-3), "ms": t, "berr_max": _fp64_berr(A32, Xm, B),
                          "iters_max": int(it.max()), "vs_plain": t_plain / t}
+        fl = 2 * n ** 3 / 3 + 2 * n * n * 16
+        for v in res.values():
+            v["GFLOP_s"] = fl * v["matrices_s"] / 1e9
+            v["alg_GB_s"] = (12 * n * n + 8 * n * 16) * v["matrices_s"] / 1e9
+        res["cpu_baseline"] = cpu_section_baseline([n] * batch, 16, f"n = {n}, nrhs = 16, N(0,1)")
         out[f"n{n}_b{batch}"] = res
         del A32, B, LU, X
         torch.cuda.empty_cache()
     return out
 
 
-def section_adjoint(ob, h, dev, reps=3):
+def section_adjoint(ob, h, dev, reps=3, batch=65536):
     """Configuration 5: X = A^{-1} B with A = G + 8 I, n = 64, nrhs = 8, 65536 matrices; forward
     getrf + getrs and the adjoint (dB = A^{-T} dX by the transposed solve on the stored factors,
     dA = -dB X^T by the batched GEMM)."""
     import torch
 
-    n, nrhs, batch = 64, 8, 65536
+    n, nrhs = 64, 8
     g = torch.Generator(device=dev).manual_seed(5)
     A = torch.randn(batch, n, n, device=dev, generator=g) + 8 * torch.eye(n, device=dev)
     B = torch.randn(batch, nrhs, n, device=dev, generator=g)
@@ -344,9 +384,29 @@ def section_adjoint(ob, h, dev, reps=3):
 
     t_f = _events_ms(fwd, reps)
     t_b = _events_ms(bwd, reps)
-    return {"workload": "adjoint_n64_nrhs8_b65536", "forward_matrices_s": batch / (t_f * 1e-3),
+    return {"workload": f"adjoint_n64_nrhs8_b{batch}", "forward_matrices_s": batch / (t_f * 1e-3),
             "backward_matrices_s": batch / (t_b * 1e-3), "fwd_bwd_matrices_s": batch / ((t_f + t_b) * 1e-3),
-            "ms": {"forward": t_f, "backward": t_b}}
+            "ms": {"forward": t_f, "backward": t_b},
+            "GFLOP_s_forward": (2 * n ** 3 / 3 + 2 * n * n * nrhs) * batch / (t_f * 1e-3) / 1e9,
+            "cpu_baseline_forward": cpu_section_baseline([n] * batch, nrhs, "n = 64, nrhs = 8, N(0,1) (the reference has no adjoint)")}
+
+def run_section(args):
+    """One measured section on its own (used for profiling captures with --small)."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    ob = load_package()
+    h = ob.Handle()
+    peak, _ = peaks()
+    if args.section == "grouped":
+        out = section_grouped(ob, h, dev, peak, reps=2, instances=5000 if args.small else 50000)
+    elif args.section == "mixed":
+        out = section_mixed(ob, h, dev, reps=2, sizes=((256, 148), (512, 32)) if args.small else ((256, 2048), (512, 256)))
+    else:
+        out = section_adjoint(ob, h, dev, reps=2, batch=8192 if args.small else 65536)
+    print(json.dumps({"section": args.section, "small": bool(args.small), **out}))
+    h.close()
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -357,6 +417,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sections", action="store_true", help="skip the grouped / mixed / adjoint measurements")
+    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint"],
+                    help="run only this measured section (one JSON line) and exit")
+    ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference" or os.environ.get("OPSBLAS_BENCH_ALLOW_SHORT"), \
         "at least 3 warm-up steps"
@@ -367,6 +430,9 @@ def main():
 
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.section:
+        run_section(args)
         return
 
     import torch

@@ -46,7 +46,7 @@ struct TmSmem {
     float b_hi[2 * kTmPart];  // U12^T: 256 trailing columns x 32, K-major
     float b_lo[2 * kTmPart];
     float u12[kTmPB][kTmMaxN + 1];  // pivot rows' trailing entries, then U12
-    float l11[kTmPB][kTmPB + 1];    // unit-lower L11 of the panel (row = position - k0)
+    float l11[kTmPB][kTmPB];        // unit-lower L11 of the panel (row = position - k0)
     float crow[2][kTmWarps][kTmPB]; // per column parity and warp: the warp's pivot candidate row
     unsigned ckey[2][kTmWarps];     //   its |value| key
     unsigned cpos[2][kTmWarps];     //   its position
@@ -88,17 +88,12 @@ __device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid
             for (int q = 0; q < kTmPB / 4; q++) dst[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
         }
         __syncthreads();
-        unsigned bk = S.ckey[buf][0], bp = S.cpos[buf][0];
-        int bw = 0;
-#pragma unroll
-        for (int q = 1; q < kTmWarps; q++) {
-            const unsigned qk = S.ckey[buf][q], qp = S.cpos[buf][q];
-            if (qk > bk || (qk == bk && qp < bp)) {
-                bk = qk;
-                bp = qp;
-                bw = q;
-            }
-        }
+        // lanes 0..7 each take one warp's candidate; two reductions pick the winner in every warp
+        const unsigned qk = lane < kTmWarps ? S.ckey[buf][lane] : 0u;
+        const unsigned qp = lane < kTmWarps ? S.cpos[buf][lane] : 0xffffffffu;
+        const unsigned bk = __reduce_max_sync(0xffffffffu, qk);
+        const unsigned bp = __reduce_min_sync(0xffffffffu, (lane < kTmWarps && qk == bk) ? qp : 0xffffffffu);
+        const int bw = __ffs(__ballot_sync(0xffffffffu, lane < kTmWarps && qk == bk && qp == bp)) - 1;
         const int ppos = (int)bp;
         const float* prow = S.crow[buf][bw];
         const float pv = prow[c];
@@ -115,7 +110,13 @@ __device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid
             const float l = p[c] / pv;
             p[c] = l;
 #pragma unroll
-            for (int cc = c + 1; cc < kTmPB; cc++) p[cc] = fmaf(-l, prow[cc], p[cc]);
+            for (int q = (c + 1) / 4; q < kTmPB / 4; q++) {
+                const float4 u = reinterpret_cast<const float4*>(prow)[q];
+                const float uu[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    if (4 * q + e > c) p[4 * q + e] = fmaf(-l, uu[e], p[4 * q + e]);
+            }
         }
     }
     return true;
@@ -200,18 +201,25 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
         if (pivot_row) {
             upanel = k0;
 #pragma unroll
-            for (int cc = 0; cc < kTmPB; cc++) S.l11[pos - k0][cc] = p[cc];
+            for (int q = 0; q < kTmPB / 4; q++)
+                reinterpret_cast<float4*>(S.l11[pos - k0])[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2],
+                                                                            p[4 * q + 3]);
         }
         if (rest <= 0) break;
         {
             const int b = row >> 7, r = row & 127;
             const bool below = valid && pos >= kend;
 #pragma unroll
-            for (int cc = 0; cc < kTmPB; cc++) {
-                const float x = (below && k0 + cc < n) ? -p[cc] : 0.0f;
-                const float hi = tf32_rne(x);
-                S.a_hi[b][tm_off(r, cc)] = hi;
-                S.a_lo[b][tm_off(r, cc)] = tf32_rne(x - hi);
+            for (int q = 0; q < kTmPB / 4; q++) {
+                float hi[4], lo[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    const float x = (below && k0 + 4 * q + e < n) ? -p[4 * q + e] : 0.0f;
+                    hi[e] = tf32_cvt(x);
+                    lo[e] = tf32_cvt(x - hi[e]);
+                }
+                *reinterpret_cast<float4*>(&S.a_hi[b][tm_off(r, 4 * q)]) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<float4*>(&S.a_lo[b][tm_off(r, 4 * q)]) = make_float4(lo[0], lo[1], lo[2], lo[3]);
             }
         }
         __syncthreads();
@@ -236,7 +244,13 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
             for (int r = 1; r < kTmPB; r++) {
                 if (r < nr) {
 #pragma unroll
-                    for (int mm = 0; mm < r; mm++) u[r] = fmaf(-S.l11[r][mm], u[mm], u[r]);
+                    for (int q = 0; q < (r + 3) / 4; q++) {
+                        const float4 lv = reinterpret_cast<const float4*>(S.l11[r])[q];
+                        const float ll[4] = {lv.x, lv.y, lv.z, lv.w};
+#pragma unroll
+                        for (int e = 0; e < 4; e++)
+                            if (4 * q + e < r) u[r] = fmaf(-ll[e], u[4 * q + e], u[r]);
+                    }
                 }
             }
             if (jj < rest) {
@@ -244,10 +258,15 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
                 for (int r = 0; r < kTmPB; r++) S.u12[r][jj] = u[r];  // written out after the MMA issue
             }
 #pragma unroll
-            for (int r = 0; r < kTmPB; r++) {
-                const float hi = tf32_rne(u[r]);
-                S.b_hi[tm_off(jj, r)] = hi;
-                S.b_lo[tm_off(jj, r)] = tf32_rne(u[r] - hi);
+            for (int q = 0; q < kTmPB / 4; q++) {
+                float hi[4], lo[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    hi[e] = tf32_cvt(u[4 * q + e]);
+                    lo[e] = tf32_cvt(u[4 * q + e] - hi[e]);
+                }
+                *reinterpret_cast<float4*>(&S.b_hi[tm_off(jj, 4 * q)]) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<float4*>(&S.b_lo[tm_off(jj, 4 * q)]) = make_float4(lo[0], lo[1], lo[2], lo[3]);
             }
         }
         fence_async_smem();

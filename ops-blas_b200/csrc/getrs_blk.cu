@@ -88,15 +88,22 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                 float4 acc[kBsRC / 4];
 #pragma unroll
                 for (int q = 0; q < kBsRC / 4; q++) acc[q] = reinterpret_cast<const float4*>(xs + i * kBsRC)[q];
-                for (int j = 0; j < bs; j++) {
-                    const float nl = -at(i, r0 + j);
+                for (int jb = 0; jb < bs; jb += 8) {
+                    float lv[8];  // eight independent loads in flight
 #pragma unroll
-                    for (int q = 0; q < kBsRC / 4; q++) {
-                        const float4 xj = reinterpret_cast<const float4*>(xs + (r0 + j) * kBsRC)[q];
-                        acc[q].x = fmaf(nl, xj.x, acc[q].x);
-                        acc[q].y = fmaf(nl, xj.y, acc[q].y);
-                        acc[q].z = fmaf(nl, xj.z, acc[q].z);
-                        acc[q].w = fmaf(nl, xj.w, acc[q].w);
+                    for (int u = 0; u < 8; u++) lv[u] = jb + u < bs ? at(i, r0 + jb + u) : 0.0f;
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        if (jb + u >= bs) break;
+                        const float nl = -lv[u];
+#pragma unroll
+                        for (int q = 0; q < kBsRC / 4; q++) {
+                            const float4 xj = reinterpret_cast<const float4*>(xs + (r0 + jb + u) * kBsRC)[q];
+                            acc[q].x = fmaf(nl, xj.x, acc[q].x);
+                            acc[q].y = fmaf(nl, xj.y, acc[q].y);
+                            acc[q].z = fmaf(nl, xj.z, acc[q].z);
+                            acc[q].w = fmaf(nl, xj.w, acc[q].w);
+                        }
                     }
                 }
 #pragma unroll
@@ -132,15 +139,23 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                 float4 acc[kBsRC / 4];
 #pragma unroll
                 for (int q = 0; q < kBsRC / 4; q++) acc[q] = reinterpret_cast<const float4*>(xs + i * kBsRC)[q];
-                for (int j = bs - 1; j >= 0; j--) {
-                    const float nu = -at(i, r0 + j);
+                for (int jt = bs; jt > 0; jt -= 8) {  // j = jt-1 down to jt-8, descending
+                    float uv[8];
 #pragma unroll
-                    for (int q = 0; q < kBsRC / 4; q++) {
-                        const float4 xj = reinterpret_cast<const float4*>(xs + (r0 + j) * kBsRC)[q];
-                        acc[q].x = fmaf(nu, xj.x, acc[q].x);
-                        acc[q].y = fmaf(nu, xj.y, acc[q].y);
-                        acc[q].z = fmaf(nu, xj.z, acc[q].z);
-                        acc[q].w = fmaf(nu, xj.w, acc[q].w);
+                    for (int u = 0; u < 8; u++) uv[u] = jt - 1 - u >= 0 ? at(i, r0 + jt - 1 - u) : 0.0f;
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        const int j = jt - 1 - u;
+                        if (j < 0) break;
+                        const float nu = -uv[u];
+#pragma unroll
+                        for (int q = 0; q < kBsRC / 4; q++) {
+                            const float4 xj = reinterpret_cast<const float4*>(xs + (r0 + j) * kBsRC)[q];
+                            acc[q].x = fmaf(nu, xj.x, acc[q].x);
+                            acc[q].y = fmaf(nu, xj.y, acc[q].y);
+                            acc[q].z = fmaf(nu, xj.z, acc[q].z);
+                            acc[q].w = fmaf(nu, xj.w, acc[q].w);
+                        }
                     }
                 }
 #pragma unroll

@@ -43,13 +43,13 @@ constexpr int kResMaxRhs = 16;  // right-hand sides per pass
 // One CTA per matrix. FP64 residual r = b - A x and normwise backward error; on the last check
 // (final != 0) only the error is recorded. d receives r in FP32; Dact[m] is set to d, or to NULL
 // when the matrix has converged, so that the correction solve and update skip it.
-__global__ void __launch_bounds__(kResThreads)
+__global__ void __launch_bounds__(kResThreads, 2)
 refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, const float* const* Barray, int ldb,
                        const float* const* Xarray, int ldx, float* const* Darray, int ldd, float** Dact, double tol,
                        int it, int final_check, int* __restrict__ done, double* __restrict__ berr,
                        int* __restrict__ iters)
 {
-    extern __shared__ double xs[];  // [n][kResMaxRhs]
+    extern __shared__ double xs[];  // [n + 8][kResMaxRhs]
     __shared__ double red[kResThreads / 32];
     __shared__ double s_anorm;
     __shared__ double s_berr;
@@ -74,59 +74,80 @@ refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, con
         __syncthreads();
         return r;
     };
-    // ||A||_inf (max row sum)
-    double rowmax = 0.0;
-    for (int i = tid; i < n; i += kResThreads) {
-        double s = 0.0;
-        for (int j = 0; j < n; j++) s += fabs((double)A[i + (long long)j * lda]);
-        rowmax = fmax(rowmax, s);
-    }
-    const double anorm = block_max(rowmax);
-    if (tid == 0) {
-        s_anorm = anorm;
-        s_berr = 0.0;
-    }
+    // r = b - A x per right-hand-side chunk; the row sums of |A| (for ||A||_inf) are gathered in
+    // the first chunk's pass over A, so A is read once per chunk. The column maxima of |x| and |b|
+    // are reduced first (into shared memory) so that the row loop keeps only r and max |r| live.
+    __shared__ double s_xn[kResMaxRhs], s_bn[kResMaxRhs];
     double worst = 0.0;
+    double rowmax = 0.0;
     for (int c0 = 0; c0 < nrhs; c0 += kResMaxRhs) {
         const int cw = min(kResMaxRhs, nrhs - c0);
         __syncthreads();
-        for (int e = tid; e < n * cw; e += kResThreads) {
-            const int i = e % n, c = e / n;
-            xs[i * kResMaxRhs + c] = (double)X[i + (long long)(c0 + c) * ldx];
+        for (int e = tid; e < (n + 8) * kResMaxRhs; e += kResThreads) {  // 8 zero rows of padding
+            const int i = e / kResMaxRhs, c = e % kResMaxRhs;
+            xs[i * kResMaxRhs + c] = (c < cw && i < n) ? (double)X[i + (long long)(c0 + c) * ldx] : 0.0;
         }
         __syncthreads();
-        double rmax[kResMaxRhs], xmax[kResMaxRhs], bmax[kResMaxRhs];
+        for (int c = 0; c < cw; c++) {
+            double xm = 0.0, bm = 0.0;
+            for (int i = tid; i < n; i += kResThreads) {
+                xm = fmax(xm, fabs(xs[i * kResMaxRhs + c]));
+                bm = fmax(bm, fabs((double)B[i + (long long)(c0 + c) * ldb]));
+            }
+            xm = block_max(xm);
+            bm = block_max(bm);
+            if (tid == 0) {
+                s_xn[c] = xm;
+                s_bn[c] = bm;
+            }
+        }
+        double rmaxs[kResMaxRhs];
 #pragma unroll
-        for (int c = 0; c < kResMaxRhs; c++) rmax[c] = xmax[c] = bmax[c] = 0.0;
+        for (int c = 0; c < kResMaxRhs; c++) rmaxs[c] = 0.0;
         for (int i = tid; i < n; i += kResThreads) {
             double r[kResMaxRhs];
 #pragma unroll
-            for (int c = 0; c < kResMaxRhs; c++) {
-                const double b = c < cw ? (double)B[i + (long long)(c0 + c) * ldb] : 0.0;
-                r[c] = b;
-                bmax[c] = fmax(bmax[c], fabs(b));
-            }
-            for (int j = 0; j < n; j++) {
-                const double a = (double)A[i + (long long)j * lda];
+            for (int c = 0; c < kResMaxRhs; c++) r[c] = c < cw ? (double)B[i + (long long)(c0 + c) * ldb] : 0.0;
+            double asum = 0.0;
+            for (int j0 = 0; j0 < n; j0 += 8) {
+                float av[8];  // eight independent loads in flight before the FMAs that use them
 #pragma unroll
-                for (int c = 0; c < kResMaxRhs; c++) r[c] = fma(-a, xs[j * kResMaxRhs + c], r[c]);
+                for (int u = 0; u < 8; u++) av[u] = j0 + u < n ? A[i + (long long)(j0 + u) * lda] : 0.0f;
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const double a = (double)av[u];
+                    asum += fabs(a);
+                    const double2* xr = reinterpret_cast<const double2*>(xs + (j0 + u) * kResMaxRhs);
+#pragma unroll
+                    for (int q = 0; q < kResMaxRhs / 2; q++) {
+                        const double2 v = xr[q];  // rows n..n+7 are zero padding
+                        r[2 * q] = fma(-a, v.x, r[2 * q]);
+                        r[2 * q + 1] = fma(-a, v.y, r[2 * q + 1]);
+                    }
+                }
             }
+            if (c0 == 0) rowmax = fmax(rowmax, asum);
 #pragma unroll
             for (int c = 0; c < kResMaxRhs; c++) {
                 if (c < cw) {
-                    rmax[c] = fmax(rmax[c], fabs(r[c]));
-                    xmax[c] = fmax(xmax[c], fabs(xs[i * kResMaxRhs + c]));
+                    rmaxs[c] = fmax(rmaxs[c], fabs(r[c]));
                     if (!final_check) D[i + (long long)(c0 + c) * ldd] = (float)r[c];
                 }
             }
         }
-        for (int c = 0; c < cw; c++) {
-            const double rn = block_max(rmax[c]);
-            const double xn = block_max(xmax[c]);
-            const double bn = block_max(bmax[c]);
-            const double den = s_anorm * xn + bn;
-            const double e = den > 0.0 ? rn / den : (rn > 0.0 ? INFINITY : 0.0);
-            worst = fmax(worst, e);
+        if (c0 == 0) {
+            const double anorm = block_max(rowmax);
+            if (tid == 0) s_anorm = anorm;
+            __syncthreads();
+        }
+#pragma unroll
+        for (int c = 0; c < kResMaxRhs; c++) {  // compile-time index keeps rmaxs in registers
+            if (c < cw) {                          // cw is uniform: block_max's barriers stay uniform
+                const double rn = block_max(rmaxs[c]);
+                const double den = s_anorm * s_xn[c] + s_bn[c];
+                const double e = den > 0.0 ? rn / den : (rn > 0.0 ? INFINITY : 0.0);
+                worst = fmax(worst, e);
+            }
         }
     }
     __syncthreads();
@@ -233,7 +254,7 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     if (err != cudaSuccess) return launch_status(kApi, err);
     const int rhs_chunk = nrhs < kResMaxRhs ? nrhs : kResMaxRhs;
     (void)rhs_chunk;
-    const size_t rsm = (size_t)n * kResMaxRhs * 8;
+    const size_t rsm = (size_t)(n + 8) * kResMaxRhs * 8;
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(refine_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -360,7 +381,7 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
                   (dbytes + 20) * (size_t)batchCount + 512, cap);
         return ACLBLAS_STATUS_INVALID_VALUE;
     }
-    const size_t rsm = (size_t)n * kResMaxRhs * 8;
+    const size_t rsm = (size_t)(n + 8) * kResMaxRhs * 8;
     if (rsm > 200 * 1024) {
         log_error(kApi, "n=%d exceeds the residual kernel's shared-memory limit", n);
         return ACLBLAS_STATUS_NOT_SUPPORTED;

@@ -148,6 +148,15 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16])
 
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
+// TF32 value of x by the hardware conversion (round to nearest, ties away from zero). Used for
+// the high/low operand split, where only hi + lo == x up to the dropped low bits matters.
+__device__ __forceinline__ float tf32_cvt(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
 // Round to nearest even at TF32 precision (10 explicit mantissa bits); Inf/NaN pass through.
 __device__ __forceinline__ float tf32_rne(float x)
 {
