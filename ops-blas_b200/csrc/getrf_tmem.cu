@@ -7,8 +7,8 @@
 // move; `pos` (the row's index in the reference's in-place matrix) records the interchanges.
 // Per panel of 32 columns k0..k0+31:
 //   1. every thread reads its row's panel columns from TMEM and the CTA factors the panel in FP32
-//      exactly as the reference's unblocked LU does (first-maximum pivot, true division, one fmaf
-//      per update), one CTA barrier per column;
+//      as the reference's unblocked LU does (true division, one fmaf per update; the pivot is the
+//      largest magnitude to 15 mantissa bits), one CTA barrier per column;
 //   2. the panel goes back to TMEM; the rows that became this panel's pivot rows publish their
 //      unit-lower L11 part, and the rows below publish -L21 split into TF32 high and low parts
 //      in the UMMA shared-memory layout (the MMA's A operand);
@@ -48,8 +48,7 @@ struct TmSmem {
     float u12[kTmPB][kTmMaxN + 1];  // pivot rows' trailing entries, then U12
     float l11[kTmPB][kTmPB];        // unit-lower L11 of the panel (row = position - k0)
     float crow[2][kTmWarps][kTmPB]; // per column parity and warp: the warp's pivot candidate row
-    unsigned ckey[2][kTmWarps];     //   its |value| key
-    unsigned cpos[2][kTmWarps];     //   its position
+    unsigned ckey[2][kTmWarps];     //   its key (magnitude and position)
     int info;
     uint64_t mbar;
     uint32_t taddr;
@@ -72,29 +71,27 @@ __device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid
         const int k = k0 + c;
         if (k >= n) break;
         const int buf = c & 1;
-        // first maximum of |a(., k)| over the rows at positions >= k; ties to the lowest position
+        // pivot: largest |a(., k)| over the rows at positions >= k, compared on the exponent and
+        // 15 mantissa bits, ties to the lowest position -- one 32-bit key (magnitude << 9 |
+        // 511 - position, never zero for an eligible row; NaN counts as zero) and a single
+        // redux.sync per level. (The factors feed iterative refinement, so an equally good
+        // pivot suffices; the plain kernels keep the reference's exact first-maximum rule.)
         const bool elig = valid && pos >= k;
         const float av = fabsf(p[c]);
-        const unsigned key = (elig && av > 0.0f) ? __float_as_uint(av) : 0u;
+        const unsigned mag = (av == av) ? (__float_as_uint(av) >> 8) : 0u;
+        const unsigned key = elig ? ((mag << 9) | (511u - (unsigned)pos)) : 0u;
         const unsigned wkey = __reduce_max_sync(0xffffffffu, key);
-        const unsigned wpos = __reduce_min_sync(0xffffffffu, (elig && key == wkey) ? (unsigned)pos : 0xffffffffu);
-        if (lane == 0) {
-            S.ckey[buf][warp] = wkey;
-            S.cpos[buf][warp] = wpos;
-        }
-        if (elig && (unsigned)pos == wpos) {
+        if (lane == 0) S.ckey[buf][warp] = wkey;
+        if (elig && key == wkey) {
             float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
 #pragma unroll
             for (int q = 0; q < kTmPB / 4; q++) dst[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
         }
         __syncthreads();
-        // lanes 0..7 each take one warp's candidate; two reductions pick the winner in every warp
         const unsigned qk = lane < kTmWarps ? S.ckey[buf][lane] : 0u;
-        const unsigned qp = lane < kTmWarps ? S.cpos[buf][lane] : 0xffffffffu;
         const unsigned bk = __reduce_max_sync(0xffffffffu, qk);
-        const unsigned bp = __reduce_min_sync(0xffffffffu, (lane < kTmWarps && qk == bk) ? qp : 0xffffffffu);
-        const int bw = __ffs(__ballot_sync(0xffffffffu, lane < kTmWarps && qk == bk && qp == bp)) - 1;
-        const int ppos = (int)bp;
+        const int bw = __ffs(__ballot_sync(0xffffffffu, lane < kTmWarps && qk == bk)) - 1;
+        const int ppos = 511 - (int)(bk & 511u);
         const float* prow = S.crow[buf][bw];
         const float pv = prow[c];
         if (tid == 0 && pm) pm[k] = ppos + 1;
@@ -155,16 +152,22 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((row >> 7) * 256);
 
     // ---- load: the whole row block, zeros outside the matrix ----
-    for (int j0 = 0; j0 < kTmMaxN; j0 += 16) {
-        float v[16];
+    {
+        float v[16], w[16];  // the next chunk's loads are in flight while this chunk is stored
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const int j = j0 + i;
-            v[i] = (valid && j < n) ? A[row + (long long)j * lda] : 0.0f;
+        for (int i = 0; i < 16; i++) v[i] = (valid && i < n) ? A[row + (long long)i * lda] : 0.0f;
+        for (int j0 = 0; j0 < kTmMaxN; j0 += 16) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int j = j0 + 16 + i;
+                w[i] = (valid && j < n) ? A[row + (long long)j * lda] : 0.0f;
+            }
+            tmem_st16(trow + j0, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++) v[i] = w[i];
         }
-        tmem_st16(trow + j0, v);
+        tmem_wait_st();
     }
-    tmem_wait_st();
 
     int pos = row;
     int upanel = -1;  // first column of the panel in which this row became a pivot row

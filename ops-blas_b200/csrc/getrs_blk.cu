@@ -75,13 +75,33 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                 blk[j * kBsLd + i] = (i < bs && j < bs) ? at(r0 + i, r0 + j) : 0.0f;
             }
             __syncthreads();
-            for (int c = warp; c < cw; c += kBsThreads / 32) {
-                float y = lane < bs ? xs[(r0 + lane) * kBsRC + c] : 0.0f;
-                for (int j = 0; j < bs; j++) {
-                    const float yj = __shfl_sync(0xffffffffu, y, j);
-                    if (lane > j && lane < bs) y = fmaf(-blk[j * kBsLd + lane], yj, y);
+            // two right-hand sides per warp, their dependency chains interleaved
+            for (int c = warp; c < cw; c += 2 * (kBsThreads / 32)) {
+                const int c1 = c + kBsThreads / 32;
+                const bool two = c1 < cw;
+                float y0 = lane < bs ? xs[(r0 + lane) * kBsRC + c] : 0.0f;
+                float y1 = (two && lane < bs) ? xs[(r0 + lane) * kBsRC + c1] : 0.0f;
+                if (two) {
+                    for (int j = 0; j < bs; j++) {
+                        const float l = -blk[j * kBsLd + lane];
+                        const float yj0 = __shfl_sync(0xffffffffu, y0, j);
+                        const float yj1 = __shfl_sync(0xffffffffu, y1, j);
+                        if (lane > j && lane < bs) {
+                            y0 = fmaf(l, yj0, y0);
+                            y1 = fmaf(l, yj1, y1);
+                        }
+                    }
+                } else {
+                    for (int j = 0; j < bs; j++) {
+                        const float l = -blk[j * kBsLd + lane];
+                        const float yj0 = __shfl_sync(0xffffffffu, y0, j);
+                        if (lane > j && lane < bs) y0 = fmaf(l, yj0, y0);
+                    }
                 }
-                if (lane < bs) xs[(r0 + lane) * kBsRC + c] = y;
+                if (lane < bs) {
+                    xs[(r0 + lane) * kBsRC + c] = y0;
+                    if (two) xs[(r0 + lane) * kBsRC + c1] = y1;
+                }
             }
             __syncthreads();
             for (int i = r0 + bs + tid; i < n; i += kBsThreads) {
@@ -122,17 +142,42 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                 blk[j * kBsLd + i] = (i < bs && j < bs) ? at(r0 + i, r0 + j) : 0.0f;
             }
             __syncthreads();
-            for (int c = warp; c < cw; c += kBsThreads / 32) {
-                float y = lane < bs ? xs[(r0 + lane) * kBsRC + c] : 0.0f;
-                for (int j = bs - 1; j >= 0; j--) {
-                    const float t = (lane == j) ? y / blk[j * kBsLd + j] : 0.0f;
-                    const float xj = __shfl_sync(0xffffffffu, t, j);
-                    if (lane == j)
-                        y = xj;
-                    else if (lane < j)
-                        y = fmaf(-blk[j * kBsLd + lane], xj, y);
+            // two right-hand sides per warp; every lane divides (no divergence), lane j's quotient
+            // x_j = y_j / U(j,j) is the one broadcast
+            for (int c = warp; c < cw; c += 2 * (kBsThreads / 32)) {
+                const int c1 = c + kBsThreads / 32;
+                const bool two = c1 < cw;
+                float y0 = lane < bs ? xs[(r0 + lane) * kBsRC + c] : 0.0f;
+                float y1 = (two && lane < bs) ? xs[(r0 + lane) * kBsRC + c1] : 0.0f;
+                if (two) {
+                    for (int j = bs - 1; j >= 0; j--) {
+                        const float ujj = blk[j * kBsLd + j];
+                        const float u = -blk[j * kBsLd + lane];
+                        const float xj0 = __shfl_sync(0xffffffffu, y0 / ujj, j);
+                        const float xj1 = __shfl_sync(0xffffffffu, y1 / ujj, j);
+                        if (lane == j) {
+                            y0 = xj0;
+                            y1 = xj1;
+                        } else if (lane < j) {
+                            y0 = fmaf(u, xj0, y0);
+                            y1 = fmaf(u, xj1, y1);
+                        }
+                    }
+                } else {
+                    for (int j = bs - 1; j >= 0; j--) {
+                        const float ujj = blk[j * kBsLd + j];
+                        const float u = -blk[j * kBsLd + lane];
+                        const float xj0 = __shfl_sync(0xffffffffu, y0 / ujj, j);
+                        if (lane == j)
+                            y0 = xj0;
+                        else if (lane < j)
+                            y0 = fmaf(u, xj0, y0);
+                    }
                 }
-                if (lane < bs) xs[(r0 + lane) * kBsRC + c] = y;
+                if (lane < bs) {
+                    xs[(r0 + lane) * kBsRC + c] = y0;
+                    if (two) xs[(r0 + lane) * kBsRC + c1] = y1;
+                }
             }
             __syncthreads();
             for (int i = tid; i < r0; i += kBsThreads) {
