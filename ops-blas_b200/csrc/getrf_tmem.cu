@@ -7,8 +7,9 @@
 // move; `pos` (the row's index in the reference's in-place matrix) records the interchanges.
 // Per panel of 32 columns k0..k0+31:
 //   1. every thread reads its row's panel columns from TMEM and the CTA factors the panel in FP32
-//      as the reference's unblocked LU does (true division, one fmaf per update; the pivot is the
-//      largest magnitude to 15 mantissa bits), one CTA barrier per column;
+//      by the reference's unblocked right-looking steps (one fmaf per update), with two
+//      relaxations that the refinement absorbs: the pivot is the largest magnitude to 15 mantissa
+//      bits and the multipliers use an approximate reciprocal; one CTA barrier per column;
 //   2. the panel goes back to TMEM; the rows that became this panel's pivot rows publish their
 //      unit-lower L11 part, and the rows below publish -L21 split into TF32 high and low parts
 //      in the UMMA shared-memory layout (the MMA's A operand);
@@ -82,10 +83,11 @@ __device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid
         const unsigned key = elig ? ((mag << 9) | (511u - (unsigned)pos)) : 0u;
         const unsigned wkey = __reduce_max_sync(0xffffffffu, key);
         if (lane == 0) S.ckey[buf][warp] = wkey;
-        if (elig && key == wkey) {
+        if (elig && key == wkey) {  // the pivot row from column c's 16-byte chunk on
             float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
 #pragma unroll
-            for (int q = 0; q < kTmPB / 4; q++) dst[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
+            for (int q = c / 4; q < kTmPB / 4; q++)
+                dst[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
         }
         __syncthreads();
         const unsigned qk = lane < kTmWarps ? S.ckey[buf][lane] : 0u;
@@ -104,15 +106,30 @@ __device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid
         else if (pos == k)
             pos = ppos;
         if (valid && pos > k) {
-            const float l = p[c] / pv;
+            // multiplier by the approximate reciprocal (refinement absorbs its last-bit error),
+            // then a(., j) -= l * u(j) two columns per packed fma
+            float rinv;
+            asm("rcp.approx.f32 %0, %1;" : "=f"(rinv) : "f"(pv));
+            const float l = p[c] * rinv;
             p[c] = l;
+            const float2 nl = make_float2(-l, -l);
 #pragma unroll
-            for (int q = (c + 1) / 4; q < kTmPB / 4; q++) {
+            for (int q = c / 4; q < kTmPB / 4; q++) {
                 const float4 u = reinterpret_cast<const float4*>(prow)[q];
-                const float uu[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-                for (int e = 0; e < 4; e++)
-                    if (4 * q + e > c) p[4 * q + e] = fmaf(-l, uu[e], p[4 * q + e]);
+                if (4 * q > c) {
+                    const float2 r = __ffma2_rn(make_float2(u.x, u.y), nl, make_float2(p[4 * q], p[4 * q + 1]));
+                    p[4 * q] = r.x;
+                    p[4 * q + 1] = r.y;
+                } else if (4 * q + 1 > c) {
+                    p[4 * q + 1] = fmaf(-l, u.y, p[4 * q + 1]);
+                }
+                if (4 * q + 2 > c) {
+                    const float2 r = __ffma2_rn(make_float2(u.z, u.w), nl, make_float2(p[4 * q + 2], p[4 * q + 3]));
+                    p[4 * q + 2] = r.x;
+                    p[4 * q + 3] = r.y;
+                } else if (4 * q + 3 > c) {
+                    p[4 * q + 3] = fmaf(-l, u.w, p[4 * q + 3]);
+                }
             }
         }
     }
