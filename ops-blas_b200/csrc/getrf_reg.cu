@@ -43,11 +43,13 @@ bool reg_shape_valid(int n, int rows, int warps)
            (rows == 4 && warps == 8);
 }
 
-// Built-in choice for the plain batched path.
+// Built-in choice (the plain batched path, and the grouped launch without a tuning table): the
+// fastest shapes measured per size bucket on B200 -- 4 warps up to 96 rows, 8 warps for 4 rows
+// per lane (ops-blas_b200/grouped_tuning.txt).
 void reg_default_shape(int n, int& rows, int& warps)
 {
     rows = (n + 31) / 32;
-    warps = 8;
+    warps = rows <= 3 ? 4 : 8;
 }
 
 bool getrf_reg_supported(int n) { return n > 32 && n <= 128; }
