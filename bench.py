@@ -201,6 +201,22 @@ def run_reference_arm(args, rank):
     return line
 
 
+def max_over_ranks(x, dist=None, device=None):
+    """The maximum of x over all ranks (every rank gets it); x itself without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(matrices_per_rank, world, steps, ms):
+    """Matrices/s of the whole job: every rank's matrices over the slowest rank's time."""
+    return matrices_per_rank * world * steps / (ms * 1e-3)
+
+
 def _events_ms(fn, reps, prep=None):
     """Median device time (ms) of fn() over reps runs, prep() outside the timed region."""
     import torch
@@ -499,10 +515,7 @@ def main():
         per["getrf"].append(e[0].elapsed_time(e[1]))
         per["getrs"].append(e[1].elapsed_time(e[2]))
         per["getri"].append(e[2].elapsed_time(e[3]))
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
 
     # e2e through the C ABI from pinned host memory
     hostA = torch.empty((BATCH, N, N), dtype=torch.float32).pin_memory()
@@ -537,10 +550,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, dev)
     h2d = hostA.numel() * 4 + hostB.numel() * 4
     d2h = hostX.numel() * 4 + hostC.numel() * 4 + hostI.numel() * 4
 
@@ -557,7 +567,7 @@ def main():
         traffic = profiled_traffic().get(dom)
         line = {
             "metric": METRIC,
-            "value": BATCH * world * args.steps / (ms * 1e-3),
+            "value": whole_job_rate(BATCH, world, args.steps, ms),
             "unit": "matrices/s",
             "n_gpus": world,
             "steps": args.steps,
