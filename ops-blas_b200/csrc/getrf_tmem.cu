@@ -24,6 +24,7 @@
 // and one write of the matrix. Rows that are not below a panel get zero A-operand rows, so the MMA
 // leaves them unchanged. On an exactly-zero pivot the factorisation stops (info = column + 1) and
 // the trailing columns keep the state of the last completed panel.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -58,6 +59,55 @@ struct TmSmem {
 __device__ __forceinline__ int tm_off(int r, int k)
 {
     return (r >> 3) * (kTmPB * 8) + (k >> 2) * 32 + (r & 7) * 4 + (k & 3);
+}
+
+// BF16 operands: the same core-matrix layout with 8 values per 16-byte row. Float offset of the
+// 16-byte chunk holding k = 8q..8q+7 of row r (SBO = 4 chunks x 128 B = 512 B).
+__device__ __forceinline__ int tm_off16(int r, int q) { return (r >> 3) * 128 + q * 32 + (r & 7) * 4; }
+
+__device__ __forceinline__ uint32_t bf16_pair(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a in the low half (lower address)
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// Splits x into hi = bf16(x) and lo = bf16(x - hi).
+__device__ __forceinline__ void bf16_split(float x, float& hi, float& lo)
+{
+    hi = __bfloat162float(__float2bfloat16_rn(x));
+    lo = x - hi;
+}
+
+// Stages 32 values v (K index 0..31) of operand row r: TF32 (PREC 1) or BF16 (PREC 2) hi/lo parts.
+template <int PREC>
+__device__ __forceinline__ void tm_stage_row(float* hi_base, float* lo_base, int r, const float (&v)[kTmPB])
+{
+    if (PREC == 1) {
+#pragma unroll
+        for (int q = 0; q < kTmPB / 4; q++) {
+            float hi[4], lo[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                hi[e] = tf32_cvt(v[4 * q + e]);
+                lo[e] = tf32_cvt(v[4 * q + e] - hi[e]);
+            }
+            *reinterpret_cast<float4*>(&hi_base[tm_off(r, 4 * q)]) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<float4*>(&lo_base[tm_off(r, 4 * q)]) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < kTmPB / 8; q++) {
+            float hi[8], lo[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) bf16_split(v[8 * q + e], hi[e], lo[e]);
+            *reinterpret_cast<uint4*>(&hi_base[tm_off16(r, q)]) =
+                make_uint4(bf16_pair(hi[0], hi[1]), bf16_pair(hi[2], hi[3]), bf16_pair(hi[4], hi[5]),
+                           bf16_pair(hi[6], hi[7]));
+            *reinterpret_cast<uint4*>(&lo_base[tm_off16(r, q)]) =
+                make_uint4(bf16_pair(lo[0], lo[1]), bf16_pair(lo[2], lo[3]), bf16_pair(lo[4], lo[5]),
+                           bf16_pair(lo[6], lo[7]));
+        }
+    }
 }
 
 // Factors the panel held in p (this thread's row, 32 columns). Returns false when a zero pivot
@@ -136,6 +186,7 @@ __device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid
     return true;
 }
 
+template <int PREC>
 __global__ void __launch_bounds__(kTmThreads, 1)
 getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* __restrict__ LUarr, int n, int ldlu,
                   int* __restrict__ piv, int* __restrict__ info)
@@ -229,18 +280,10 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
         {
             const int b = row >> 7, r = row & 127;
             const bool below = valid && pos >= kend;
+            float x[kTmPB];
 #pragma unroll
-            for (int q = 0; q < kTmPB / 4; q++) {
-                float hi[4], lo[4];
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const float x = (below && k0 + 4 * q + e < n) ? -p[4 * q + e] : 0.0f;
-                    hi[e] = tf32_cvt(x);
-                    lo[e] = tf32_cvt(x - hi[e]);
-                }
-                *reinterpret_cast<float4*>(&S.a_hi[b][tm_off(r, 4 * q)]) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-                *reinterpret_cast<float4*>(&S.a_lo[b][tm_off(r, 4 * q)]) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-            }
+            for (int cc = 0; cc < kTmPB; cc++) x[cc] = (below && k0 + cc < n) ? -p[cc] : 0.0f;
+            tm_stage_row<PREC>(S.a_hi[b], S.a_lo[b], r, x);
         }
         __syncthreads();
         // ---- 3. U12 = L11^-1 * A12 ----
@@ -277,17 +320,7 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
 #pragma unroll
                 for (int r = 0; r < kTmPB; r++) S.u12[r][jj] = u[r];  // written out after the MMA issue
             }
-#pragma unroll
-            for (int q = 0; q < kTmPB / 4; q++) {
-                float hi[4], lo[4];
-#pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    hi[e] = tf32_cvt(u[4 * q + e]);
-                    lo[e] = tf32_cvt(u[4 * q + e] - hi[e]);
-                }
-                *reinterpret_cast<float4*>(&S.b_hi[tm_off(jj, 4 * q)]) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-                *reinterpret_cast<float4*>(&S.b_lo[tm_off(jj, 4 * q)]) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-            }
+            tm_stage_row<PREC>(S.b_hi, S.b_lo, jj, u);
         }
         fence_async_smem();
         tc_fence_before_sync();
@@ -295,21 +328,27 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
         // ---- 4. A22 += (-L21) * U12 on the tensor cores, into the resident matrix ----
         if (tid == 0) {
             tc_fence_after_sync();
-            const uint32_t idesc = umma_idesc(128, npad, 2);
-            const uint32_t sbo = kTmPB * 32;
+            const uint32_t idesc = umma_idesc(128, npad, PREC == 1 ? 2u : 1u);
+            const uint32_t sbo = PREC == 1 ? kTmPB * 32 : kTmPB * 16;  // bytes between 8-row groups
             for (int b = 0; b < 2; b++) {
                 if (128 * b >= n) break;
                 const uint32_t d = tbase + (uint32_t)(b * 256 + j0);
 #pragma unroll
-                for (int s = 0; s < kTmPB / 8; s++) {
-                    const uint32_t step = s * 256;
+                for (int s = 0; s < (PREC == 1 ? kTmPB / 8 : kTmPB / 16); s++) {
+                    const uint32_t step = s * 256;  // two core matrices along K
                     const uint64_t ah = umma_smem_desc(smem_u32(S.a_hi[b]) + step, 128, sbo);
                     const uint64_t al = umma_smem_desc(smem_u32(S.a_lo[b]) + step, 128, sbo);
                     const uint64_t bh = umma_smem_desc(smem_u32(S.b_hi) + step, 128, sbo);
                     const uint64_t bl = umma_smem_desc(smem_u32(S.b_lo) + step, 128, sbo);
-                    umma_tf32(d, ah, bl, idesc, 1);
-                    umma_tf32(d, al, bh, idesc, 1);
-                    umma_tf32(d, ah, bh, idesc, 1);
+                    if (PREC == 1) {
+                        umma_tf32(d, ah, bl, idesc, 1);
+                        umma_tf32(d, al, bh, idesc, 1);
+                        umma_tf32(d, ah, bh, idesc, 1);
+                    } else {
+                        umma_f16(d, ah, bl, idesc, 1);
+                        umma_f16(d, al, bh, idesc, 1);
+                        umma_f16(d, ah, bh, idesc, 1);
+                    }
                 }
             }
             umma_commit(&S.mbar);
@@ -354,18 +393,26 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
 bool getrf_tmem_supported(int n) { return n > 32 && n <= kTmMaxN; }
 
 cudaError_t getrf_tmem_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
-                              int ldlu, int* piv, int* info, int batch)
+                              int ldlu, int* piv, int* info, int batch, int prec)
 {
     static int configured_device = -1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (configured_device != dev) {
-        cudaError_t e =
-            cudaFuncSetAttribute(getrf_tmem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TmSmem));
+        cudaError_t e = cudaFuncSetAttribute(getrf_tmem_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sizeof(TmSmem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(getrf_tmem_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(TmSmem));
         if (e != cudaSuccess) return e;
         configured_device = dev;
     }
-    getrf_tmem_kernel<<<(unsigned)batch, kTmThreads, sizeof(TmSmem), st>>>(Aarray, lda, LUarray, n, ldlu, piv, info);
+    if (prec == 2)
+        getrf_tmem_kernel<2><<<(unsigned)batch, kTmThreads, sizeof(TmSmem), st>>>(Aarray, lda, LUarray, n, ldlu, piv,
+                                                                                 info);
+    else
+        getrf_tmem_kernel<1><<<(unsigned)batch, kTmThreads, sizeof(TmSmem), st>>>(Aarray, lda, LUarray, n, ldlu, piv,
+                                                                                 info);
     return cudaGetLastError();
 }
 

@@ -61,11 +61,12 @@ cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int
                            const float* const* A, long long a_off, int lda, const float* const* B, long long b_off,
                            int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split);
 
-// getrf_tmem.cu: 32 < n <= 256, TF32-split mixed-precision LU with the matrix resident in TMEM.
+// getrf_tmem.cu: 32 < n <= 256, mixed-precision LU with the matrix resident in TMEM.
 bool getrf_tmem_supported(int n);
-// Reads A (lda), writes the factors to LU (ldlu); A may equal LU.
+// Reads A (lda), writes the factors to LU (ldlu); A may equal LU. prec 1: TF32 split update,
+// 2: BF16 split update.
 cudaError_t getrf_tmem_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
-                              int ldlu, int* piv, int* info, int batch);
+                              int ldlu, int* piv, int* info, int batch, int prec);
 
 // getrf_large.cu: 32 < n <= 640, matrix in global memory; mode 0 plain FP32 (reference
 // operation order), 1 = TF32 split trailing update, 2 = BF16 split trailing update.

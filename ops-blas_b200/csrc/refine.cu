@@ -2,10 +2,9 @@
 //
 // No counterpart in the reference (an extension next to the drop-in chain). Per matrix:
 //   LU = A (copy; A is kept for the residual), P*LU = A factored by aclblasSgetrfBatched's
-//   kernels -- plain FP32 for ACLBLAS_COMPUTE_32F; for ACLBLAS_COMPUTE_32F_FAST_TF32 with the
-//   split-TF32 trailing update on the tensor cores, the matrix resident in TMEM (getrf_tmem.cu,
-//   n <= 256; getrf_large.cu on the CUDA cores above); for _FAST_16BF with the split BF16 update
-//   (getrf_large.cu);
+//   kernels -- plain FP32 for ACLBLAS_COMPUTE_32F; for ACLBLAS_COMPUTE_32F_FAST_TF32 / _FAST_16BF
+//   with the split TF32 / BF16 trailing update on the tensor cores, the matrix resident in TMEM
+//   (getrf_tmem.cu, n <= 256; getrf_large.cu on the CUDA cores above);
 //   X = LU \ B (aclblasSgetrsBatched's kernels);
 //   repeat up to maxIter times: r = B - A X in FP64 on the GPU, backward error
 //     berr = max_c ||r_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf) in FP64;
@@ -236,12 +235,12 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     init_ptr_array_kernel<<<bgrid, 256, 0, st>>>(dptr, dbase, (long long)(dbytes / 4), batchCount);
     fill_int_kernel<<<bgrid, 256, 0, st>>>(done, 0, batchCount);
     fill_int_kernel<<<bgrid, 256, 0, st>>>(iterArray, maxIter, batchCount);
-    const bool tmem = mode == 1 && getrf_tmem_supported(n);  // reads A, writes LU: no copy
+    const bool tmem = mode != 0 && getrf_tmem_supported(n);  // reads A, writes LU: no copy
     if (!tmem) copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
-        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount);
+        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
     } else if (n > 32 && getrf_large_supported(n) && (mode != 0 || n > 128)) {
         err = getrf_large_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
     } else {
@@ -407,12 +406,12 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
     init_ptr_array_kernel<<<bgrid, 256, 0, st>>>(dptr, dbase, (long long)(dbytes / 4), batchCount);
     fill_int_kernel<<<bgrid, 256, 0, st>>>(done, 0, batchCount);
     fill_int_kernel<<<bgrid, 256, 0, st>>>(iterArray, maxIter, batchCount);
-    const bool tmem = mode == 1 && getrf_tmem_supported(n);  // reads A, writes LU: no copy
+    const bool tmem = mode != 0 && getrf_tmem_supported(n);  // reads A, writes LU: no copy
     if (!tmem) copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
     err = cudaGetLastError();
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
-        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount);
+        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
     } else if (n > 32 && getrf_large_supported(n) && (mode != 0 || n > 128)) {
         err = getrf_large_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
     } else {

@@ -278,17 +278,19 @@ def _apply_pivots(a, piv):
     return a
 
 
+@pytest.mark.parametrize("compute,rtol", [(6, 2e-6), (5, 1e-4)], ids=["tf32", "bf16"])
 @pytest.mark.parametrize("n", [33, 48, 100, 128, 129, 200, 255, 256])
-def test_tmem_mixed_lu_reconstructs(handle, n):
-    """TF32 mode (factors resident in tensor memory, split-TF32 tcgen05 trailing update): the
-    factors reproduce P*A = L*U to near FP32 accuracy in FP64, pivots form a permutation."""
+def test_tmem_mixed_lu_reconstructs(handle, n, compute, rtol):
+    """TF32 / BF16 modes (factors resident in tensor memory, split hi/lo tcgen05 trailing update):
+    the factors reproduce P*A = L*U in FP64 to the split's precision, pivots form a permutation,
+    and refinement reaches an FP64 backward error <= 1e-6."""
     import torch
 
     batch, nrhs = 12, 2
     A64, a32 = conditioned_batch(n, batch, 1e3, seed=n)
     b = np.random.default_rng(n).standard_normal((batch, nrhs, n)).astype(np.float32)
     X, LU, piv, info, berr, iters = handle.refine(to_dev(a32, "cuda"), to_dev(b, "cuda"), n, nrhs,
-                                                  compute=6, max_iter=10, tol=1e-6)
+                                                  compute=compute, max_iter=10, tol=1e-6)
     torch.cuda.synchronize()
     assert int(info.max()) == 0 and int(info.min()) == 0
     lu, pv = to_host(LU), to_host(piv)
@@ -299,12 +301,13 @@ def test_tmem_mixed_lu_reconstructs(handle, n):
         U = np.triu(F)
         PA = _apply_pivots(a32[q].T.astype(np.float64), pv[q])
         rel = np.linalg.norm(PA - L @ U) / np.linalg.norm(PA)
-        assert rel < 2e-6, (q, rel)
+        assert rel < rtol, (q, rel)
     assert float(to_host(berr).max()) <= 1e-6
 
 
-def test_tmem_mixed_lu_singular(handle):
-    """A zero column stops the TF32-mode factorisation with info = that column + 1."""
+@pytest.mark.parametrize("compute", [6, 5], ids=["tf32", "bf16"])
+def test_tmem_mixed_lu_singular(handle, compute):
+    """A zero column stops the mixed-mode factorisation with info = that column + 1."""
     import torch
 
     n, batch = 96, 4
@@ -313,7 +316,7 @@ def test_tmem_mixed_lu_singular(handle):
     for q, col in enumerate([0, 31, 32, 77]):
         a[q, col, :] = 0.0  # column col (column-major batch convention)
     b = rng.standard_normal((batch, 1, n)).astype(np.float32)
-    X, LU, piv, info, berr, iters = handle.refine(to_dev(a, "cuda"), to_dev(b, "cuda"), n, 1, compute=6,
+    X, LU, piv, info, berr, iters = handle.refine(to_dev(a, "cuda"), to_dev(b, "cuda"), n, 1, compute=compute,
                                                   max_iter=2, tol=1e-6)
     torch.cuda.synchronize()
     inf = to_host(info)
