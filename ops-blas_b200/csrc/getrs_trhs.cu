@@ -1,0 +1,89 @@
+// aclblasSgetrsBatched, trans T / C, n > 32: one thread per (matrix, right-hand side).
+//
+// The reference's transposed solve (sgetrs_batched_kernel.cpp:202-388) runs, per right-hand
+// side: the U^T forward sweep x_j /= U(j,j), x_i -= U(j,i) x_j (i > j), then the L^T backward
+// sweep as dot products s = x_j - sum_{i>j} L(i,j) x_i accumulated in increasing i, then the
+// interchanges in reverse order. The dot-product order makes every element depend on the whole
+// chain before it, so this kernel keeps the reference's thread-per-right-hand-side structure:
+// thread g solves column g % nrhs of matrix g / nrhs with its x vector in shared memory (odd
+// row stride: the threads of a warp hit distinct banks), reading LU through L1/L2 (the threads
+// of one matrix read the same addresses). Bit-identical to the reference order.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace opsblas {
+
+constexpr int kTrThreads = 128;
+
+static int trhs_stride(int n) { return n | 1; }
+
+__global__ void __launch_bounds__(kTrThreads)
+getrs_trhs_kernel(const float* const* __restrict__ Aarray, int n, int lda, const int* __restrict__ ipiv,
+                  float* const* __restrict__ Barray, int ldb, int nrhs, long long chains, int stride)
+{
+    extern __shared__ float xs_all[];
+    const long long g = (long long)blockIdx.x * kTrThreads + threadIdx.x;
+    if (g >= chains) return;
+    const long long m = g / nrhs;
+    const int c = (int)(g % nrhs);
+    float* B = Barray[m];
+    if (B == nullptr) return;  // a NULL right-hand side skips the matrix
+    const float* A = Aarray[m];
+    float* x = xs_all + (size_t)threadIdx.x * stride;
+    float* bc = B + (long long)c * ldb;
+    for (int i = 0; i < n; i++) x[i] = bc[i];
+
+    // U^T forward sweep (row j of U: A[j + i*lda], i > j)
+    for (int j = 0; j < n; j++) {
+        const float xj = x[j] / A[j + (long long)j * lda];
+        x[j] = xj;
+        const float* urow = A + j;
+        for (int i = j + 1; i < n; i++) x[i] = fmaf(-urow[(long long)i * lda], xj, x[i]);
+    }
+    // L^T backward sweep (column j of L: A[i + j*lda], i > j), dot products in increasing i
+    for (int j = n - 1; j >= 0; j--) {
+        const float* lcol = A + (long long)j * lda;
+        float s = x[j];
+        for (int i = j + 1; i < n; i++) s = fmaf(-lcol[i], x[i], s);
+        x[j] = s;
+    }
+    // interchanges in reverse (sgetrs_batched_kernel.cpp:94-100 semantics: invalid pivots skipped)
+    if (ipiv != nullptr) {
+        const int* p = ipiv + m * n;
+        for (int k = n - 1; k >= 0; k--) {
+            const int q = p[k] - 1;
+            if ((unsigned)q < (unsigned)n && q != k) {
+                const float t = x[k];
+                x[k] = x[q];
+                x[q] = t;
+            }
+        }
+    }
+    for (int i = 0; i < n; i++) bc[i] = x[i];
+}
+
+bool getrs_trhs_supported(int n) { return n > 32 && (size_t)kTrThreads * trhs_stride(n) * 4 <= 200 * 1024; }
+
+cudaError_t getrs_trhs_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda, const int* ipiv,
+                              float* const* Barray, int ldb, int batch)
+{
+    static int configured_device = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (configured_device != dev) {
+        cudaError_t e =
+            cudaFuncSetAttribute(getrs_trhs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return e;
+        configured_device = dev;
+    }
+    const long long chains = (long long)batch * nrhs;
+    const long long blocks = (chains + kTrThreads - 1) / kTrThreads;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    const int stride = trhs_stride(n);
+    getrs_trhs_kernel<<<(unsigned)blocks, kTrThreads, (size_t)kTrThreads * stride * 4, st>>>(
+        Aarray, n, lda, ipiv, Barray, ldb, nrhs, chains, stride);
+    return cudaGetLastError();
+}
+
+}  // namespace opsblas
