@@ -174,9 +174,9 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrsAdjointBatched(
  * A plan describes groupCount groups (host arrays): group g has groupSizeArray[g] instances of
  * order nArray[g], nrhsArray[g] right-hand sides (0: factor only), leading dimensions
  * ldaArray[g] / ldbArray[g]. Instances are numbered group by group. configArray is NULL or holds
- * 3 ints per group {lanes per matrix (n <= 32: 4/8/16/32), warps per matrix (n > 32: 4 or 8),
- * rows per lane (n > 32: 2, 3 or 4, with 32 * rows >= n; 4 rows need 8 warps)}, 0 = take the
- * tuning table's choice; the table is the file
+ * 3 ints per group {lanes per matrix (n <= 32: 4/8/16/32), warps per matrix (n > 32: 2, 4 or 8),
+ * rows per lane (n > 32: 2, 3 or 4, with 32 * rows >= n; 2 warps only with 2 rows, 4 rows need
+ * 8 warps)}, 0 = take the tuning table's choice; the table is the file
  * named by OPSBLAS_GROUPED_TUNING, else grouped_tuning.txt beside the library, else built-in
  * defaults. Invalid choices are replaced; aclblasSgetrfGetrsGroupedPlanGetConfig returns the
  * ones in use. Creating a plan allocates and uploads its task lists (synchronously). */

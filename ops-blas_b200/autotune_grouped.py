@@ -8,9 +8,9 @@ side), keeps the fastest, and writes the table that aclblasSgetrfGetrsGroupedPla
     1 4 4 0 0
     ...
 
-Candidates: n <= 16 -- lanes per matrix {natural segment, 32}; 33 <= n <= 128 -- warps per
-matrix {4, 8} x rows per lane {ceil(n/32), ..., 4} (the instantiated register shapes; a 4-warp
-shape puts two matrices in one CTA). Every candidate computes the same bits, so only time
+Candidates: n <= 16 -- lanes per matrix {natural segment, 32}; 33 <= n <= 128 -- the instantiated
+register shapes (rows per lane, warps per matrix) with 32 * rows >= n: (2,2), (2,4), (2,8), (3,4),
+(3,8), (4,8); a 2- or 4-warp shape puts four or two matrices in one CTA. Every candidate computes the same bits, so only time
 decides. Usage (needs a B200):
 
     python ops-blas_b200/autotune_grouped.py [--out PATH] [--reps 7]
@@ -50,7 +50,8 @@ def candidates(lo, hi):
     if hi <= 32:
         return [(_natural(hi), 0, 0)] + ([(32, 0, 0)] if hi <= 16 else [])
     rmin = (hi + 31) // 32
-    return [(0, w, r) for r in range(rmin, 5) for w in (4, 8) if not (r == 4 and w == 4)]
+    shapes = [(2, 2), (2, 4), (2, 8), (3, 4), (3, 8), (4, 8)]  # (rows per lane, warps) instantiated
+    return [(0, w, r) for r, w in shapes if r >= rmin]
 
 
 def time_bucket(ob, handle, lo, hi, config, reps, seed=0, target_bytes=256 << 20, max_instances=400_000):

@@ -13,7 +13,7 @@
 namespace opsblas {
 
 template <int R, int NW, bool PIVOT>
-__global__ void __launch_bounds__(NW * 32, NW == 8 ? 2 : 3)
+__global__ void __launch_bounds__(NW * 32, NW == 8 ? 2 : (NW == 4 ? 3 : 8))
 getrf_reg_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __restrict__ piv, int* __restrict__ info)
 {
     constexpr int CW = RegShape<R, NW>::CW;
@@ -39,17 +39,17 @@ getrf_reg_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __restr
 bool reg_shape_valid(int n, int rows, int warps)
 {
     if (n <= 32 || n > 32 * rows) return false;
-    return (rows == 2 && (warps == 4 || warps == 8)) || (rows == 3 && (warps == 4 || warps == 8)) ||
+    return (rows == 2 && (warps == 2 || warps == 4 || warps == 8)) || (rows == 3 && (warps == 4 || warps == 8)) ||
            (rows == 4 && warps == 8);
 }
 
 // Built-in choice (the plain batched path, and the grouped launch without a tuning table): the
-// fastest shapes measured per size bucket on B200 -- 4 warps up to 96 rows, 8 warps for 4 rows
-// per lane (ops-blas_b200/grouped_tuning.txt).
+// fastest shapes measured per size bucket on B200 -- 2 warps up to 64 rows, 4 warps up to 96,
+// 8 warps for 4 rows per lane (ops-blas_b200/grouped_tuning.txt).
 void reg_default_shape(int n, int& rows, int& warps)
 {
     rows = (n + 31) / 32;
-    warps = rows <= 3 ? 4 : 8;
+    warps = rows == 2 ? 2 : (rows == 3 ? 4 : 8);
 }
 
 bool getrf_reg_supported(int n) { return n > 32 && n <= 128; }
@@ -67,7 +67,8 @@ cudaError_t getrf_reg_launch(cudaStream_t st, float* const* Aarray, int n, int l
                              int rows, int warps)
 {
     if (!reg_shape_valid(n, rows, warps)) reg_default_shape(n, rows, warps);
-    if (rows == 2 && warps == 4) launch_shape<2, 4>(st, Aarray, n, lda, piv, info, batch);
+    if (rows == 2 && warps == 2) launch_shape<2, 2>(st, Aarray, n, lda, piv, info, batch);
+    else if (rows == 2 && warps == 4) launch_shape<2, 4>(st, Aarray, n, lda, piv, info, batch);
     else if (rows == 2) launch_shape<2, 8>(st, Aarray, n, lda, piv, info, batch);
     else if (rows == 3 && warps == 4) launch_shape<3, 4>(st, Aarray, n, lda, piv, info, batch);
     else if (rows == 3) launch_shape<3, 8>(st, Aarray, n, lda, piv, info, batch);

@@ -11,7 +11,7 @@
 // then one launch of grouped_lu_kernel on the handle's stream (plus the regular batched kernels
 // for groups with n > 128): a grid of one wave of 256-thread CTAs that take tasks from two
 // device counters --
-//   phase 1, CTA tasks (n > 32): the CTA (8 warps) or each 4-warp half of it factors one matrix
+//   phase 1, CTA tasks (n > 32): the CTA (8 warps) or each 4-warp / 2-warp team factors one matrix
 //     held in registers (reg_getrf_core), stores LU, pivots and info, and solves the
 //     right-hand sides from a copy of the factors in shared memory (med_solve_core);
 //   phase 2, warp tasks (n <= 32): each warp takes 32/lanes matrices, factors them in
@@ -41,9 +41,10 @@ struct GroupDev {
     long long piv_off;  // first pivot of the group's first instance
     int first;          // index of the group's first instance in the pointer arrays
     int lanes;          // n <= 32: lanes per matrix (SEG)
-    int warps;          // n > 32: warps per matrix (4 or 8)
+    int warps;          // n > 32: warps per matrix (2, 4 or 8)
     int rows;           // n > 32: rows per lane (2, 3 or 4; 32 * rows >= n)
-    int pad[2];
+    int team_floats;    // n > 32: shared-memory floats between consecutive teams' staged factors
+    int pad;
 };
 
 struct GroupTask {
@@ -123,7 +124,9 @@ __device__ __forceinline__ void grouped_reg_dispatch(const GroupDev& g, int li, 
                                                      float* const* Barray, int* piv, int* info, RegTeamSmem& S,
                                                      float* sa, int warp, int lane, int bar)
 {
-    if (NW == 4) {
+    if (NW == 2) {
+        grouped_reg<2, 2>(g, li, Aarray, Barray, piv, info, S, sa, warp, lane, bar);
+    } else if (NW == 4) {
         if (g.rows == 2)
             grouped_reg<2, 4>(g, li, Aarray, Barray, piv, info, S, sa, warp, lane, bar);
         else
@@ -194,12 +197,12 @@ __device__ __forceinline__ void grouped_small_dispatch(const GroupDev& g, const 
 }
 
 __global__ void __launch_bounds__(kGrpThreads, 2)
-grouped_lu_kernel(const GroupDev* __restrict__ groups, const GroupTask* __restrict__ cta_tasks, int n_cta,
+grouped_lu_kernel(const GroupDev* groups, const GroupTask* __restrict__ cta_tasks, int n_cta,
                   const GroupTask* __restrict__ warp_tasks, int n_warp, int* __restrict__ counters,
-                  float* const* Aarray, float* const* Barray, int* piv, int* info, int team_floats)
+                  float* const* Aarray, float* const* Barray, int* piv, int* info)
 {
     extern __shared__ __align__(16) float dyn[];  // per team: staged factors for the solve
-    __shared__ RegTeamSmem team[2];
+    __shared__ RegTeamSmem team[4];
     __shared__ int s_task;
     __shared__ __align__(16) float rowbuf[kGrpWarps][2][32];
     __shared__ int owner[kGrpWarps][32];
@@ -213,12 +216,17 @@ grouped_lu_kernel(const GroupDev* __restrict__ groups, const GroupTask* __restri
         __syncthreads();
         if (t >= n_cta) break;
         const GroupTask task = cta_tasks[t];
-        const GroupDev g = groups[task.group];
-        if (g.warps == 4) {
+        const GroupDev& g = groups[task.group];  // fields read when needed: fewer live registers
+        if (g.warps == 2) {  // four 2-warp teams, one matrix each
+            const int tm = warp >> 1;
+            if (tm < task.count)
+                grouped_reg_dispatch<2>(g, task.first + tm, Aarray, Barray, piv, info, team[tm],
+                                        dyn + (size_t)tm * g.team_floats, warp & 1, lane, 1 + tm);
+        } else if (g.warps == 4) {
             const int tm = warp >> 2;
             if (tm < task.count)
                 grouped_reg_dispatch<4>(g, task.first + tm, Aarray, Barray, piv, info, team[tm],
-                                        dyn + (size_t)tm * team_floats, warp & 3, lane,
+                                        dyn + (size_t)tm * g.team_floats, warp & 3, lane,
                                         1 + tm);
         } else {
             grouped_reg_dispatch<8>(g, task.first, Aarray, Barray, piv, info, team[0], dyn, warp, lane, -1);
@@ -344,7 +352,6 @@ struct _aclblas_grouped_plan {
     int* d_counters = nullptr;
     int n_cta = 0, n_warp = 0;
     int grid = 0;
-    int team_floats = 0;  // shared-memory floats per team for the staged factors
     size_t smem = 0;      // dynamic shared memory per CTA
     bool has_persistent = false;
 };
@@ -423,19 +430,20 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
     for (int g = 0; g < groupCount; g++) order[g] = g;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p->groups[a].n > p->groups[b].n; });
     std::vector<GroupTask> cta, warp;
-    size_t team_floats = 0, smem = 0;
+    size_t smem = 0;
+    std::vector<int> team_stride(std::max(groupCount, 1), 0);
     for (int g : order) {
         const GroupHost& h = p->groups[g];
         if (h.n == 0 || h.size == 0 || h.n > kGrpMaxN) continue;
         if (h.n > 32) {
-            const int per = h.cfg[1] == 4 ? 2 : 1;
+            const int per = kGrpWarps / h.cfg[1];  // matrices per CTA task (teams)
             for (int i = 0; i < h.size; i += per) cta.push_back({g, i, std::min(per, h.size - i), 0});
             if (h.nrhs > 0) {
-                const size_t f = ((size_t)(h.n | 1) * h.n + 3) & ~(size_t)3;  // staged factors, 16-byte rounded
-                if (per == 2)
-                    team_floats = std::max(team_floats, f);  // second team starts here
-                else
-                    smem = std::max(smem, f * 4);
+                // staged factors, 16-byte rounded; team t's region starts at t * f, the teams of a
+                // CTA stage side by side
+                const size_t f = ((size_t)(h.n | 1) * h.n + 3) & ~(size_t)3;
+                team_stride[g] = (int)f;
+                smem = std::max(smem, (size_t)per * f * 4);
             }
         } else {
             const int per = 32 / h.cfg[0];
@@ -445,13 +453,12 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
     p->n_cta = (int)cta.size();
     p->n_warp = (int)warp.size();
     p->has_persistent = p->n_cta + p->n_warp > 0;
-    p->team_floats = (int)team_floats;
-    p->smem = std::max(smem, 2 * team_floats * 4);  // the two 4-warp teams of a CTA stage side by side
+    p->smem = smem;
 
     std::vector<GroupDev> gd(std::max(groupCount, 1));
     for (int g = 0; g < groupCount; g++) {
         const GroupHost& h = p->groups[g];
-        gd[g] = {h.n, h.nrhs, h.lda, h.ldb, h.piv_off, h.first, h.cfg[0], h.cfg[1], h.cfg[2], {0, 0}};
+        gd[g] = {h.n, h.nrhs, h.lda, h.ldb, h.piv_off, h.first, h.cfg[0], h.cfg[1], h.cfg[2], team_stride[g], 0};
     }
     if (p->has_persistent) {
         const size_t bg = gd.size() * sizeof(GroupDev);
@@ -537,7 +544,7 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedBatched(aclblasHandle_t hand
     if (plan->has_persistent) {
         grouped_lu_kernel<<<(unsigned)plan->grid, kGrpThreads, plan->smem, st>>>(
             plan->d_groups, plan->d_cta, plan->n_cta, plan->d_warp, plan->n_warp, plan->d_counters, Aarray, Barray,
-            PivotArray, infoArray, plan->team_floats);
+            PivotArray, infoArray);
         cudaError_t err = cudaGetLastError();
         if (err != cudaSuccess) return launch_status(kApi, err);
     }

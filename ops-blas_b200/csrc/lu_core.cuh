@@ -162,11 +162,14 @@ __device__ __forceinline__ float small_solve_core(const float4 (&a4)[(N + 3) / 4
     return y;
 }
 
-// Barrier over the team: bar < 0 means the team is the whole CTA.
+// Barrier over the team: bar < 0 means the team is the whole CTA; a one-warp team needs only
+// the warp barrier.
 template <int NT>
 __device__ __forceinline__ void team_sync(int bar)
 {
-    if (bar < 0)
+    if (NT == 32)
+        __syncwarp();
+    else if (bar < 0)
         __syncthreads();
     else
         asm volatile("bar.sync %0, %1;\n" ::"r"(bar), "n"(NT) : "memory");
@@ -191,15 +194,13 @@ template <int R, int NW>
 struct RegShape {
     static constexpr int NMAX = 32 * R;
     static constexpr int CW = NMAX / NW;  // column slots per warp
-    static_assert(NMAX % NW == 0, "columns must deal out evenly");
+    static_assert(NMAX % NW == 0 && CW % 4 == 0, "columns must deal out evenly, in float4 chunks");
 };
-
-constexpr int kRegMaxCW = 24;  // largest CW of the instantiated shapes
 
 // Shared state of one team.
 struct __align__(16) RegTeamSmem {
     float l[2][128];               // multipliers of the current column by physical row (double buffered)
-    float u[8][kRegMaxCW];         // per warp: the pivot row's entries in the warp's columns
+    float u[128];                  // the pivot row's entries; warp w's columns at u[w * CW]
     int lmap[128];                 // after factoring: logical row -> physical row
     int ppos[2];
     float pv[2];
@@ -294,7 +295,7 @@ __device__ __forceinline__ int reg_getrf_core(float (&a)[R][RegShape<R, NW>::CW]
                         if (np > k && np < n) {
                             const float l = a[t][c] / pv;
                             a[t][c] = l;
-                            S.l[buf][lane + 32 * t] = l;
+                            if (NW > 1) S.l[buf][lane + 32 * t] = l;
                         }
                     }
                 }
@@ -319,10 +320,10 @@ __device__ __forceinline__ int reg_getrf_core(float (&a)[R][RegShape<R, NW>::CW]
 #pragma unroll
             for (int t = 0; t < R; t++) {
                 below[t] = pos[t] > k && pos[t] < n;
-                l[t] = below[t] ? S.l[buf][lane + 32 * t] : 0.0f;
+                l[t] = below[t] ? (NW == 1 ? a[t][c] : S.l[buf][lane + 32 * t]) : 0.0f;
             }
             // the lane holding logical row k publishes its slots (from chunk c/4 on) as float4s
-            float4* ub4 = reinterpret_cast<float4*>(S.u[warp]);
+            float4* ub4 = reinterpret_cast<float4*>(S.u + warp * CW);
 #pragma unroll
             for (int t = 0; t < R; t++) {
                 if (pos[t] == k) {
@@ -332,38 +333,36 @@ __device__ __forceinline__ int reg_getrf_core(float (&a)[R][RegShape<R, NW>::CW]
                 }
             }
             __syncwarp();
-            float u[CW];
+            // update, one float4 chunk of the pivot row at a time (slot c only for warps after the
+            // owner; slots > c always), two slots per packed fma; fma(u, -l, a) == fma(-l, u, a)
 #pragma unroll
             for (int q = c / 4; q < CW / 4; q++) {
                 const float4 v = ub4[q];
-                u[4 * q] = v.x;
-                u[4 * q + 1] = v.y;
-                u[4 * q + 2] = v.z;
-                u[4 * q + 3] = v.w;
-            }
-            // slot c holds column k itself (owner warp) or a column right of k (later warps)
-            if (warp > w) {
+                const float uu[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
-                for (int t = 0; t < R; t++)
-                    if (below[t]) a[t][c] = fmaf(-l[t], u[c], a[t][c]);
-            }
-            // slots c+1.. : two columns per packed fma, fma(u, -l, a) == fma(-l, u, a) exactly
+                for (int e = 0; e < 4; e += 2) {
+                    const int s0 = 4 * q + e;
+                    if (s0 > c) {
 #pragma unroll
-            for (int s2 = c + 1; s2 < CW; s2 += 2) {
-                if (s2 + 1 < CW) {
+                        for (int t = 0; t < R; t++) {
+                            if (below[t]) {
+                                const float2 r2 = __ffma2_rn(make_float2(uu[e], uu[e + 1]), make_float2(-l[t], -l[t]),
+                                                             make_float2(a[t][s0], a[t][s0 + 1]));
+                                a[t][s0] = r2.x;
+                                a[t][s0 + 1] = r2.y;
+                            }
+                        }
+                    } else {
 #pragma unroll
-                    for (int t = 0; t < R; t++) {
-                        if (below[t]) {
-                            const float2 r2 = __ffma2_rn(make_float2(u[s2], u[s2 + 1]), make_float2(-l[t], -l[t]),
-                                                         make_float2(a[t][s2], a[t][s2 + 1]));
-                            a[t][s2] = r2.x;
-                            a[t][s2 + 1] = r2.y;
+                        for (int h = 0; h < 2; h++) {
+                            const int sl = s0 + h;
+                            if (sl > c || (sl == c && warp > w)) {
+#pragma unroll
+                                for (int t = 0; t < R; t++)
+                                    if (below[t]) a[t][sl] = fmaf(-l[t], uu[e + h], a[t][sl]);
+                            }
                         }
                     }
-                } else {
-#pragma unroll
-                    for (int t = 0; t < R; t++)
-                        if (below[t]) a[t][s2] = fmaf(-l[t], u[s2], a[t][s2]);
                 }
             }
         }

@@ -97,7 +97,7 @@ def test_grouped_repeated_executions_reset_counters(ob, handle):
         _assert_same(o, ref)
 
 
-@pytest.mark.parametrize("config", [(32, 0, 0), (0, 4, 2), (0, 8, 2), (0, 4, 3), (0, 8, 3), (0, 8, 4)])
+@pytest.mark.parametrize("config", [(32, 0, 0), (0, 2, 2), (0, 4, 2), (0, 8, 2), (0, 4, 3), (0, 8, 3), (0, 8, 4)])
 def test_grouped_every_config_gives_the_same_bits(ob, handle, config):
     d = _setup(ob, **MIXED, seed=3, ldpad=3)
     cfgs = [config] * len(d["ns"])
@@ -106,8 +106,8 @@ def test_grouped_every_config_gives_the_same_bits(ob, handle, config):
     for n, (lanes, warps, rows) in zip(d["ns"], used):
         if n <= 32:
             assert lanes in (4, 8, 16, 32) and (config[0] != 32 or lanes == 32)
-        else:
-            assert 32 * rows >= n and warps in (4, 8) and not (rows == 4 and warps == 4)
+        elif n <= 128:  # larger orders run on the batched kernels, their shape is unused
+            assert 32 * rows >= n and (rows, warps) in [(2, 2), (2, 4), (2, 8), (3, 4), (3, 8), (4, 8)]
             if config[2] and 32 * config[2] >= n:
                 assert (warps, rows) == (config[1], config[2])
 
