@@ -9,7 +9,8 @@ not in L2 (126 MB) when the step starts; no L2 flush is needed.
 
   value       matrices/s of the whole chain, device time, inputs resident in HBM;
   e2e         the same through the C ABI from pinned host buffers: H2D of A and B, the chain,
-              D2H of X, inv(A) and info inside the timed region;
+              D2H of X, inv(A) and info inside the timed region, the batch in 16 chunks over
+              three streams so that both copy directions and the chain overlap;
   roofline    the dominant kernel's algorithmic bytes per launch / its CUDA-event duration,
               against the measured HBM copy bandwidth (MEASURED_PEAKS.json);
   cpu_baseline  the reference's CPU golden path (LAPACK through its test headers, built in
@@ -33,6 +34,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "getrf+getrs batched matrices/s: mixed/grouped vs plain FP32 at equal FP64 err"
 N, BATCH, NRHS = 32, 131072, 4
+E2E_CHUNKS = 16  # e2e leg: chunks of the batch pipelined over three streams
 FALLBACK_HBM_GBS = 6650.0
 
 # Algorithmic bytes per matrix (reads + writes of each kernel):
@@ -406,6 +408,40 @@ def section_adjoint(ob, h, dev, reps=3, batch=65536):
             "GFLOP_s_forward": (2 * n ** 3 / 3 + 2 * n * n * nrhs) * batch / (t_f * 1e-3) / 1e9,
             "cpu_baseline_forward": cpu_section_baseline([n] * batch, nrhs, "n = 64, nrhs = 8, N(0,1) (the reference has no adjoint)")}
 
+def section_matinv(ob, h, dev, peak, reps=5, batch=131072):
+    """aclblasSmatinvBatched at the chain's shape, n = 32 (512 MiB of input, larger than L2): the
+    fused launch against the two-call sequence the reference's matinv runs -- a copy of A,
+    aclblasSgetrfBatched on it, aclblasSgetriBatched into Ainv."""
+    import torch
+
+    n = 32
+    g = torch.Generator(device=dev).manual_seed(7)
+    A = torch.randn(batch, n, n, device=dev, generator=g)
+    Ainv, LU = torch.empty_like(A), torch.empty_like(A)
+    pa, pc, pl = ob.ptr_array(A), ob.ptr_array(Ainv), ob.ptr_array(LU)
+    piv = torch.empty((batch, n), dtype=torch.int32, device=dev)
+    info = torch.empty(batch, dtype=torch.int32, device=dev)
+    finfo = torch.empty(batch, dtype=torch.int32, device=dev)
+
+    def fused():
+        h.matinv(A, n, n, Ainv, n, info=info, aptr=pa, cptr=pc)
+
+    def two_call():
+        LU.copy_(A)
+        h.getrf(LU, n, n, piv=piv, info=finfo, aptr=pl)
+        h.getri(LU, n, n, piv, Ainv, n, info=info, aptr=pl, cptr=pc)
+
+    t_f = _events_ms(fused, reps)
+    t_s = _events_ms(two_call, reps)
+    alg = (8 * n * n + 20) * batch  # A read, Ainv written, info, two pointers
+    return {"workload": f"matinv_n32_b{batch}", "fused_matrices_s": batch / (t_f * 1e-3),
+            "two_call_matrices_s": batch / (t_s * 1e-3), "speedup_vs_two_call": t_s / t_f,
+            "ms": {"fused": t_f, "two_call": t_s},
+            "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved_GB_s": alg / (t_f * 1e-3) / 1e9,
+                         "frac": alg / (t_f * 1e-3) / 1e9 / peak},
+            "two_call_note": "copy of A + getrf + getri, the reference matinv's device sequence"}
+
+
 def run_section(args):
     """One measured section on its own (used for profiling captures with --small)."""
     import torch
@@ -418,6 +454,8 @@ def run_section(args):
         out = section_grouped(ob, h, dev, peak, reps=2, instances=5000 if args.small else 50000)
     elif args.section == "mixed":
         out = section_mixed(ob, h, dev, reps=2, sizes=((256, 148), (512, 32)) if args.small else ((256, 2048), (512, 256)))
+    elif args.section == "matinv":
+        out = section_matinv(ob, h, dev, peak, reps=2, batch=65536 if args.small else 131072)
     else:
         out = section_adjoint(ob, h, dev, reps=2, batch=8192 if args.small else 65536)
     print(json.dumps({"section": args.section, "small": bool(args.small), **out}))
@@ -433,7 +471,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sections", action="store_true", help="skip the grouped / mixed / adjoint measurements")
-    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint"],
+    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv"],
                     help="run only this measured section (one JSON line) and exit")
     ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
     args = ap.parse_args()
@@ -526,20 +564,42 @@ def main():
     hostC = torch.empty_like(hostA).pin_memory()
     hostI = torch.empty(BATCH, dtype=torch.int32).pin_memory()
     dA, dB = A0[0], B0[0]
+    # The batch goes through in E2E_CHUNKS chunks round-robin over three streams (one handle
+    # each), so the host-to-device copy of one chunk, the chain of the previous one and the
+    # device-to-host copy of the one before run at the same time (PCIe is full duplex).
+    e2e_streams = [torch.cuda.Stream(dev) for _ in range(3)]
+    e2e_handles = [ob.Handle(stream=s_) for s_ in e2e_streams]
+    per_chunk = (BATCH + E2E_CHUNKS - 1) // E2E_CHUNKS
 
     def e2e_step():
-        dA.copy_(hostA, non_blocking=True)
-        dB.copy_(hostB, non_blocking=True)
-        h.getrf(dA, N, N, piv=piv, info=info, aptr=aptr[0])
-        h.getrs("N", dA, N, N, piv, dB, NRHS, N, aptr=aptr[0], bptr=bptr[0])
-        h.getri(dA, N, N, piv, Cinv, N, info=rinfo, aptr=aptr[0], cptr=cptr)
-        hostX.copy_(dB, non_blocking=True)
-        hostC.copy_(Cinv, non_blocking=True)
-        hostI.copy_(rinfo, non_blocking=True)
+        head = torch.cuda.Event()
+        head.record(stream)
+        for s_ in e2e_streams:
+            s_.wait_event(head)
+        for c in range(E2E_CHUNKS):
+            i0, i1 = c * per_chunk, min(BATCH, (c + 1) * per_chunk)
+            if i0 >= i1:
+                break
+            s_, hh = e2e_streams[c % 3], e2e_handles[c % 3]
+            with torch.cuda.stream(s_):
+                a_, b_, ap, bp = dA[i0:i1], dB[i0:i1], aptr[0][i0:i1], bptr[0][i0:i1]
+                a_.copy_(hostA[i0:i1], non_blocking=True)
+                b_.copy_(hostB[i0:i1], non_blocking=True)
+                hh.getrf(a_, N, N, piv=piv[i0:i1], info=info[i0:i1], aptr=ap)
+                hh.getrs("N", a_, N, N, piv[i0:i1], b_, NRHS, N, aptr=ap, bptr=bp)
+                hh.getri(a_, N, N, piv[i0:i1], Cinv[i0:i1], N, info=rinfo[i0:i1], aptr=ap, cptr=cptr[i0:i1])
+                hostX[i0:i1].copy_(b_, non_blocking=True)
+                hostC[i0:i1].copy_(Cinv[i0:i1], non_blocking=True)
+                hostI[i0:i1].copy_(rinfo[i0:i1], non_blocking=True)
+        for s_ in e2e_streams:
+            tail = torch.cuda.Event()
+            tail.record(s_)
+            stream.wait_event(tail)
 
     for _ in range(2):
         e2e_step()
     torch.cuda.synchronize()
+    assert int(hostI.max()) == 0
     if dist:
         dist.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -585,13 +645,14 @@ def main():
                          "unit": "GB/s", "frac": kern[dom]["frac_hbm"], "peak_source": peak_kind,
                          "traffic": traffic, "alg_bytes_per_launch": ALG_BYTES[dom] * BATCH},
             "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "matrices/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                    "pipeline": f"{E2E_CHUNKS} chunks over 3 streams"},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks.summary(),
         }
         if world == 1 and not args.no_sections:
             line["sections"] = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
-                                "adjoint": section_adjoint(ob, h, dev)}
+                                "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline()

@@ -108,6 +108,25 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetriBatched(
     aclblasHandle_t handle, int n, const float* const Aarray[], int lda, const int* PivotArray,
     float* const Carray[], int ldc, int* infoArray, int batchSize);
 
+/* Replaces aclblasSgemmBatched (include/cann_ops_blas.h:415;
+ * blas/gemm_batched/arch35/gemm_batched_host.cpp:397-435). C[i] = alpha * op(A[i]) * op(B[i]) +
+ * beta * C[i] in FP32 (plain FP32 products and accumulation), alpha and beta host floats. k == 0
+ * or alpha == 0 scales C by beta (beta == 1: C untouched); an operation outside N/T/C is
+ * INVALID_VALUE. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgemmBatched(
+    aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m, int n, int k,
+    const float* alpha, const float* const Aarray[], int lda, const float* const Barray[], int ldb,
+    const float* beta, float* const Carray[], int ldc, int batchCount);
+
+/* Replaces aclblasSmatinvBatched (include/cann_ops_blas.h:434;
+ * blas/matinv_batched/arch35/matinv_batched_host.cpp:44-257). Ainv[i] = inverse of A[i] for
+ * n <= 32, as aclblasSgetrfBatched on a copy of A followed by aclblasSgetriBatched (bit for
+ * bit), in one launch and without workspace. info (required, device) receives 0, or the getri's
+ * j+1 for the highest-index j with U(j,j) == 0 when A is singular. n > 32 is INVALID_VALUE. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSmatinvBatched(
+    aclblasHandle_t handle, int n, const float* const A[], int lda, float* const Ainv[], int lda_inv, int* info,
+    int batchSize);
+
 /* Replaces aclblasGemmBatchedEx (include/cann_ops_blas.h:409;
  * blas/gemm_batched_ex/arch35/gemm_batched_ex_host.cpp:156-581). C[i] = alpha*op(A[i])*op(B[i]) +
  * beta*C[i]; alpha and beta are HOST pointers to float. Validation order: handle, alpha/beta

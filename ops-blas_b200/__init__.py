@@ -50,6 +50,9 @@ SIGNATURES = {
     "aclblasSgetrsBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip,
                                        C.c_int]),
     "aclblasSgetriBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int]),
+    "aclblasSmatinvBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
+    "aclblasSgemmBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp,
+                                      C.c_int, _vp, _vp, C.c_int, C.c_int]),
     "aclblasGemmBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int,
                                        _vp, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "aclblasSgetrfsRefineBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp,
@@ -235,6 +238,28 @@ class Handle:
         cptr = ptr_array(Cinv) if cptr is None else cptr
         check("aclblasSgetriBatched", lib().aclblasSgetriBatched(
             self.h, n, aptr.data_ptr(), lda, _addr(piv), cptr.data_ptr(), ldc, info.data_ptr(), LU.shape[0]))
+        return info
+
+    def sgemm(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, aptr=None, bptr=None,
+              cptr=None):
+        """aclblasSgemmBatched over batch tensors A, B, C (column-major matrices); alpha, beta floats."""
+        aptr = ptr_array(A) if aptr is None else aptr
+        bptr = ptr_array(B) if bptr is None else bptr
+        cptr = ptr_array(Cm) if cptr is None else cptr
+        al, be = C.c_float(alpha), C.c_float(beta)
+        check("aclblasSgemmBatched", lib().aclblasSgemmBatched(
+            self.h, TRANS[transa], TRANS[transb], m, n, k, C.byref(al), aptr.data_ptr(), lda, bptr.data_ptr(), ldb,
+            C.byref(be), cptr.data_ptr(), ldc, Cm.shape[0]))
+
+    def matinv(self, A, n, lda, Ainv, lda_inv, info=None, aptr=None, cptr=None):
+        """Ainv = inverse of every matrix of A (n <= 32) in one launch; returns the info tensor."""
+        torch = _torch()
+        if info is None:
+            info = torch.empty(A.shape[0], dtype=torch.int32, device=A.device)
+        aptr = ptr_array(A) if aptr is None else aptr
+        cptr = ptr_array(Ainv) if cptr is None else cptr
+        check("aclblasSmatinvBatched", lib().aclblasSmatinvBatched(
+            self.h, n, aptr.data_ptr(), lda, cptr.data_ptr(), lda_inv, info.data_ptr(), A.shape[0]))
         return info
 
 

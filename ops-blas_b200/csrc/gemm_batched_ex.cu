@@ -124,16 +124,18 @@ gemm_batched_simt_kernel(bool transA, bool transB, int m, int n, int k, float al
     }
 }
 
-// k == 0 or alpha == 0: C = beta * C (beta == 0 writes zeros), as the reference's early-exit
-// kernel (gemm_batched_ex_host.cpp:462-491).
-template <GemmElem TC>
+// k == 0 or alpha == 0: C = beta * C. GemmBatchedEx writes zeros for beta == 0, as its
+// reference early-exit kernel (gemm_batched_ex_host.cpp:462-491); SgemmBatched multiplies
+// unconditionally, as its reference (gemm_batched_host.cpp:350-390, GemmBatchedEarlyExitOp in
+// gemm_batched_kernel.cpp:682-760: Muls by beta), so 0 * Inf or NaN stays NaN there.
+template <GemmElem TC, bool ZERO_ON_BETA0 = true>
 __global__ void gemm_batched_scale_kernel(int m, int n, float beta, void* const* Carray, int ldc)
 {
     void* C = Carray[blockIdx.x];  // one CTA per matrix
     for (long long e = threadIdx.x; e < (long long)m * n; e += blockDim.x) {
         const long long i = e % m, j = e / m;
         const long long idx = i + j * ldc;
-        store_elem<TC>(C, idx, beta == 0.0f ? 0.0f : beta * load_elem<TC>(C, idx));
+        store_elem<TC>(C, idx, (ZERO_ON_BETA0 && beta == 0.0f) ? 0.0f : beta * load_elem<TC>(C, idx));
     }
 }
 
@@ -301,4 +303,55 @@ extern "C" aclblasStatus_t aclblasGemmBatchedEx(
             return ACLBLAS_STATUS_NOT_SUPPORTED;
     }
     return launch_status(kApi, err);
+}
+
+// aclblasSgemmBatched (include/cann_ops_blas.h:415; gemm_batched_host.cpp:397-435): FP32 batched
+// GEMM with plain FP32 products (the reference disables HF32), on the same FP32 CUDA-core kernel
+// as GemmBatchedEx with COMPUTE_32F operands; alpha and beta are host floats applied in the
+// kernel's epilogue. Validation order of ValidateSgemmBatchedParams (:53-98); an operation value
+// outside N/T/C is INVALID_VALUE there (not INVALID_ENUM).
+extern "C" aclblasStatus_t aclblasSgemmBatched(aclblasHandle_t handle, aclblasOperation_t transa,
+                                               aclblasOperation_t transb, int m, int n, int k, const float* alpha,
+                                               const float* const Aarray[], int lda, const float* const Barray[],
+                                               int ldb, const float* beta, float* const Carray[], int ldc,
+                                               int batchCount)
+{
+    using namespace opsblas;
+    static const char* kApi = "aclblasSgemmBatched";
+    if (handle == nullptr) {
+        log_error(kApi, "handle is nullptr");
+        return ACLBLAS_STATUS_HANDLE_IS_NULLPTR;
+    }
+    if (alpha == nullptr || beta == nullptr) {
+        log_error(kApi, "alpha and beta must not be nullptr");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (m < 0 || n < 0 || k < 0 || batchCount < 0) {
+        log_error(kApi, "invalid dimensions (m=%d n=%d k=%d batch=%d)", m, n, k, batchCount);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (!valid_op(transa) || !valid_op(transb)) {
+        log_error(kApi, "invalid transa=%d or transb=%d", (int)transa, (int)transb);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    const bool ta = transa != ACLBLAS_OP_N, tb = transb != ACLBLAS_OP_N;
+    if (lda < max1(ta ? k : m) || ldb < max1(tb ? n : k) || ldc < max1(m)) {
+        log_error(kApi, "invalid leading dimension (lda=%d ldb=%d ldc=%d)", lda, ldb, ldc);
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (batchCount > 0 && (Aarray == nullptr || Barray == nullptr || Carray == nullptr)) {
+        log_error(kApi, "Aarray, Barray and Carray must not be nullptr when batchCount > 0");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    if (m == 0 || n == 0 || batchCount == 0) return ACLBLAS_STATUS_SUCCESS;
+    const float a = *alpha, b = *beta;
+    cudaStream_t st = handle->stream;
+    if (k == 0 || a == 0.0f) {
+        if (b == 1.0f) return ACLBLAS_STATUS_SUCCESS;
+        gemm_batched_scale_kernel<GemmElem::F32, false><<<(unsigned)batchCount, 256, 0, st>>>(
+            m, n, b, reinterpret_cast<void* const*>(Carray), ldc);
+        return launch_status(kApi, cudaGetLastError());
+    }
+    return launch_status(kApi, gemm_f32_launch(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b, Carray, ldc,
+                                               batchCount, 0));
 }

@@ -183,6 +183,80 @@ GETRI_ERRORS = [
     ("TC_L1_E06", 32, 32, 32, 4, False, False, True, False, IV),
 ]
 
+# aclblasSmatinvBatched success rows of test/matinv_batched/arch35/matinv_batched_test.csv with
+# work to do: (name, n, lda, lda_inv, batch, matrix_type); every row uses random_seed 42.
+MATINV_CASES = [
+    ("TC_L0_01", 4, 4, 4, 1, "RANDOM_NONSINGULAR"),
+    ("TC_L0_02", 8, 8, 8, 2, "RANDOM_NONSINGULAR"),
+    ("TC_L0_03", 16, 16, 16, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L0_04", 32, 32, 32, 8, "RANDOM_NONSINGULAR"),
+    ("TC_L0_05", 1, 1, 1, 1, "RANDOM_NONSINGULAR"),
+    ("TC_L0_06", 2, 2, 2, 1, "RANDOM_NONSINGULAR"),
+    ("TC_L0_07", 4, 4, 4, 2, "RANDOM_NONSINGULAR"),
+    ("TC_L0_08", 8, 8, 8, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L0_09", 16, 16, 16, 8, "RANDOM_NONSINGULAR"),
+    ("TC_L0_10", 32, 32, 32, 1, "RANDOM_NONSINGULAR"),
+    ("TC_L0_11", 1, 1, 1, 8, "RANDOM_NONSINGULAR"),
+    ("TC_L0_12", 4, 4, 4, 2, "IDENTITY"),
+    ("TC_L0_16", 3, 3, 3, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L0_17", 8, 8, 8, 2, "SINGULAR_ZERO_COL"),
+    ("TC_L0_18", 5, 5, 5, 2, "RANDOM_NONSINGULAR"),
+    ("TC_L0_19", 20, 20, 20, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L1_01", 8, 8, 8, 64, "RANDOM_NONSINGULAR"),
+    ("TC_L1_02", 8, 8, 8, 128, "RANDOM_NONSINGULAR"),
+    ("TC_L1_03", 4, 4, 4, 256, "RANDOM_NONSINGULAR"),
+    ("TC_L1_04", 4, 4, 4, 512, "RANDOM_NONSINGULAR"),
+    ("TC_L1_05", 4, 4, 4, 1024, "RANDOM_NONSINGULAR"),
+    ("TC_L1_06", 32, 32, 32, 64, "RANDOM_NONSINGULAR"),
+    ("TC_L1_07", 32, 32, 32, 256, "RANDOM_NONSINGULAR"),
+    ("TC_L1_08", 32, 32, 32, 512, "RANDOM_NONSINGULAR"),
+    ("TC_L1_09", 32, 32, 32, 1024, "RANDOM_NONSINGULAR"),
+    ("TC_L1_10", 16, 16, 16, 512, "RANDOM_NONSINGULAR"),
+    ("TC_L1_11", 1, 1, 1, 1024, "RANDOM_NONSINGULAR"),
+    ("TC_L1_12", 16, 16, 16, 4, "SINGULAR_ZERO_COL"),
+    ("TC_L1_13", 8, 8, 8, 4, "SINGULAR_ZERO_COL"),
+    ("TC_L1_14", 16, 16, 16, 4, "SINGULAR_DEPENDENT_ROW"),
+    ("TC_L1_15", 16, 16, 16, 4, "MIXED"),
+    ("TC_L1_16", 8, 8, 8, 4, "MIXED"),
+    ("TC_L1_17", 7, 7, 7, 2, "RANDOM_NONSINGULAR"),
+    ("TC_L1_18", 12, 12, 12, 8, "RANDOM_NONSINGULAR"),
+    ("TC_L1_19", 24, 24, 24, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L1_20", 8, 16, 8, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L1_21", 8, 8, 16, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L1_22", 16, 32, 32, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L1_23", 4, 32, 4, 2, "RANDOM_NONSINGULAR"),
+    ("TC_L1_24", 4, 32, 32, 4, "RANDOM_NONSINGULAR"),
+    ("TC_L1_25", 16, 16, 16, 2, "IDENTITY"),
+    ("TC_L1_26", 8, 8, 8, 2, "DIAGONAL"),
+    ("TC_L1_27", 16, 16, 16, 4, "DIAGONALLY_DOMINANT"),
+    ("TC_L1_28", 8, 8, 8, 2, "UPPER_TRIANGULAR"),
+    ("TC_L1_29", 8, 8, 8, 2, "LOWER_TRIANGULAR"),
+    ("TC_L1_OBS_01", 4, 4, 4, 2, "ILL_CONDITIONED"),
+]
+MATINV_SEED = 42
+
+# aclblasSmatinvBatched rows of test/matinv_batched/arch35/matinv_batched_test.csv that expect an
+# error or the empty-operation success: (name, n, lda, lda_inv, batch, null_a, null_ainv,
+# null_info, status)
+MATINV_ARG_ROWS = [
+    ("TC_L0_13", 0, 1, 1, 4, False, False, False, S),
+    ("TC_L0_14", 32, 32, 32, 0, False, False, False, S),
+    ("TC_L0_15", 0, 1, 1, 0, False, False, False, S),
+    ("TC_L0_E02", -1, 1, 1, 4, False, False, False, IV),
+    ("TC_L0_E03", 33, 33, 33, 4, False, False, False, IV),
+    ("TC_L0_E04", 16, 16, 16, -1, False, False, False, IV),
+    ("TC_L1_E01", 16, 8, 16, 4, False, False, False, IV),
+    ("TC_L1_E02", 16, 16, 8, 4, False, False, False, IV),
+    ("TC_L1_E03", 16, 16, 16, 4, True, False, False, IV),
+    ("TC_L1_E04", 16, 16, 16, 4, False, True, False, IV),
+    ("TC_L1_E05", 16, 16, 16, 4, False, False, True, IV),
+    ("TC_L1_E06", -100, 1, 1, 4, False, False, False, IV),
+    ("TC_L1_E07", 64, 64, 64, 4, False, False, False, IV),
+    ("TC_L1_E08", 0, 0, 1, 4, False, False, False, IV),
+    ("TC_L1_E09", 16, 16, 16, 4, True, True, True, IV),
+    ("TC_L1_E10", 0, 1, 0, 4, False, False, False, IV),
+]
+
 
 def work(case) -> int:
     """Rough n^3 * batch size, to keep the slowest CPU-side checks optional."""
@@ -217,3 +291,200 @@ GEMM_ERRORS = [
     ("L1_42", "N", "N", 128, 128, 128, "F16", "F16", "F16", 128, 128, 128, 4, "16F", 1, 0, 0, 0, 0, 0, 0,
      "NOT_SUPPORTED"),
 ]
+
+# aclblasSgemmBatched rows of test/gemm_batched/sgemm_batched/arch35/sgemm_batched_test.csv.
+# Success rows: name transA transB m n k alpha beta lda ldb ldc batch c_fill (0 = the default
+# leading dimension; c_fill Z = zeros, R = N(0,1); A and B are N(0,1) in every row).
+_SGEMM_OK = """
+L0_012 N N 0 128 128 1 0 0 0 0 4 Z
+L0_013 N N 128 0 128 1 0 0 0 0 4 Z
+L0_014 N N 128 128 0 1 0 0 0 0 4 Z
+L0_015 N N 128 128 128 1 0 0 0 0 0 Z
+G1_Msweep_001 N N 1 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_002 N N 3 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_003 N N 13 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_004 N N 32 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_005 N N 55 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_006 N N 64 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_007 N N 128 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_008 N N 234 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_009 N N 256 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_010 N N 591 64 64 1.0 0.0 0 0 0 1 Z
+G1_Msweep_011 N N 512 64 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_012 N N 64 1 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_013 N N 64 3 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_014 N N 64 13 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_015 N N 64 32 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_016 N N 64 55 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_017 N N 64 128 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_018 N N 64 234 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_019 N N 64 256 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_020 N N 64 591 64 1.0 0.0 0 0 0 1 Z
+G1_Nsweep_021 N N 64 512 64 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_022 N N 64 64 1 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_023 N N 64 64 3 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_024 N N 64 64 13 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_025 N N 64 64 32 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_026 N N 64 64 55 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_027 N N 64 64 128 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_028 N N 64 64 234 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_029 N N 64 64 256 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_030 N N 64 64 591 1.0 0.0 0 0 0 1 Z
+G1_Ksweep_031 N N 64 64 512 1.0 0.0 0 0 0 1 Z
+G2_Mixed_032 N N 1 3 13 1.0 0.0 0 0 0 1 Z
+G2_Mixed_033 N N 32 55 64 1.0 0.0 0 0 0 1 Z
+G2_Mixed_034 N N 128 234 256 1.0 0.0 0 0 0 1 Z
+G2_Mixed_035 N N 591 512 128 1.0 0.0 0 0 0 1 Z
+G2_Mixed_036 N N 256 13 55 1.0 0.0 0 0 0 1 Z
+G2_Mixed_037 N N 512 234 3 1.0 0.0 0 0 0 1 Z
+G2_Mixed_038 N N 55 256 591 1.0 0.0 0 0 0 1 Z
+G2_Mixed_039 N N 234 128 1 1.0 0.0 0 0 0 1 Z
+G2_Mixed_040 N N 13 591 32 1.0 0.0 0 0 0 1 Z
+G2_Mixed_041 N N 3 512 234 1.0 0.0 0 0 0 1 Z
+G3_Trans_042 N N 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_043 N T 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_044 N C 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_045 T N 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_046 T T 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_047 T C 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_048 C N 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_049 C T 64 64 64 1.5 0.3 0 0 0 1 R
+G3_Trans_050 C C 64 64 64 1.5 0.3 0 0 0 1 R
+G4_Alpha_051 N N 64 64 64 0.0 0.0 0 0 0 1 Z
+G4_Alpha_052 N N 64 64 64 0.3 0.0 0 0 0 1 Z
+G4_Alpha_053 N N 64 64 64 0.5 0.0 0 0 0 1 Z
+G4_Alpha_054 N N 64 64 64 0.7 0.0 0 0 0 1 Z
+G4_Alpha_055 N N 64 64 64 1.0 0.0 0 0 0 1 Z
+G4_Alpha_056 N N 64 64 64 1.2 0.0 0 0 0 1 Z
+G4_Alpha_057 N N 64 64 64 1.7 0.0 0 0 0 1 Z
+G4_Alpha_058 N N 64 64 64 2.0 0.0 0 0 0 1 Z
+G4_Alpha_059 N N 64 64 64 2.3 0.0 0 0 0 1 Z
+G5_Beta_060 N N 64 64 64 1.0 0.0 0 0 0 1 Z
+G5_Beta_061 N N 64 64 64 1.0 0.3 0 0 0 1 R
+G5_Beta_062 N N 64 64 64 1.0 0.5 0 0 0 1 R
+G5_Beta_063 N N 64 64 64 1.0 0.7 0 0 0 1 R
+G5_Beta_064 N N 64 64 64 1.0 1.0 0 0 0 1 R
+G5_Beta_065 N N 64 64 64 1.0 1.2 0 0 0 1 R
+G5_Beta_066 N N 64 64 64 1.0 1.7 0 0 0 1 R
+G5_Beta_067 N N 64 64 64 1.0 2.0 0 0 0 1 R
+G5_Beta_068 N N 64 64 64 1.0 2.3 0 0 0 1 R
+G6_AB_069 N N 64 64 64 0.0 0.3 0 0 0 1 R
+G6_AB_070 N N 64 64 64 0.3 1.7 0 0 0 1 R
+G6_AB_071 N N 64 64 64 0.5 0.5 0 0 0 1 R
+G6_AB_072 N N 64 64 64 0.7 2.0 0 0 0 1 R
+G6_AB_073 N N 64 64 64 1.0 0.0 0 0 0 1 Z
+G6_AB_074 N N 64 64 64 1.2 1.2 0 0 0 1 R
+G6_AB_075 N N 64 64 64 1.7 0.3 0 0 0 1 R
+G6_AB_076 N N 64 64 64 2.0 0.5 0 0 0 1 R
+G6_AB_077 N N 64 64 64 2.3 1.0 0 0 0 1 R
+G6_AB_078 N N 64 64 64 0.0 0.0 0 0 0 1 Z
+G7_Batch_079 N N 64 64 64 1.5 0.3 0 0 0 1 R
+G7_Batch_080 N N 64 64 64 1.5 0.3 0 0 0 2 R
+G7_Batch_081 N N 64 64 64 1.5 0.3 0 0 0 3 R
+G7_Batch_082 N N 64 64 64 1.5 0.3 0 0 0 4 R
+G7_Batch_083 N N 64 64 64 1.5 0.3 0 0 0 8 R
+G8_Edge_084 N N 1 1 1 1.0 0.0 0 0 0 1 Z
+G8_Edge_085 N N 3 3 3 1.0 0.0 0 0 0 1 Z
+G8_Edge_086 N N 13 13 13 1.0 0.0 0 0 0 1 Z
+G8_Edge_087 N N 1 128 128 1.0 0.0 0 0 0 1 Z
+G8_Edge_088 N N 128 1 128 1.0 0.0 0 0 0 1 Z
+G8_Edge_089 N N 128 128 1 1.0 0.0 0 0 0 1 Z
+G8_Stress_090 T T 128 256 13 2.0 1.0 0 0 0 1 R
+G8_Stress_091 N T 256 128 55 1.7 0.7 0 0 0 1 R
+G8_Stress_092 N N 234 591 32 0.5 0.3 0 0 0 1 R
+G8_Stress_093 N N 512 512 64 1.0 0.0 0 0 0 1 Z
+G8_Stress_094 N N 512 512 512 1.0 0.0 0 0 0 1 Z
+G8_Stress_095 N N 512 512 512 1.5 0.3 0 0 0 1 R
+G8_Stress_096 N N 591 591 591 1.0 0.0 0 0 0 1 Z
+G8_Stress_097 N N 256 512 256 1.2 0.5 0 0 0 3 R
+G8_Stress_098 T N 128 128 128 0.7 1.7 0 0 0 3 R
+G8_Stress_099 N T 1 512 591 2.3 0.0 0 0 0 1 Z
+G9_NonAligned_100 N N 17 19 23 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_101 N T 17 19 23 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_102 T N 17 19 23 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_103 T T 17 19 23 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_104 N N 33 47 29 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_105 N T 33 47 29 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_106 T N 33 47 29 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_107 T T 33 47 29 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_108 N N 55 13 7 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_109 N T 55 13 7 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_110 T N 55 13 7 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_111 T T 55 13 7 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_112 N N 13 55 23 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_113 N T 13 55 23 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_114 T N 13 55 23 1.0 0.0 0 0 0 1 Z
+G9_NonAligned_115 T T 13 55 23 1.0 0.0 0 0 0 1 Z
+G10_LdLarge_116 N N 128 128 128 1.0 0.0 0 0 0 4 Z
+G10_LdLarge_117 N N 128 128 128 1.0 0.0 256 128 128 4 Z
+G10_LdLarge_118 N N 128 128 128 1.0 0.0 128 256 128 4 Z
+G10_LdLarge_119 N N 128 128 128 1.0 0.0 128 128 256 4 Z
+G11_K0_beta0_120 N N 128 128 0 1.0 0.0 0 0 0 4 Z
+G11_K0_beta1_121 N N 128 128 0 1.0 1.0 0 0 0 4 R
+G11_K0_beta0p5_122 N N 128 128 0 1.0 0.5 0 0 0 4 R
+G11_A0_beta1_123 N N 128 128 128 0.0 1.0 0 0 0 4 R
+G11_A0_beta0_124 N N 128 128 128 0.0 0.0 0 0 0 4 Z
+DIAG_M1_PP_NN N N 1 128 128 1.5 0.3 0 0 0 1 R
+DIAG_M1_PP_NN_b0 N N 1 128 128 2.0 0.0 0 0 0 1 Z
+DIAG_N1_PP_NN N N 128 1 128 1.5 0.3 0 0 0 1 R
+DIAG_M1_PP_NT N T 1 128 128 2.3 0.0 0 0 0 1 Z
+DIAG_M1_PP_TN T N 1 128 128 1.5 0.3 0 0 0 1 R
+DIAG_M3_PP_NN N N 3 128 128 1.5 0.3 0 0 0 1 R
+DIAG_M7_PP_NN N N 7 128 128 1.5 0.3 0 0 0 1 R
+DIAG_M8_PP_NN N N 8 128 128 1.5 0.3 0 0 0 1 R
+DIAG_M9_PP_NN N N 9 128 128 1.5 0.3 0 0 0 1 R
+G12_LargeBatch_155 N N 64 64 64 1.5 0.3 0 0 0 16 R
+G12_LargeBatch_156 N N 64 64 64 1.0 0.0 0 0 0 32 Z
+G12_LargeBatch_157 T T 32 32 32 1.7 0.7 0 0 0 64 R
+"""
+# Error rows: name transA transB m n k lda ldb ldc batch nulls(alpha beta A B C) null_handle status
+_SGEMM_ERR = """
+L0_016 N N 128 128 128 0 0 0 4 00000 1 HN
+L0_017 N N -1 128 128 0 0 0 4 00000 0 IV
+L0_018 N N 128 128 128 0 0 0 4 10000 0 IV
+L0_019 N N 128 128 128 0 0 0 4 01000 0 IV
+L0_020 N N 128 128 128 0 0 0 -1 00000 0 IV
+L0_021 N N 128 128 128 0 0 0 4 00100 0 IV
+L0_022 N N 128 128 128 0 0 0 4 00010 0 IV
+L0_023 N N 128 128 128 0 0 0 4 00001 0 IV
+L0_024 N N 128 128 128 64 128 128 4 00000 0 IV
+L0_025 N N 128 128 128 128 64 128 4 00000 0 IV
+L0_026 N N 128 128 128 128 128 64 4 00000 0 IV
+L0_027 T N 128 128 128 64 128 128 4 00000 0 IV
+L0_028 N N 128 -1 128 0 0 0 4 00000 0 IV
+L0_029 N N 128 128 -1 0 0 0 4 00000 0 IV
+L0_030 INVALID N 128 128 128 0 0 0 4 00000 0 IV
+L0_031 N INVALID 128 128 128 0 0 0 4 00000 0 IV
+"""
+
+
+def _sgemm_ld(v, default):
+    return int(v) if int(v) > 0 else max(1, default)
+
+
+def _sgemm_rows():
+    out = []
+    for line in _SGEMM_OK.split("\n"):
+        if not line.strip():
+            continue
+        name, ta, tb, m, n, k, alpha, beta, lda, ldb, ldc, batch, cfill = line.split()
+        m, n, k = int(m), int(n), int(k)
+        out.append((name, ta, tb, m, n, k, float(alpha), float(beta), _sgemm_ld(lda, k if ta != "N" else m),
+                    _sgemm_ld(ldb, n if tb != "N" else k), _sgemm_ld(ldc, m), int(batch), cfill))
+    return out
+
+
+def _sgemm_errors():
+    out = []
+    for line in _SGEMM_ERR.split("\n"):
+        if not line.strip():
+            continue
+        name, ta, tb, m, n, k, lda, ldb, ldc, batch, nulls, hn, status = line.split()
+        m, n, k = int(m), int(n), int(k)
+        out.append((name, ta, tb, m, n, k, _sgemm_ld(lda, k if ta == "T" else m), _sgemm_ld(ldb, n if tb == "T" else k),
+                    _sgemm_ld(ldc, m), int(batch), [c == "1" for c in nulls], hn == "1", {"IV": IV, "HN": HN}[status]))
+    return out
+
+
+SGEMM_CASES = _sgemm_rows()
+SGEMM_ERRORS = _sgemm_errors()

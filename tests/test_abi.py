@@ -15,7 +15,7 @@ import re
 
 import pytest
 
-from cases import GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS
+from cases import GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS, MATINV_ARG_ROWS, SGEMM_ERRORS
 from conftest import ROOT
 
 DUMMY = C.create_string_buffer(256)
@@ -144,6 +144,42 @@ def test_getri_noop_and_null_handle(ob):
     assert L.aclblasSgetriBatched(None, 32, None, 32, None, None, 32, None, 4) == ob.HANDLE_IS_NULLPTR
     assert L.aclblasSgetriBatched(H, 0, None, 1, None, None, 1, None, 4) == ob.SUCCESS
     assert L.aclblasSgetriBatched(H, 32, None, 32, None, None, 32, None, 0) == ob.SUCCESS
+
+
+@pytest.mark.parametrize("row", MATINV_ARG_ROWS, ids=lambda r: r[0])
+def test_matinv_argument_rows(ob, row):
+    name, n, lda, lda_inv, batch, null_a, null_ainv, null_info, status = row
+    st = ob.lib().aclblasSmatinvBatched(H, n, None if null_a else P, lda, None if null_ainv else P, lda_inv,
+                                        None if null_info else P, batch)
+    assert ob.STATUS[st] == status
+
+
+def test_matinv_null_handle(ob):
+    assert ob.lib().aclblasSmatinvBatched(None, -1, None, 0, None, 0, None, -1) == ob.HANDLE_IS_NULLPTR
+
+
+@pytest.mark.parametrize("row", SGEMM_ERRORS, ids=lambda r: r[0])
+def test_sgemm_batched_error_rows(ob, row):
+    name, ta, tb, m, n, k, lda, ldb, ldc, batch, nulls, null_h, status = row
+    one = C.c_float(1.0)
+    op = lambda t: 999 if t == "INVALID" else ob.TRANS[t]
+    ptr = lambda null, p: None if null else p
+    st = ob.lib().aclblasSgemmBatched(None if null_h else H, op(ta), op(tb), m, n, k, ptr(nulls[0], C.byref(one)),
+                                      ptr(nulls[2], P), lda, ptr(nulls[3], P), ldb, ptr(nulls[1], C.byref(one)),
+                                      ptr(nulls[4], P), ldc, batch)
+    assert ob.STATUS[st] == status
+
+
+def test_sgemm_batched_noops(ob):
+    L, one = ob.lib(), C.c_float(1.0)
+    # m, n or batch zero: success before any array is read (gemm_batched_host.cpp:420-422)
+    assert L.aclblasSgemmBatched(H, ob.OP_N, ob.OP_N, 0, 128, 128, C.byref(one), P, 1, P, 128, C.byref(one), P, 1,
+                                 4) == ob.SUCCESS
+    assert L.aclblasSgemmBatched(H, ob.OP_N, ob.OP_N, 8, 8, 8, C.byref(one), None, 8, None, 8, C.byref(one), None, 8,
+                                 0) == ob.SUCCESS
+    # k == 0 with beta == 1 leaves C untouched without a launch
+    assert L.aclblasSgemmBatched(H, ob.OP_N, ob.OP_N, 8, 8, 0, C.byref(one), P, 8, P, 1, C.byref(one), P, 8,
+                                 4) == ob.SUCCESS
 
 
 def test_logger_callback_receives_validation_errors(ob):
