@@ -442,6 +442,25 @@ def section_matinv(ob, h, dev, peak, reps=5, batch=131072):
             "two_call_note": "copy of A + getrf + getri, the reference matinv's device sequence"}
 
 
+def section_geqrf(ob, h, dev, peak, reps=5, batch=131072):
+    """aclblasSgeqrfBatched at the chain's shape, 32 x 32 (512 MiB of input, larger than L2):
+    in-place Householder QR, tau out."""
+    import torch
+
+    m = n = 32
+    g = torch.Generator(device=dev).manual_seed(9)
+    A0 = torch.randn(batch, n, m, device=dev, generator=g)
+    A = torch.empty_like(A0)
+    tau = torch.empty(batch, n, device=dev)
+    pa, pt = ob.ptr_array(A), ob.ptr_array(tau)
+    t = _events_ms(lambda: h.geqrf(A, m, n, m, tau=tau, aptr=pa, tptr=pt), reps, prep=lambda: A.copy_(A0))
+    alg = (8 * m * n + 4 * n + 16) * batch  # A read and written, tau, two pointers
+    return {"workload": f"geqrf_32x32_b{batch}", "matrices_s": batch / (t * 1e-3), "ms": t,
+            "GFLOP_s": (2 * m * n * n - 2 * n ** 3 / 3) * batch / (t * 1e-3) / 1e9,
+            "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved_GB_s": alg / (t * 1e-3) / 1e9,
+                         "frac": alg / (t * 1e-3) / 1e9 / peak}}
+
+
 def run_section(args):
     """One measured section on its own (used for profiling captures with --small)."""
     import torch
@@ -454,6 +473,8 @@ def run_section(args):
         out = section_grouped(ob, h, dev, peak, reps=2, instances=5000 if args.small else 50000)
     elif args.section == "mixed":
         out = section_mixed(ob, h, dev, reps=2, sizes=((256, 148), (512, 32)) if args.small else ((256, 2048), (512, 256)))
+    elif args.section == "geqrf":
+        out = section_geqrf(ob, h, dev, peak, reps=2, batch=65536 if args.small else 131072)
     elif args.section == "matinv":
         out = section_matinv(ob, h, dev, peak, reps=2, batch=65536 if args.small else 131072)
     else:
@@ -471,7 +492,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sections", action="store_true", help="skip the grouped / mixed / adjoint measurements")
-    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv"],
+    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv", "geqrf"],
                     help="run only this measured section (one JSON line) and exit")
     ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
     args = ap.parse_args()
@@ -652,7 +673,8 @@ def main():
         }
         if world == 1 and not args.no_sections:
             line["sections"] = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
-                                "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak)}
+                                "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak),
+                                "geqrf": section_geqrf(ob, h, dev, peak)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline()

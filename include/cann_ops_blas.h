@@ -108,6 +108,26 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetriBatched(
     aclblasHandle_t handle, int n, const float* const Aarray[], int lda, const int* PivotArray,
     float* const Carray[], int ldc, int* infoArray, int batchSize);
 
+/* Replaces aclblasSgeqrfBatched (include/cann_ops_blas.h:399;
+ * blas/geqrf_batched/arch35/sgeqrf_batched_host.cpp:19-141). Householder QR of every
+ * m x n matrix in place (R above, the reflectors below the diagonal), TauArray[i] receives
+ * min(m,n) scalars. info is HOST memory: 0, or the LAPACK-style -position of the first invalid
+ * argument (m=1, n=2, Aarray=3, lda=4, TauArray=5, batchSize=6). */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgeqrfBatched(
+    aclblasHandle_t handle, int m, int n, float* const Aarray[], int lda, float* const TauArray[], int* info,
+    int batchSize);
+
+/* Replaces aclblasSgelsBatched (include/cann_ops_blas.h:405;
+ * blas/gels_batched/arch35/sgels_batched_host.cpp:23-190). Least squares (m >= n after op) or
+ * minimum-norm (m < n) solutions of op(A[i]) X = C[i] by Householder QR / LQ, trans N or T;
+ * C[i] (ldc >= max(m, n)) receives the solutions, A[i] the factors (for T: of A^T, stored n x m
+ * with leading dimension n). devInfo[i] (device, one per matrix) is 0 or i+1 for a zero
+ * triangular diagonal. trans T needs lda * n <= 51200 (shared-memory transpose), otherwise
+ * NOT_SUPPORTED. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgelsBatched(
+    aclblasHandle_t handle, aclblasOperation_t trans, int m, int n, int nrhs, float* const Aarray[], int lda,
+    float* const Carray[], int ldc, int* devInfo, int batchSize);
+
 /* Replaces aclblasSgemmBatched (include/cann_ops_blas.h:415;
  * blas/gemm_batched/arch35/gemm_batched_host.cpp:397-435). C[i] = alpha * op(A[i]) * op(B[i]) +
  * beta * C[i] in FP32 (plain FP32 products and accumulation), alpha and beta host floats. k == 0

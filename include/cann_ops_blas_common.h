@@ -67,6 +67,20 @@ typedef enum aclblasGemmAlgo {
     ACLBLAS_GEMM_ALGO7 = 8
 } aclblasGemmAlgo_t;
 
+/* Host-side LAPACK-style info of the QR entry points (include/cann_ops_blas_common.h:122-132
+ * of the reference): 0, or -k when the k-th argument (handle and info not counted) is invalid. */
+typedef enum aclblasLapackInfo {
+    ACLBLAS_LAPACK_INFO_OK = 0,
+    ACLBLAS_LAPACK_INFO_ARG_1 = -1,
+    ACLBLAS_LAPACK_INFO_ARG_2 = -2,
+    ACLBLAS_LAPACK_INFO_ARG_3 = -3,
+    ACLBLAS_LAPACK_INFO_ARG_4 = -4,
+    ACLBLAS_LAPACK_INFO_ARG_5 = -5,
+    ACLBLAS_LAPACK_INFO_ARG_6 = -6,
+    ACLBLAS_LAPACK_INFO_ARG_7 = -7,
+    ACLBLAS_LAPACK_INFO_ARG_8 = -8
+} aclblasLapackInfo_t;
+
 #ifdef __cplusplus
 }
 #endif

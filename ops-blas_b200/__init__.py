@@ -51,6 +51,9 @@ SIGNATURES = {
                                        C.c_int]),
     "aclblasSgetriBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int]),
     "aclblasSmatinvBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
+    "aclblasSgeqrfBatched": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int]),
+    "aclblasSgelsBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp,
+                                      C.c_int]),
     "aclblasSgemmBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp,
                                       C.c_int, _vp, _vp, C.c_int, C.c_int]),
     "aclblasGemmBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int,
@@ -250,6 +253,32 @@ class Handle:
         check("aclblasSgemmBatched", lib().aclblasSgemmBatched(
             self.h, TRANS[transa], TRANS[transb], m, n, k, C.byref(al), aptr.data_ptr(), lda, bptr.data_ptr(), ldb,
             C.byref(be), cptr.data_ptr(), ldc, Cm.shape[0]))
+
+    def geqrf(self, A, m, n, lda, tau=None, aptr=None, tptr=None):
+        """In-place QR of every matrix of A (batch, n, lda); returns the tau tensor (batch, min(m,n))."""
+        torch = _torch()
+        if tau is None:
+            tau = torch.zeros((A.shape[0], max(1, min(m, n))), dtype=torch.float32, device=A.device)
+        aptr = ptr_array(A) if aptr is None else aptr
+        tptr = ptr_array(tau) if tptr is None else tptr
+        info = C.c_int(-99)
+        check("aclblasSgeqrfBatched", lib().aclblasSgeqrfBatched(
+            self.h, m, n, aptr.data_ptr(), lda, tptr.data_ptr(), C.byref(info), A.shape[0]))
+        assert info.value == 0, info.value
+        return tau
+
+    def gels(self, trans, A, m, n, nrhs, lda, Cm, ldc, info=None, aptr=None, cptr=None):
+        """aclblasSgelsBatched in place on batch tensors A (batch, n, lda) and C (batch, nrhs, ldc);
+        returns the per-matrix info tensor."""
+        torch = _torch()
+        if info is None:
+            info = torch.full((A.shape[0],), -1, dtype=torch.int32, device=A.device)
+        aptr = ptr_array(A) if aptr is None else aptr
+        cptr = ptr_array(Cm) if cptr is None else cptr
+        check("aclblasSgelsBatched", lib().aclblasSgelsBatched(
+            self.h, TRANS[trans], m, n, nrhs, aptr.data_ptr(), lda, cptr.data_ptr(), ldc, info.data_ptr(),
+            A.shape[0]))
+        return info
 
     def matinv(self, A, n, lda, Ainv, lda_inv, info=None, aptr=None, cptr=None):
         """Ainv = inverse of every matrix of A (n <= 32) in one launch; returns the info tensor."""

@@ -59,6 +59,9 @@ def lib():
                                             C.c_int64, C.c_int, C.c_int]
         L.oracle_sgetri_batched.argtypes = [C.c_int, _f32p, C.c_int64, C.c_int, _i32p, _f32p, C.c_int64, C.c_int,
                                             _i32p, C.c_int]
+        L.oracle_sgeqrf_batched.argtypes = [C.c_int, C.c_int, _f32p, C.c_int64, C.c_int, _f32p, C.c_int64, C.c_int]
+        L.oracle_sgels_batched.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_int64, C.c_int, _f32p,
+                                           C.c_int64, C.c_int, _i32p, C.c_int, _f32p]
         L.case_matrix_batch.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_int]
         L.case_rhs_batch.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_int]
         _lib = L
@@ -83,6 +86,10 @@ def ref():
                                          C.c_longlong, C.c_int, C.c_int, C.c_int]
         L.ref_sgetri_batched.argtypes = [C.c_int, _f32p, C.c_longlong, C.c_int, _i32p, _f32p, C.c_longlong, C.c_int,
                                          _i32p, C.c_int, C.c_int]
+        L.ref_sgels_batched.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_longlong, C.c_int, _f32p,
+                                        C.c_longlong, C.c_int, _i32p, C.c_int, C.c_int]
+        L.ref_sgeqrf_batched.argtypes = [C.c_int, C.c_int, _f32p, C.c_longlong, C.c_int, _f32p, C.c_longlong, _i32p,
+                                         C.c_int, C.c_int]
         if not L.ref_available():
             return None
         _ref = L
@@ -142,6 +149,28 @@ def port_getri(lu, n, lda, piv, c, ldc):
     return info
 
 
+def port_geqrf(a, m, n, lda):
+    """In-place Householder QR of every matrix of ``a`` (batch, n, lda); returns tau (batch, min(m,n))."""
+    _check(a, n, lda)
+    k = max(1, min(m, n))
+    tau = np.zeros((a.shape[0], k), np.float32)
+    lib().oracle_sgeqrf_batched(m, n, _p(a, _f32p), a.shape[1] * a.shape[2], lda, _p(tau, _f32p), k, a.shape[0])
+    return tau
+
+
+def port_gels(trans, a, m, n, nrhs, lda, c, ldc):
+    """In place: a (batch, n, lda) factored (transposed first for 'T'), c (batch, nrhs, ldc) the
+    solutions; returns info per matrix. trans in 'N', 'T'."""
+    _check(a, n, lda)
+    _check(c, nrhs, ldc)
+    info = np.zeros(a.shape[0], np.int32)
+    scratch = np.zeros(max(1, lda * n), np.float32)
+    lib().oracle_sgels_batched(1 if trans == "T" else 0, m, n, nrhs, _p(a, _f32p), a.shape[1] * a.shape[2], lda,
+                               _p(c, _f32p), c.shape[1] * c.shape[2], ldc, _p(info, _i32p), a.shape[0],
+                               _p(scratch, _f32p))
+    return info
+
+
 # ----------------------------------------------------------------- reference golden path --
 
 def ref_getrf(a, n, lda, pivot=True, nthreads=0):
@@ -177,6 +206,31 @@ def ref_getrs(trans, lu, n, lda, piv, b, nrhs, ldb, nthreads=0):
     rc = L.ref_sgetrs_batched(TRANS_ACL[trans], n, nrhs, _p(lu, _f32p), lu.shape[1] * lu.shape[2], lda,
                               _p(piv, _i32p), _p(b, _f32p), b.shape[1] * b.shape[2], ldb, lu.shape[0], nthreads)
     assert rc == 0, rc
+
+
+def ref_geqrf(a, m, n, lda, nthreads=0):
+    """aclblasSgeqrfBatched_cpu (LAPACK sgeqrf_) in place; returns tau (batch, min(m,n))."""
+    L = ref()
+    assert L is not None, "reference golden library unavailable"
+    _check(a, n, lda)
+    k = max(1, min(m, n))
+    tau = np.zeros((a.shape[0], k), np.float32)
+    info = np.zeros(1, np.int32)
+    rc = L.ref_sgeqrf_batched(m, n, _p(a, _f32p), a.shape[1] * a.shape[2], lda, _p(tau, _f32p), k, _p(info, _i32p),
+                              a.shape[0], nthreads)
+    assert rc == 0 and info[0] == 0, (rc, info[0])
+    return tau
+
+
+def ref_gels(trans, a, m, n, nrhs, lda, c, ldc, nthreads=0):
+    """aclblasSgelsBatched_cpu (LAPACK sgels_) per matrix; c receives the solution rows."""
+    L = ref()
+    assert L is not None, "reference golden library unavailable"
+    info = np.zeros(a.shape[0], np.int32)
+    rc = L.ref_sgels_batched(TRANS_ACL[trans], m, n, nrhs, _p(a, _f32p), a.shape[1] * a.shape[2], lda, _p(c, _f32p),
+                             c.shape[1] * c.shape[2], ldc, _p(info, _i32p), a.shape[0], nthreads)
+    assert rc == 0, rc
+    return info
 
 
 def ref_getri(lu, n, lda, piv, c, ldc, nthreads=0):
@@ -218,6 +272,22 @@ def mixed_tolerance_ok(out, gold):
         return False
     fails = np.count_nonzero(diff > 1.52587890625e-5 + 0.0009765625 * np.abs(g))
     return (count - fails) / count >= 0.99
+
+
+def mere_mare_ok(out, gold, threshold=1.0 / 8192.0, multiplier=10.0):
+    """The reference's MERE_MARE rule (test/frame/verify.h:153-200): elements equal or both NaN
+    are skipped; an Inf among the rest fails; with rel = |out - gold| / (|gold| + 2^-14), the mean
+    of rel must stay below ``threshold`` and its maximum below ``multiplier * threshold``."""
+    o = np.asarray(out, np.float32).ravel()
+    g = np.asarray(gold, np.float32).ravel()
+    skip = (o == g) | (np.isnan(o) & np.isnan(g))
+    o, g = o[~skip].astype(np.float64), g[~skip].astype(np.float64)
+    if o.size == 0:
+        return True
+    if np.any(np.isinf(o)) or np.any(np.isinf(g)):
+        return False
+    rel = np.abs(o - g) / (np.abs(g) + 2.0 ** -14)
+    return bool(rel.mean() < threshold and rel.max() < multiplier * threshold)
 
 
 def backward_error(M, x, b):

@@ -60,6 +60,8 @@ def build_ref(force: bool = False) -> str | None:
         os.path.join(REFERENCE_ROOT, "test/getrf_batched/sgetrf_batched/sgetrf_batched_golden.h"),
         os.path.join(REFERENCE_ROOT, "test/getrs_batched/sgetrs_batched_golden.h"),
         os.path.join(REFERENCE_ROOT, "test/getri_batched/sgetri_batched/sgetri_batched_golden.h"),
+        os.path.join(REFERENCE_ROOT, "test/geqrf_batched/sgeqrf_batched/sgeqrf_batched_golden.h"),
+        os.path.join(REFERENCE_ROOT, "test/gels_batched/sgels_batched/sgels_batched_golden.h"),
     ]
     if not all(os.path.exists(h) for h in hdrs):
         return REF_LIB if os.path.exists(REF_LIB) else None
@@ -75,6 +77,8 @@ def build_ref(force: bool = False) -> str | None:
         "-I", os.path.dirname(hdrs[0]),
         "-I", os.path.dirname(hdrs[1]),
         "-I", os.path.dirname(hdrs[2]),
+        "-I", os.path.dirname(hdrs[3]),
+        "-I", os.path.dirname(hdrs[4]),
         "-o", REF_LIB, src, "-ldl",
     ]
     subprocess.check_call(cmd)

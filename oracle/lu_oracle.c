@@ -246,3 +246,193 @@ ORACLE_API void oracle_sgetri_batched(
                       ldc, info + b);
     }
 }
+
+/* aclblasSgeqrfBatched (blas/geqrf_batched/arch35/sgeqrf_batched_kernel.cpp:44-190): unblocked
+ * Householder QR, for i = 0 .. min(m,n)-1:
+ *   sigma = sum_{r>i} A(r,i)^2 (ComputeSigma :94-111), x1 = A(i,i);
+ *   sigma == 0: tau = 0, A(i,i) unchanged, no update (ComputeTauAndNormalize :113-149);
+ *   else normX = sqrt(sigma + x1*x1), alpha = x1 >= 0 ? -normX : normX, tau = (alpha - x1) / alpha,
+ *        A(r,i) /= (x1 - alpha) for r > i, A(i,i) = alpha;
+ *   then for every column c > i (ComputeCoefficients :44-60, ApplyUpdate :62-83):
+ *        dot = A(i,c) + sum_{r>i} A(r,i) A(r,c), coef = tau * dot,
+ *        A(r,c) -= coef * A(r,i) for r > i, A(i,c) = A(i,c) - coef.
+ * The reference's sums are thread-tree reductions; this restatement (and the CUDA kernels,
+ * which follow it bit for bit) sums in row order with every product rounded before the add.
+ * Parity with the reference is by its own test rule: MIXED_TOLERANCE against LAPACK sgeqrf_
+ * (tests/test_geqrf_oracle.py). */
+/* a product rounded on its own (the file is compiled with -ffp-contract=off) */
+static inline float rmul(float a, float b) { return a * b; }
+
+static void oracle_sgeqrf(int m, int n, float* A, int lda, float* tau)
+{
+    const int k = m < n ? m : n;
+    for (int i = 0; i < k; i++) {
+        float* ci = A + (int64_t)i * lda;
+        float sigma = 0.0f;
+        for (int r = i + 1; r < m; r++) sigma = sigma + rmul(ci[r], ci[r]);
+        const float x1 = ci[i];
+        float t, alpha;
+        if (sigma == 0.0f) {
+            t = 0.0f;
+            alpha = x1;
+        } else {
+            const float normX = sqrtf(sigma + rmul(x1, x1));
+            alpha = (x1 >= 0.0f) ? -normX : normX;
+            t = (alpha - x1) / alpha;
+        }
+        tau[i] = t;
+        if (t == 0.0f) {
+            ci[i] = alpha;
+            continue;
+        }
+        const float vscale = x1 - alpha;
+        for (int r = i + 1; r < m; r++) ci[r] = ci[r] / vscale;
+        ci[i] = alpha;
+        for (int c = i + 1; c < n; c++) {
+            float* cc = A + (int64_t)c * lda;
+            float dot = cc[i];
+            for (int r = i + 1; r < m; r++) dot = dot + rmul(ci[r], cc[r]);
+            const float coef = rmul(t, dot);
+            for (int r = i + 1; r < m; r++) cc[r] = cc[r] - rmul(coef, ci[r]);
+            cc[i] = cc[i] - coef;
+        }
+    }
+}
+
+ORACLE_API void oracle_sgeqrf_batched(int m, int n, float* A, int64_t strideA, int lda, float* tau,
+                                      int64_t strideTau, int batch)
+{
+    for (int b = 0; b < batch; b++) oracle_sgeqrf(m, n, A + (int64_t)b * strideA, lda, tau + (int64_t)b * strideTau);
+}
+
+/* aclblasSgelsBatched (blas/gels_batched/arch35/sgels_batched_kernel.cpp:25-400), per matrix:
+ * trans T first transposes A in place into an n x m matrix of leading dimension n
+ * (SgelsTransposeSimt); then with (M, N) the effective shape:
+ *   M >= N: Householder QR (column reflectors: xnorm = ||A(k+1:,k)||; xnorm < 1e-30 with
+ *           A(k,k) >= 0 gives tau = 0; else the scaled norm nm = sc sqrt((akk/sc)^2 + (xnorm/sc)^2),
+ *           beta = -sign(akk) nm, tau = (beta - akk)/beta, v *= 1/(akk - beta), A(k,k) = beta,
+ *           columns j > k: w = v.a + a(k), a(k) -= tau w, a += (-tau w) v), Q^T applied to C the
+ *           same way, then back substitution R x = c per right-hand side; a zero R(i,i) sets
+ *           info = i + 1 and stops (the right-hand sides after the current one stay untouched);
+ *   M <  N: LQ with row reflectors, forward substitution L y = c (same stop rule), C rows M..N-1
+ *           zeroed, Q^T applied in reverse reflector order (the minimum-norm solution).
+ * Sums run in index order with each product rounded before the add, as in the CUDA kernel. */
+static float gels_norm(const float* v, int len, int stride)
+{
+    float ss = 0.0f;
+    for (int i = 0; i < len; i++) ss = ss + rmul(v[(int64_t)i * stride], v[(int64_t)i * stride]);
+    return sqrtf(ss);
+}
+
+/* Reflector k: returns 0 (tau = 0, no reflection) or 1 with tau and the scale of v. */
+static int gels_reflector(float akk, float xnorm, float* tau, float* beta, float* scalev)
+{
+    if (xnorm < 1.0e-30f && akk >= 0.0f) {
+        *tau = 0.0f;
+        return 0;
+    }
+    const float na = fabsf(akk);
+    const float sc = na > xnorm ? na : xnorm;
+    const float sa = akk / sc, sx = xnorm / sc;
+    const float nm = rmul(sc, sqrtf(rmul(sa, sa) + rmul(sx, sx)));
+    *beta = akk >= 0.0f ? -nm : nm;
+    *tau = (*beta - akk) / *beta;
+    *scalev = 1.0f / (akk - *beta);
+    return 1;
+}
+
+/* a(-stride) and a(0..len-1)*stride updated with the reflector (v, tau) */
+static void gels_apply(const float* v, int vstride, float* a, int astride, int len, float t)
+{
+    float w = 0.0f;
+    for (int i = 0; i < len; i++) w = w + rmul(v[(int64_t)i * vstride], a[(int64_t)i * astride]);
+    w = w + a[-(int64_t)astride];
+    a[-(int64_t)astride] = a[-(int64_t)astride] - rmul(t, w);
+    const float alpha = -rmul(t, w);
+    for (int i = 0; i < len; i++) a[(int64_t)i * astride] = a[(int64_t)i * astride] + rmul(alpha, v[(int64_t)i * vstride]);
+}
+
+static void oracle_sgels(int trans, int m, int n, int nrhs, float* A, int lda, float* C, int ldc, int* info,
+                         float* scratch)
+{
+    int M = m, N = n, ld = lda;
+    if (trans) {
+        memcpy(scratch, A, sizeof(float) * (size_t)lda * n);
+        for (int col = 0; col < m; col++)
+            for (int row = 0; row < n; row++) A[(int64_t)col * n + row] = scratch[(int64_t)row * lda + col];
+        M = n;
+        N = m;
+        ld = n;
+    }
+    const int k = M < N ? M : N;
+    float tau[4096];
+    if (M >= N) {
+        for (int kk = 0; kk < N; kk++) {
+            const int tail = M - kk - 1;
+            float* v = A + (int64_t)kk * ld + kk + 1;
+            const float akk = A[(int64_t)kk * ld + kk];
+            float beta = 0.0f, scalev = 0.0f;
+            if (!gels_reflector(akk, gels_norm(v, tail, 1), &tau[kk], &beta, &scalev)) continue;
+            A[(int64_t)kk * ld + kk] = beta;
+            for (int i = 0; i < tail; i++) v[i] = rmul(v[i], scalev);
+            for (int j = kk + 1; j < N; j++) gels_apply(v, 1, A + (int64_t)j * ld + kk + 1, 1, tail, tau[kk]);
+        }
+        for (int kk = 0; kk < k; kk++) {
+            if (tau[kk] == 0.0f) continue;
+            const float* v = A + (int64_t)kk * ld + kk + 1;
+            for (int j = 0; j < nrhs; j++) gels_apply(v, 1, C + (int64_t)j * ldc + kk + 1, 1, M - kk - 1, tau[kk]);
+        }
+        for (int j = 0; j < nrhs; j++) {
+            for (int i = N - 1; i >= 0; i--) {
+                const float rii = A[(int64_t)i * ld + i];
+                if (rii == 0.0f) {
+                    *info = i + 1;
+                    return;
+                }
+                float sum = 0.0f;
+                for (int p = i + 1; p < N; p++) sum = sum + rmul(A[(int64_t)p * ld + i], C[(int64_t)j * ldc + p]);
+                C[(int64_t)j * ldc + i] = (C[(int64_t)j * ldc + i] - sum) / rii;
+            }
+        }
+        *info = 0;
+    } else {
+        for (int kk = 0; kk < M; kk++) {
+            const int tail = N - kk - 1;
+            float* v = A + (int64_t)(kk + 1) * ld + kk;
+            const float akk = A[(int64_t)kk * ld + kk];
+            float beta = 0.0f, scalev = 0.0f;
+            if (!gels_reflector(akk, gels_norm(v, tail, ld), &tau[kk], &beta, &scalev)) continue;
+            A[(int64_t)kk * ld + kk] = beta;
+            for (int i = 0; i < tail; i++) v[(int64_t)i * ld] = rmul(v[(int64_t)i * ld], scalev);
+            for (int ii = kk + 1; ii < M; ii++) gels_apply(v, ld, A + (int64_t)(kk + 1) * ld + ii, ld, tail, tau[kk]);
+        }
+        *info = 0;
+        for (int j = 0; j < nrhs; j++) {
+            for (int i = 0; i < M; i++) {
+                const float lii = A[(int64_t)i * ld + i];
+                if (lii == 0.0f) {
+                    *info = i + 1;
+                    return;
+                }
+                float sum = 0.0f;
+                for (int p = 0; p < i; p++) sum = sum + rmul(A[(int64_t)p * ld + i], C[(int64_t)j * ldc + p]);
+                C[(int64_t)j * ldc + i] = (C[(int64_t)j * ldc + i] - sum) / lii;
+            }
+        }
+        for (int j = 0; j < nrhs; j++)
+            for (int i = M; i < N; i++) C[(int64_t)j * ldc + i] = 0.0f;
+        for (int kk = M - 1; kk >= 0; kk--) {
+            if (tau[kk] == 0.0f) continue;
+            const float* v = A + (int64_t)(kk + 1) * ld + kk;
+            for (int j = 0; j < nrhs; j++) gels_apply(v, ld, C + (int64_t)j * ldc + kk + 1, 1, N - kk - 1, tau[kk]);
+        }
+    }
+}
+
+ORACLE_API void oracle_sgels_batched(int trans, int m, int n, int nrhs, float* A, int64_t strideA, int lda, float* C,
+                                     int64_t strideC, int ldc, int* info, int batch, float* scratch)
+{
+    for (int b = 0; b < batch; b++)
+        oracle_sgels(trans, m, n, nrhs, A + (int64_t)b * strideA, lda, C + (int64_t)b * strideC, ldc, info + b,
+                     scratch);
+}

@@ -23,6 +23,8 @@
 #include "sgetrf_batched_golden.h"
 #include "sgetrs_batched_golden.h"
 #include "sgetri_batched_golden.h"
+#include "sgeqrf_batched_golden.h"
+#include "sgels_batched_golden.h"
 
 namespace {
 
@@ -30,6 +32,9 @@ using getrf_fn = void (*)(const int*, const int*, float*, const int*, int*, int*
 using getrs_fn = void (*)(const char*, const int*, const int*, const float*, const int*, const int*, float*,
                           const int*, int*);
 using getri_fn = void (*)(const int*, float*, const int*, int*, float*, const int*, int*);
+using geqrf_fn = void (*)(const int*, const int*, float*, const int*, float*, float*, const int*, int*);
+using gels_fn = void (*)(const char*, const int*, const int*, const int*, float*, const int*, float*, const int*,
+                        float*, const int*, int*);
 using nthreads_fn = void (*)(int);
 using config_fn = char* (*)();
 
@@ -37,6 +42,8 @@ struct Lapack {
     getrf_fn getrf = nullptr;
     getrs_fn getrs = nullptr;
     getri_fn getri = nullptr;
+    geqrf_fn geqrf = nullptr;
+    gels_fn gels = nullptr;
     config_fn config = nullptr;
     bool ok = false;
 };
@@ -55,10 +62,12 @@ Lapack& lapack()
         l.getrf = reinterpret_cast<getrf_fn>(dlsym(h, "scipy_sgetrf_"));
         l.getrs = reinterpret_cast<getrs_fn>(dlsym(h, "scipy_sgetrs_"));
         l.getri = reinterpret_cast<getri_fn>(dlsym(h, "scipy_sgetri_"));
+        l.geqrf = reinterpret_cast<geqrf_fn>(dlsym(h, "scipy_sgeqrf_"));
+        l.gels = reinterpret_cast<gels_fn>(dlsym(h, "scipy_sgels_"));
         l.config = reinterpret_cast<config_fn>(dlsym(h, "scipy_openblas_get_config"));
         auto setn = reinterpret_cast<nthreads_fn>(dlsym(h, "scipy_openblas_set_num_threads"));
         if (setn) setn(1);
-        l.ok = l.getrf && l.getrs && l.getri;
+        l.ok = l.getrf && l.getrs && l.getri && l.geqrf && l.gels;
         return l;
     }();
     return L;
@@ -97,6 +106,16 @@ void sgetrs_(const char* trans, const int* n, const int* nrhs, const float* a, c
 void sgetri_(const int* n, float* a, const int* lda, int* ipiv, float* work, const int* lwork, int* info)
 {
     lapack().getri(n, a, lda, ipiv, work, lwork, info);
+}
+void sgeqrf_(const int* m, const int* n, float* a, const int* lda, float* tau, float* work, const int* lwork,
+             int* info)
+{
+    lapack().geqrf(m, n, a, lda, tau, work, lwork, info);
+}
+void sgels_(const char* trans, const int* m, const int* n, const int* nrhs, float* a, const int* lda, float* b,
+            const int* ldb, float* work, const int* lwork, int* info)
+{
+    lapack().gels(trans, m, n, nrhs, a, lda, b, ldb, work, lwork, info);
 }
 }
 
@@ -178,6 +197,45 @@ REF_API int ref_sgetri_batched(int n, const float* LU, long long strideA, int ld
                                                       piv ? piv + (long long)b0 * n : nullptr, cp.data(), ldc,
                                                       info + b0, cnt);
         if (st != ACLBLAS_STATUS_SUCCESS) status = static_cast<int>(st);
+    });
+    return status;
+}
+
+/* aclblasSgeqrfBatched_cpu over a strided batch; returns its status, *info its LAPACK-style info. */
+REF_API int ref_sgeqrf_batched(int m, int n, float* A, long long strideA, int lda, float* tau, long long strideTau,
+                               int* info, int batch, int nthreads)
+{
+    if (!lapack().ok) return -1;
+    int status = 0;
+    *info = 0;
+    for_chunks(batch, nthreads, [&](int b0, int cnt) {
+        std::vector<float*> ap(cnt), tp(cnt);
+        for (int i = 0; i < cnt; i++) {
+            ap[i] = A + (long long)(b0 + i) * strideA;
+            tp[i] = tau + (long long)(b0 + i) * strideTau;
+        }
+        int inf = 0;
+        aclblasStatus_t st = aclblasSgeqrfBatched_cpu(dummy_handle(), m, n, ap.data(), lda, tp.data(), &inf, cnt);
+        if (st != ACLBLAS_STATUS_SUCCESS) status = static_cast<int>(st);
+    });
+    return status;
+}
+
+/* aclblasSgelsBatched_cpu one matrix at a time (its info is one value per call), over a strided
+ * batch; info receives each matrix's LAPACK info. */
+REF_API int ref_sgels_batched(int trans, int m, int n, int nrhs, float* A, long long strideA, int lda, float* C,
+                              long long strideC, int ldc, int* info, int batch, int nthreads)
+{
+    if (!lapack().ok) return -1;
+    int status = 0;
+    for_chunks(batch, nthreads, [&](int b0, int cnt) {
+        for (int i = 0; i < cnt; i++) {
+            float* a = A + (long long)(b0 + i) * strideA;
+            float* c = C + (long long)(b0 + i) * strideC;
+            aclblasStatus_t st = aclblasSgelsBatched_cpu(dummy_handle(), static_cast<aclblasOperation_t>(trans), m, n,
+                                                         nrhs, &a, lda, &c, ldc, info + b0 + i, 1);
+            if (st != ACLBLAS_STATUS_SUCCESS) status = static_cast<int>(st);
+        }
     });
     return status;
 }

@@ -488,3 +488,83 @@ def _sgemm_errors():
 
 SGEMM_CASES = _sgemm_rows()
 SGEMM_ERRORS = _sgemm_errors()
+
+
+# aclblasSgeqrfBatched rows of test/geqrf_batched/sgeqrf_batched/arch35/sgeqrf_batched_test.csv:
+# (name, m, n, lda, batch, a_fill, a_array_null, tau_array_null, status); the verification
+# multiplier of MERE_MARE (threshold 0.000122) is 10 except where GEQRF_MARE_MULTIPLIER says.
+GEQRF_MARE_MULTIPLIER = {"TC_L0_005": 15.0, "TC_L1_031": 1000.0, "TC_L1_032": 10000.0}
+GEQRF_ROWS = [
+    ("TC_L0_001", 4, 4, 4, 1, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_002", 8, 8, 8, 4, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_003", 16, 4, 16, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_004", 4, 16, 4, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_005", 32, 32, 32, 4, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_006", 0, 8, 1, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_007", 8, 0, 8, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_008", 8, 8, 8, 0, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_009", 1, 1, 1, 1, "RANDOM_NORM_2", False, False, S),
+    ("TC_L0_011", -1, 8, 1, 2, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L0_012", 8, -1, 8, 2, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L0_013", 8, 8, 4, 2, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L0_014", 8, 8, 8, -1, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L1_002", 64, 16, 64, 4, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_003", 16, 64, 16, 4, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_006", 8, 8, 16, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_007", 16, 16, 32, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_008", 4, 4, 4, 32, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_009", 8, 8, 8, 64, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_011", 0, 0, 1, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_012", 1, 8, 1, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_013", 8, 1, 8, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_014", 2, 2, 2, 1, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_015", 3, 3, 3, 1, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_016", 1, 1, 1, 4, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_017", 8, 8, 8, 2, "VALUE_DIAG_1", False, False, S),
+    ("TC_L1_018", 8, 8, 8, 2, "VALUE_NORM_0", False, False, S),
+    ("TC_L1_019", 8, 8, 8, 2, "RANDOM_DIAG", False, False, S),
+    ("TC_L1_020", 8, 8, 8, 2, "RANDOM_UPPER", False, False, S),
+    ("TC_L1_021", 8, 8, 8, 2, "RANDOM_LOWER", False, False, S),
+    ("TC_L1_022", 8, 8, 8, 2, "RANDOM_NORM_1E6", False, False, S),
+    ("TC_L1_023", 8, 8, 8, 2, "RANDOM_NORM_1EN6", False, False, S),
+    ("TC_L1_024", 8, 8, 8, 2, "RANDOM_ILLCOND", False, False, S),
+    ("TC_L1_025", 8, 8, 8, 2, "RANDOM_NORM_2", True, False, IV),
+    ("TC_L1_026", 8, 8, 8, 2, "RANDOM_NORM_2", False, True, IV),
+    ("TC_L1_027", 0, 8, 0, 2, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L1_028", -2, 8, 1, 2, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L1_029", 8, -2, 8, 2, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L1_030", 8, 8, 8, -2, "RANDOM_NORM_2", False, False, IV),
+    ("TC_L1_031", 66, 66, 66, 2, "RANDOM_NORM_2", False, False, S),
+    ("TC_L1_032", 512, 512, 512, 2, "RANDOM_NORM_2", False, False, S),
+]
+
+
+def geqrf_matrices(m, n, lda, fill, seed, batch):
+    """Inputs of the geqrf rows, shape (batch, n, lda) column-major, padding rows set to 99.
+    The fills follow the CSV's names (N(0,1) scaled as named, identity, zeros, random diagonal /
+    triangular, and a graded ill-conditioned matrix); the values are this suite's own draw."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    a = np.full((batch, max(1, n), lda), 99.0, np.float32)
+    if m == 0 or n == 0 or batch == 0:
+        return a
+    g = rng.standard_normal((batch, m, n))  # [batch, row, column]
+    if fill == "VALUE_DIAG_1":
+        g = np.broadcast_to(np.eye(m, n), g.shape).copy()
+    elif fill == "VALUE_NORM_0":
+        g = np.zeros_like(g)
+    elif fill == "RANDOM_DIAG":
+        g = g * np.eye(m, n)
+    elif fill == "RANDOM_UPPER":
+        g = np.triu(g)
+    elif fill == "RANDOM_LOWER":
+        g = np.tril(g)
+    elif fill == "RANDOM_NORM_1E6":
+        g = g * 1e6
+    elif fill == "RANDOM_NORM_1EN6":
+        g = g * 1e-6
+    elif fill == "RANDOM_ILLCOND":
+        g = g * np.logspace(0, -6, n)[None, None, :]
+    a[:, :n, :m] = np.swapaxes(g, 1, 2).astype(np.float32)
+    return a

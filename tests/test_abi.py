@@ -15,7 +15,7 @@ import re
 
 import pytest
 
-from cases import GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS, MATINV_ARG_ROWS, SGEMM_ERRORS
+from cases import GEQRF_ROWS, GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS, MATINV_ARG_ROWS, SGEMM_ERRORS
 from conftest import ROOT
 
 DUMMY = C.create_string_buffer(256)
@@ -180,6 +180,41 @@ def test_sgemm_batched_noops(ob):
     # k == 0 with beta == 1 leaves C untouched without a launch
     assert L.aclblasSgemmBatched(H, ob.OP_N, ob.OP_N, 8, 8, 0, C.byref(one), P, 8, P, 1, C.byref(one), P, 8,
                                  4) == ob.SUCCESS
+
+
+def _geqrf_expected_info(m, n, lda, batch, null_a, null_tau):
+    """LAPACK-style -position of ValidateGeqrfBatchedParams (sgeqrf_batched_host.cpp:21-58)."""
+    if m < 0:
+        return -1
+    if n < 0:
+        return -2
+    if lda < max(1, m):
+        return -4
+    if batch < 0:
+        return -6
+    if batch > 0 and null_a:
+        return -3
+    if batch > 0 and m > 0 and n > 0 and null_tau:
+        return -5
+    return 0
+
+
+@pytest.mark.parametrize("row", [r for r in GEQRF_ROWS if r[8] != "SUCCESS" or min(r[1], r[2], r[4]) == 0],
+                         ids=lambda r: r[0])
+def test_geqrf_argument_rows(ob, row):
+    name, m, n, lda, batch, fill, null_a, null_tau, status = row
+    info = C.c_int(12345)
+    st = ob.lib().aclblasSgeqrfBatched(H, m, n, None if null_a else P, lda, None if null_tau else P, C.byref(info),
+                                       batch)
+    assert ob.STATUS[st] == status
+    assert info.value == _geqrf_expected_info(m, n, lda, batch, null_a, null_tau)
+
+
+def test_geqrf_null_handle_and_info(ob):
+    L, info = ob.lib(), C.c_int(7)
+    assert L.aclblasSgeqrfBatched(None, 8, 8, P, 8, P, C.byref(info), 2) == ob.HANDLE_IS_NULLPTR
+    assert info.value == 7
+    assert L.aclblasSgeqrfBatched(H, 8, 8, P, 8, P, None, 2) == ob.INVALID_VALUE
 
 
 def test_logger_callback_receives_validation_errors(ob):
