@@ -461,6 +461,31 @@ def section_geqrf(ob, h, dev, peak, reps=5, batch=131072):
                          "frac": alg / (t * 1e-3) / 1e9 / peak}}
 
 
+def section_gels(ob, h, dev, peak, reps=5, batch=65536):
+    """aclblasSgelsBatched, least squares 32 x 16 with 2 right-hand sides (overdetermined, the
+    QR path), inputs in HBM: A read and written, C read and written."""
+    import torch
+
+    m, n, nrhs = 32, 16, 2
+    g = torch.Generator(device=dev).manual_seed(13)
+    A0 = torch.randn(batch, n, m, device=dev, generator=g)
+    C0 = torch.randn(batch, nrhs, m, device=dev, generator=g)
+    A, Cm = torch.empty_like(A0), torch.empty_like(C0)
+    pa, pc = ob.ptr_array(A), ob.ptr_array(Cm)
+    info = torch.empty(batch, dtype=torch.int32, device=dev)
+
+    def prep():
+        A.copy_(A0)
+        Cm.copy_(C0)
+
+    t = _events_ms(lambda: h.gels("N", A, m, n, nrhs, m, Cm, m, info=info, aptr=pa, cptr=pc), reps, prep=prep)
+    alg = (8 * m * n + 8 * m * nrhs + 4 + 16) * batch
+    return {"workload": f"gels_32x16_nrhs2_b{batch}", "matrices_s": batch / (t * 1e-3), "ms": t,
+            "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved_GB_s": alg / (t * 1e-3) / 1e9,
+                         "frac": alg / (t * 1e-3) / 1e9 / peak},
+            "note": "one CTA per matrix with serial sums (correctness path)"}
+
+
 def run_section(args):
     """One measured section on its own (used for profiling captures with --small)."""
     import torch
@@ -473,6 +498,8 @@ def run_section(args):
         out = section_grouped(ob, h, dev, peak, reps=2, instances=5000 if args.small else 50000)
     elif args.section == "mixed":
         out = section_mixed(ob, h, dev, reps=2, sizes=((256, 148), (512, 32)) if args.small else ((256, 2048), (512, 256)))
+    elif args.section == "gels":
+        out = section_gels(ob, h, dev, peak, reps=2, batch=16384 if args.small else 65536)
     elif args.section == "geqrf":
         out = section_geqrf(ob, h, dev, peak, reps=2, batch=65536 if args.small else 131072)
     elif args.section == "matinv":
@@ -492,7 +519,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sections", action="store_true", help="skip the grouped / mixed / adjoint measurements")
-    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv", "geqrf"],
+    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv", "geqrf", "gels"],
                     help="run only this measured section (one JSON line) and exit")
     ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
     args = ap.parse_args()
@@ -674,7 +701,7 @@ def main():
         if world == 1 and not args.no_sections:
             line["sections"] = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
                                 "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak),
-                                "geqrf": section_geqrf(ob, h, dev, peak)}
+                                "geqrf": section_geqrf(ob, h, dev, peak), "gels": section_gels(ob, h, dev, peak)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline()

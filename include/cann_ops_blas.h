@@ -108,6 +108,25 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetriBatched(
     aclblasHandle_t handle, int n, const float* const Aarray[], int lda, const int* PivotArray,
     float* const Carray[], int ldc, int* infoArray, int batchSize);
 
+/* Extension (no counterpart): ptrArray[i] = (char*)base + i * strideBytes for i < count, written
+ * on the handle's stream by a kernel (ptrArray is device memory with count entries). */
+ACLBLAS_EXPORT aclblasStatus_t aclblasBuildPointerArray(
+    aclblasHandle_t handle, const void* base, long long strideBytes, int count, void** ptrArray);
+
+/* Extensions (no counterpart): strided-batch forms of aclblasSgetrfBatched / SgetrsBatched /
+ * SgetriBatched -- matrix i at base + i * stride (elements). The pointer arrays are built in the
+ * handle's workspace (8 bytes per matrix and operand, 256-byte aligned; EXECUTION_FAILED when it
+ * is too small) and the batched entry points run on them: same validation, same results. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfStridedBatched(
+    aclblasHandle_t handle, int n, float* A, int lda, long long strideA, int* PivotArray, int* infoArray,
+    int batchSize);
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrsStridedBatched(
+    aclblasHandle_t handle, aclblasOperation_t trans, int n, int nrhs, const float* A, int lda, long long strideA,
+    const int* devIpiv, float* B, int ldb, long long strideB, int* info, int batchCount);
+ACLBLAS_EXPORT aclblasStatus_t aclblasSgetriStridedBatched(
+    aclblasHandle_t handle, int n, const float* A, int lda, long long strideA, const int* PivotArray, float* C,
+    int ldc, long long strideC, int* infoArray, int batchSize);
+
 /* Replaces aclblasSgeqrfBatched (include/cann_ops_blas.h:399;
  * blas/geqrf_batched/arch35/sgeqrf_batched_host.cpp:19-141). Householder QR of every
  * m x n matrix in place (R above, the reflectors below the diagonal), TauArray[i] receives

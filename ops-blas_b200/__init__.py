@@ -52,6 +52,12 @@ SIGNATURES = {
     "aclblasSgetriBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _vp, C.c_int]),
     "aclblasSmatinvBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
     "aclblasSgeqrfBatched": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int]),
+    "aclblasBuildPointerArray": (C.c_int, [_vp, _vp, C.c_longlong, C.c_int, _vp]),
+    "aclblasSgetrfStridedBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_longlong, _vp, _vp, C.c_int]),
+    "aclblasSgetrsStridedBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_longlong, _vp, _vp,
+                                              C.c_int, C.c_longlong, _vp, C.c_int]),
+    "aclblasSgetriStridedBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_longlong, _vp, _vp, C.c_int,
+                                              C.c_longlong, _vp, C.c_int]),
     "aclblasSgelsBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp,
                                       C.c_int]),
     "aclblasSgemmBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp,

@@ -568,3 +568,107 @@ def geqrf_matrices(m, n, lda, fill, seed, batch):
         g = g * np.logspace(0, -6, n)[None, None, :]
     a[:, :n, :m] = np.swapaxes(g, 1, 2).astype(np.float32)
     return a
+
+# aclblasSgelsBatched rows of test/gels_batched/sgels_batched/arch35/sgels_batched_test.csv:
+# name trans m n nrhs lda ldc batch c_fill null(A/C/I/H/-) status description (trans X = invalid)
+_GELS = """
+TC_L0_01 N 8 4 1 8 8 1 RANDOM - S overdetermined_small_transN
+TC_L0_02 N 4 8 1 4 8 1 RANDOM - S underdetermined_small_transN
+TC_L0_03 N 8 8 1 8 8 1 RANDOM - S square_transN
+TC_L0_04 T 8 4 1 8 8 1 RANDOM - S overdetermined_small_transT
+TC_L0_05 T 4 8 1 4 8 1 RANDOM - S underdetermined_small_transT
+TC_L0_06 N 32 16 1 32 32 1 RANDOM - S overdetermined_medium_transN
+TC_L0_07 N 16 8 4 16 16 1 RANDOM - S multi_rhs_overdetermined
+TC_L0_08 N 8 4 1 8 8 4 RANDOM - S multi_batch_overdetermined
+TC_L0_09 N 16 8 3 16 16 4 RANDOM - S multi_batch_multi_rhs
+TC_L0_10 N 1 1 1 1 1 1 RANDOM - S minimal_1x1
+TC_L0_11 N 1 8 1 1 8 1 RANDOM - S single_row_underdetermined
+TC_L0_12 N 8 1 1 8 8 1 RANDOM - S single_column_overdetermined
+TC_L0_13 N 0 8 1 1 8 1 RANDOM - S m_zero_fast_return
+TC_L0_14 N 8 0 1 8 8 1 RANDOM - S n_zero_fast_return
+TC_L0_15 N 8 4 0 8 8 1 RANDOM - S nrhs_zero_fast_return
+TC_L0_16 N 8 4 1 8 8 0 RANDOM - S batch_zero_fast_return
+TC_L0_17 T 8 8 1 8 8 1 RANDOM - S square_transT
+TC_L0_18 N 16 32 1 16 32 1 RANDOM - S underdetermined_medium
+TC_L0_19 N 8 16 2 8 16 3 RANDOM - S multi_batch_underdetermined
+TC_L0_20 N 8 8 1 8 8 1 RANDOM - S identity_matrix
+TC_L1_01 N 128 64 1 128 128 1 RANDOM - S large_overdetermined
+TC_L1_02 N 64 128 1 64 128 1 RANDOM - S large_underdetermined
+TC_L1_03 N 128 128 1 128 128 1 RANDOM - S large_square
+TC_L1_04 N 256 4 1 256 256 1 RANDOM - S extreme_aspect_m_gt_n
+TC_L1_05 N 4 256 1 4 256 1 RANDOM - S extreme_aspect_n_gt_m
+TC_L1_06 N 8 4 1 16 8 1 RANDOM - S noncompact_lda
+TC_L1_07 N 8 4 1 8 16 1 RANDOM - S noncompact_ldc
+TC_L1_08 N 8 4 1 16 16 1 RANDOM - S noncompact_lda_ldc
+TC_L1_09 N 31 17 1 31 31 1 RANDOM - S prime_dimensions
+TC_L1_10 N 127 97 1 127 127 1 RANDOM - S prime_dimensions_large
+TC_L1_11 N 8 4 1 8 8 1 RANDOM - S rank_deficient
+TC_L1_12 N 8 4 1 8 8 1 ZEROS - S rhs_zeros
+TC_L1_13 N 16 8 1 16 16 1 RANDOM - S known_solution
+TC_L1_14 N 8 4 1 8 8 16 RANDOM - S large_batch
+TC_L1_15 N 4 8 1 4 8 16 RANDOM - S large_batch_underdetermined
+TC_L1_16 T 128 64 1 128 128 1 RANDOM - S transT_large_overdetermined
+TC_L1_17 T 64 128 1 64 128 1 RANDOM - S transT_large_underdetermined
+TC_L1_18 T 32 16 4 32 32 1 RANDOM - S transT_multi_rhs
+TC_L1_19 T 16 8 1 16 16 4 RANDOM - S transT_multi_batch
+TC_L1_20 T 16 8 3 16 16 4 RANDOM - S transT_multi_rhs_batch
+TC_L1_21 N 16 8 2 32 32 4 RANDOM - S noncompact_multi_batch_rhs
+TC_L1_22 N 256 2 1 256 256 1 RANDOM - S extreme_aspect_m_gt_n_large
+TC_L1_23 N 2 256 1 2 256 1 RANDOM - S extreme_aspect_n_gt_m_large
+TC_L1_24 N 2 2 1 2 2 1 RANDOM - S small_2x2_square
+TC_L1_25 N 64 32 1 64 64 1 RANDOM - S medium_single_batch
+TC_L1_26 N 8 4 1 8 8 1 RANDOM H HN handle_nullptr
+TC_L1_27 N -1 4 1 1 4 1 RANDOM - IV m_negative
+TC_L1_28 N 8 -1 1 8 8 1 RANDOM - IV n_negative
+TC_L1_29 N 8 4 -1 8 8 1 RANDOM - IV nrhs_negative
+TC_L1_30 N 8 4 1 8 8 -1 RANDOM - IV batch_negative
+TC_L1_31 N 8 4 1 4 8 1 RANDOM - IV lda_lt_max1m
+TC_L1_32 N 0 4 1 0 4 1 RANDOM - IV lda_lt_1_m0
+TC_L1_33 N 8 16 1 8 8 1 RANDOM - IV ldc_lt_max1mn
+TC_L1_34 X 8 4 1 8 8 1 RANDOM - IE trans_invalid
+TC_L1_35 N 8 4 1 8 8 1 RANDOM A IV aarray_nullptr
+TC_L1_36 N 8 4 1 8 8 1 RANDOM C IV carray_nullptr
+TC_L1_37 N 8 4 1 8 8 1 RANDOM I IV devinfo_nullptr
+"""
+
+
+def _gels_rows():
+    st = {"S": S, "IV": IV, "HN": HN, "IE": IE}
+    out = []
+    for line in _GELS.split("\n"):
+        if not line.strip():
+            continue
+        name, t, m, n, nrhs, lda, ldc, batch, cfill, null, status, desc = line.split()
+        out.append((name, t, int(m), int(n), int(nrhs), int(lda), int(ldc), int(batch), cfill, null, st[status], desc))
+    return out
+
+
+GELS_ROWS = _gels_rows()
+
+
+def gels_inputs(row, seed):
+    """A (batch, n, lda) and C (batch, nrhs, ldc) of a gels row, column-major, padding 99 / 77.
+    A is N(0,1) except the identity and rank-deficient (a repeated column) rows; C holds the
+    right-hand sides in its first m (trans N) or n (trans T) rows: N(0,1), zeros, or A x for a
+    known x."""
+    import numpy as np
+
+    name, t, m, n, nrhs, lda, ldc, batch, cfill, null, status, desc = row
+    rng = np.random.default_rng(seed)
+    rows_b = m if t == "N" else n
+    a = np.full((batch, max(1, n), lda), 99.0, np.float32)
+    c = np.full((batch, max(1, nrhs), ldc), 77.0, np.float32)
+    g = rng.standard_normal((batch, m, n))
+    if desc == "identity_matrix":
+        g = np.broadcast_to(np.eye(m, n), g.shape).copy()
+    if desc == "rank_deficient" and n > 1:
+        g[:, :, n - 1] = g[:, :, 0]
+    a[:, :n, :m] = np.swapaxes(g, 1, 2)
+    rhs = rng.standard_normal((batch, rows_b, nrhs))
+    if cfill == "ZEROS":
+        rhs[:] = 0.0
+    if desc == "known_solution":
+        op = g if t == "N" else np.swapaxes(g, 1, 2)
+        rhs = op @ rng.standard_normal((batch, op.shape[2], nrhs))
+    c[:, :nrhs, :rows_b] = np.swapaxes(rhs, 1, 2)
+    return a, c

@@ -15,7 +15,7 @@ import re
 
 import pytest
 
-from cases import GEQRF_ROWS, GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS, MATINV_ARG_ROWS, SGEMM_ERRORS
+from cases import GELS_ROWS, GEQRF_ROWS, GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS, MATINV_ARG_ROWS, SGEMM_ERRORS
 from conftest import ROOT
 
 DUMMY = C.create_string_buffer(256)
@@ -215,6 +215,33 @@ def test_geqrf_null_handle_and_info(ob):
     assert L.aclblasSgeqrfBatched(None, 8, 8, P, 8, P, C.byref(info), 2) == ob.HANDLE_IS_NULLPTR
     assert info.value == 7
     assert L.aclblasSgeqrfBatched(H, 8, 8, P, 8, P, None, 2) == ob.INVALID_VALUE
+
+
+@pytest.mark.parametrize("row", [r for r in GELS_ROWS if r[10] != "SUCCESS" or min(r[2], r[3], r[4], r[7]) == 0],
+                         ids=lambda r: r[0])
+def test_gels_argument_rows(ob, row):
+    name, t, m, n, nrhs, lda, ldc, batch, cfill, null, status, desc = row
+    op = 999 if t == "X" else ob.TRANS[t]
+    st = ob.lib().aclblasSgelsBatched(None if null == "H" else H, op, m, n, nrhs, None if null == "A" else P, lda,
+                                      None if null == "C" else P, ldc, None if null == "I" else P, batch)
+    assert ob.STATUS[st] == status
+
+
+def test_strided_and_builder_validation(ob):
+    L, info = ob.lib(), C.c_int(0)
+    assert L.aclblasBuildPointerArray(None, P, 16, 4, P) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasBuildPointerArray(H, P, 16, -1, P) == ob.INVALID_VALUE
+    assert L.aclblasBuildPointerArray(H, None, 16, 4, P) == ob.INVALID_VALUE
+    assert L.aclblasBuildPointerArray(H, None, 16, 0, None) == ob.SUCCESS
+    # the batched calls' validation and no-op paths, reached before any pointer array is built
+    assert L.aclblasSgetrfStridedBatched(None, 8, P, 8, 64, P, P, 2) == ob.HANDLE_IS_NULLPTR
+    assert L.aclblasSgetrfStridedBatched(H, -1, P, 8, 64, P, P, 2) == ob.INVALID_VALUE
+    assert L.aclblasSgetrfStridedBatched(H, 0, P, 1, 0, P, P, 2) == ob.SUCCESS
+    assert L.aclblasSgetrfStridedBatched(H, 8, None, 8, 64, P, P, 2) == ob.INVALID_VALUE
+    assert L.aclblasSgetrsStridedBatched(H, 999, 8, 1, P, 8, 64, P, P, 8, 8, C.byref(info), 2) == ob.INVALID_ENUM
+    assert L.aclblasSgetrsStridedBatched(H, ob.OP_N, 8, 0, P, 8, 64, P, P, 8, 8, C.byref(info), 2) == ob.SUCCESS
+    assert L.aclblasSgetriStridedBatched(H, 8, P, 8, 64, P, None, 8, 64, P, 2) == ob.INVALID_VALUE
+    assert L.aclblasSgetriStridedBatched(H, 8, P, 8, 64, P, P, 8, 64, P, 0) == ob.SUCCESS
 
 
 def test_logger_callback_receives_validation_errors(ob):
