@@ -19,6 +19,10 @@ not in L2 (126 MB) when the step starts; no L2 flush is needed.
 --impl reference times that CPU golden path alone on the same workload (rank 0 only).
 Multi-GPU (torchrun): replicas only -- every rank runs its own batch, no collective on the
 data path; value = all ranks' matrices / max-over-ranks time.
+
+sections (single GPU, skipped with --no-sections): grouped uneven batch vs per-n launches,
+mixed precision + refinement vs plain FP32, adjoint, fused matinv, geqrf and gels; --section NAME
+[--small] runs one of them alone.
 """
 from __future__ import annotations
 
@@ -34,7 +38,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "getrf+getrs batched matrices/s: mixed/grouped vs plain FP32 at equal FP64 err"
 N, BATCH, NRHS = 32, 131072, 4
-E2E_CHUNKS = 16  # e2e leg: chunks of the batch pipelined over three streams
+E2E_CHUNKS = 16  # e2e leg: chunks of the batch, pipelined over E2E_STREAMS streams
+E2E_STREAMS = 3
 FALLBACK_HBM_GBS = 6650.0
 
 # Algorithmic bytes per matrix (reads + writes of each kernel):
@@ -518,7 +523,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-sections", action="store_true", help="skip the grouped / mixed / adjoint measurements")
+    ap.add_argument("--no-sections", action="store_true", help="skip the section measurements (grouped, mixed, adjoint, matinv, geqrf, gels)")
     ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv", "geqrf", "gels"],
                     help="run only this measured section (one JSON line) and exit")
     ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
@@ -615,7 +620,7 @@ def main():
     # The batch goes through in E2E_CHUNKS chunks round-robin over three streams (one handle
     # each), so the host-to-device copy of one chunk, the chain of the previous one and the
     # device-to-host copy of the one before run at the same time (PCIe is full duplex).
-    e2e_streams = [torch.cuda.Stream(dev) for _ in range(3)]
+    e2e_streams = [torch.cuda.Stream(dev) for _ in range(E2E_STREAMS)]
     e2e_handles = [ob.Handle(stream=s_) for s_ in e2e_streams]
     per_chunk = (BATCH + E2E_CHUNKS - 1) // E2E_CHUNKS
 
@@ -628,7 +633,7 @@ def main():
             i0, i1 = c * per_chunk, min(BATCH, (c + 1) * per_chunk)
             if i0 >= i1:
                 break
-            s_, hh = e2e_streams[c % 3], e2e_handles[c % 3]
+            s_, hh = e2e_streams[c % E2E_STREAMS], e2e_handles[c % E2E_STREAMS]
             with torch.cuda.stream(s_):
                 a_, b_, ap, bp = dA[i0:i1], dB[i0:i1], aptr[0][i0:i1], bptr[0][i0:i1]
                 a_.copy_(hostA[i0:i1], non_blocking=True)
@@ -694,7 +699,7 @@ def main():
                          "traffic": traffic, "alg_bytes_per_launch": ALG_BYTES[dom] * BATCH},
             "e2e": {"value": BATCH * world / (e2e_ms * 1e-3), "unit": "matrices/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                    "pipeline": f"{E2E_CHUNKS} chunks over 3 streams"},
+                    "pipeline": f"{E2E_CHUNKS} chunks over {E2E_STREAMS} streams"},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks.summary(),
         }
