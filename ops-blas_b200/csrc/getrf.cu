@@ -209,7 +209,7 @@ extern "C" aclblasStatus_t aclblasSgetrfBatched(
         return launch_status(kApi, getrf_reg_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize, rows,
                                                     warps));
     } else if (getrf_large_supported(n)) {
-        return launch_status(kApi, getrf_large_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize, 0));
+        return launch_status(kApi, getrf_large_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize));
     } else {
         if (pivot)
             getrf_generic_kernel<true><<<(unsigned)batchSize, kGenericThreads, 0, st>>>(Aarray, n, lda, PivotArray,

@@ -1,5 +1,5 @@
-// aclblasSgetrfBatched for 128 < n <= 1024 and the mixed-precision factorisation: one CTA per
-// matrix, blocked right-looking LU with the matrix in global memory (L2 resident per CTA).
+// aclblasSgetrfBatched for 128 < n <= 640: one CTA per matrix, blocked right-looking LU with the
+// matrix in global memory (L2 resident per CTA).
 //
 // Per panel of PB columns:
 //   1. the panel (rows k0..n-1) is staged in shared memory and factored by the whole CTA:
@@ -9,14 +9,11 @@
 //      (whole-row swaps, as the reference's SwapRows, sgetrf_batched_kernel.cpp:81-91);
 //   3. U12 (panel rows, right of the panel) by forward substitution with the unit L11;
 //   4. A22 -= L21 * U12 with 4x4 register tiles.
-// In the plain mode every element receives its updates one fmaf at a time in increasing
-// column order -- the reference's operation sequence, so results match it bit for bit. In the
-// mixed modes the L21 / U12 operands of step 4 (the dense trailing update, ~90% of the flops)
-// are split into a high and a low part of reduced precision (TF32 or BF16, x = hi + lo) and
-// the update accumulates hi*hi + hi*lo + lo*hi in FP32 -- the error-compensated three-product
-// scheme, which keeps the factorisation close to FP32 accuracy so that iterative refinement
-// converges for condition numbers up to ~1e6; the panel and U12 stay FP32.
-#include <cuda_bf16.h>
+// Every element receives its updates one fmaf at a time in increasing column order -- the
+// reference's operation sequence, so results match it bit for bit. (A variant that split the
+// step-4 operands into TF32 / BF16 high and low parts on the CUDA cores was measured slower than
+// this plain kernel at n = 512 and removed; the mixed modes use the tensor-memory kernel up to
+// n = 256 and these plain factors above.)
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -27,45 +24,32 @@ namespace opsblas {
 constexpr int kLgThreads = 256;
 constexpr int kLgWarps = kLgThreads / 32;
 constexpr int kLgPB = 16;
-constexpr int kLgMaxN = 640;  // mixed-mode staging keeps shared memory under 227 KiB
+constexpr int kLgMaxN = 640;
 constexpr int kLgPS = kLgPB + 1;  // panel row stride in shared memory (odd: conflict-free)
-
-__device__ __forceinline__ float lg_round(float x, int mode)
-{
-    if (mode == 1) {  // TF32: keep 10 mantissa bits, round to nearest even
-        unsigned u = __float_as_uint(x);
-        if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x0fffu + ((u >> 13) & 1u)) & 0xffffe000u;
-        return __uint_as_float(u);
-    }
-    if (mode == 2) return __bfloat162float(__float2bfloat16_rn(x));
-    return x;
-}
 
 struct LgLayout {
     int lsd;
     size_t bytes;
-    __host__ __device__ LgLayout(int n, int mode = 0)
+    __host__ __device__ explicit LgLayout(int n)
     {
         lsd = (n + 3) & ~3;
-        bytes = (size_t)n * kLgPS * 4                        // panel
-                + (size_t)(mode ? 4 : 2) * kLgPB * lsd * 4     // staged L21 (transposed) and U12 (+ low parts)
+        bytes = (size_t)n * kLgPS * 4             // panel
+                + (size_t)2 * kLgPB * lsd * 4     // staged L21 (transposed) and U12
                 + (size_t)kLgPB * 2 * 4           // recorded interchanges
                 + (size_t)kLgWarps * 2 * 4 + 64;  // per-warp argmax, scalars
     }
 };
 
-template <bool PIVOT, int MODE>
+template <bool PIVOT>
 __global__ void __launch_bounds__(kLgThreads)
 getrf_large_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __restrict__ piv, int* __restrict__ info)
 {
     extern __shared__ __align__(16) float smem[];
-    const LgLayout L(n, MODE);
+    const LgLayout L(n);
     const int lsd = L.lsd;
     float* l21 = smem;                           // [PB][lsd] (negated)
     float* u12 = l21 + kLgPB * lsd;              // [PB][lsd]
-    float* l21lo = MODE ? u12 + kLgPB * lsd : nullptr;     // low parts (mixed modes)
-    float* u12lo = MODE ? l21lo + kLgPB * lsd : nullptr;
-    float* pb_s = u12 + (MODE ? 3 : 1) * kLgPB * lsd;  // [n][PS]: panel row i-k0 at pb_s[(i-k0)*PS]
+    float* pb_s = u12 + kLgPB * lsd;             // [n][PS]: panel row i-k0 at pb_s[(i-k0)*PS]
     int* swaps = reinterpret_cast<int*>(pb_s + (size_t)n * kLgPS);  // [PB] pivot rows (logical)
     float* wv = reinterpret_cast<float*>(swaps + 2 * kLgPB);          // per-warp best value
     int* wr = reinterpret_cast<int*>(wv + kLgWarps);                  // per-warp best row
@@ -197,18 +181,13 @@ getrf_large_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __res
                 for (int r = 0; r < kLgPB; r++) {
                     if (r < w) {
                         at(k0 + r, j) = u[r];
-                        const float hi = lg_round(u[r], MODE);
-                        u12[r * lsd + jj] = hi;
-                        if (MODE) u12lo[r * lsd + jj] = lg_round(u[r] - hi, MODE);
+                        u12[r * lsd + jj] = u[r];
                     }
                 }
             }
             for (int e = tid; e < rows * w; e += kLgThreads) {
                 const int ii = e % rows, mm = e / rows;
-                const float v = pb_s[(r0 - k0 + ii) * kLgPS + mm];
-                const float hi = lg_round(v, MODE);
-                l21[mm * lsd + ii] = -hi;
-                if (MODE) l21lo[mm * lsd + ii] = -lg_round(v - hi, MODE);
+                l21[mm * lsd + ii] = -pb_s[(r0 - k0 + ii) * kLgPS + mm];
             }
             __syncthreads();
             // ------------------------------------------- 4. A22 -= L21 * U12 --
@@ -238,27 +217,10 @@ getrf_large_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __res
                     const float4 uv = *reinterpret_cast<const float4*>(u12 + mm * lsd + bj);
                     const float la[4] = {lv.x, lv.y, lv.z, lv.w};
                     const float ub[4] = {uv.x, uv.y, uv.z, uv.w};
-                    if (MODE) {
-                        // small terms first: hi*lo + lo*hi, then hi*hi
-                        const float4 lw = *reinterpret_cast<const float4*>(l21lo + mm * lsd + bi);
-                        const float4 uw = *reinterpret_cast<const float4*>(u12lo + mm * lsd + bj);
-                        const float ll[4] = {lw.x, lw.y, lw.z, lw.w};
-                        const float ul[4] = {uw.x, uw.y, uw.z, uw.w};
-                        float t[4][4];
 #pragma unroll
-                        for (int a = 0; a < 4; a++)
+                    for (int a = 0; a < 4; a++)
 #pragma unroll
-                            for (int b = 0; b < 4; b++) t[a][b] = fmaf(la[a], ul[b], ll[a] * ub[b]);
-#pragma unroll
-                        for (int a = 0; a < 4; a++)
-#pragma unroll
-                            for (int b = 0; b < 4; b++) acc[a][b] = fmaf(la[a], ub[b], acc[a][b] + t[a][b]);
-                    } else {
-#pragma unroll
-                        for (int a = 0; a < 4; a++)
-#pragma unroll
-                            for (int b = 0; b < 4; b++) acc[a][b] = fmaf(la[a], ub[b], acc[a][b]);
-                    }
+                        for (int b = 0; b < 4; b++) acc[a][b] = fmaf(la[a], ub[b], acc[a][b]);
                 }
 #pragma unroll
                 for (int b = 0; b < 4; b++) {
@@ -282,29 +244,21 @@ getrf_large_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __res
 
 bool getrf_large_supported(int n) { return n > 32 && n <= kLgMaxN; }
 
-cudaError_t getrf_large_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch,
-                               int mode)
+cudaError_t getrf_large_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch)
 {
-    const LgLayout L(n, piv ? mode : 0);
+    const LgLayout L(n);
     static bool configured = false;
     if (!configured) {
-        const int big = (int)LgLayout(kLgMaxN, 1).bytes;
-        cudaFuncSetAttribute(getrf_large_kernel<true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(getrf_large_kernel<false, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(getrf_large_kernel<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(getrf_large_kernel<true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        const int big = (int)LgLayout(kLgMaxN).bytes;
+        cudaFuncSetAttribute(getrf_large_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        cudaFuncSetAttribute(getrf_large_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         configured = true;
     }
     const unsigned grid = (unsigned)batch;
-    if (piv == nullptr) {
-        getrf_large_kernel<false, 0><<<grid, kLgThreads, L.bytes, st>>>(Aarray, n, lda, nullptr, info);
-    } else if (mode == 1) {
-        getrf_large_kernel<true, 1><<<grid, kLgThreads, L.bytes, st>>>(Aarray, n, lda, piv, info);
-    } else if (mode == 2) {
-        getrf_large_kernel<true, 2><<<grid, kLgThreads, L.bytes, st>>>(Aarray, n, lda, piv, info);
-    } else {
-        getrf_large_kernel<true, 0><<<grid, kLgThreads, L.bytes, st>>>(Aarray, n, lda, piv, info);
-    }
+    if (piv == nullptr)
+        getrf_large_kernel<false><<<grid, kLgThreads, L.bytes, st>>>(Aarray, n, lda, nullptr, info);
+    else
+        getrf_large_kernel<true><<<grid, kLgThreads, L.bytes, st>>>(Aarray, n, lda, piv, info);
     return cudaGetLastError();
 }
 

@@ -72,11 +72,9 @@ bool getrf_tmem_supported(int n);
 cudaError_t getrf_tmem_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
                               int ldlu, int* piv, int* info, int batch, int prec);
 
-// getrf_large.cu: 32 < n <= 640, matrix in global memory; mode 0 plain FP32 (reference
-// operation order), 1 = TF32 split trailing update, 2 = BF16 split trailing update.
+// getrf_large.cu: 32 < n <= 640, matrix in global memory, the reference's operation order.
 bool getrf_large_supported(int n);
-cudaError_t getrf_large_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch,
-                               int mode);
+cudaError_t getrf_large_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch);
 
 // getrf_reg.cu: 32 < n <= 128, matrix in registers; shape = rows per lane x warps per matrix.
 bool getrf_reg_supported(int n);

@@ -4,7 +4,9 @@
 //   LU = A (copy; A is kept for the residual), P*LU = A factored by aclblasSgetrfBatched's
 //   kernels -- plain FP32 for ACLBLAS_COMPUTE_32F; for ACLBLAS_COMPUTE_32F_FAST_TF32 / _FAST_16BF
 //   with the split TF32 / BF16 trailing update on the tensor cores, the matrix resident in TMEM
-//   (getrf_tmem.cu, n <= 256; getrf_large.cu on the CUDA cores above);
+//   (getrf_tmem.cu, 32 < n <= 256); other orders factor in plain FP32 (above n = 256 the matrix
+//   does not fit one SM's tensor memory, and a split update on the CUDA cores measured slower
+//   than the plain kernel), after which refinement converges at once;
 //   X = LU \ B (aclblasSgetrsBatched's kernels);
 //   repeat up to maxIter times: r = B - A X in FP64 on the GPU, backward error
 //     berr = max_c ||r_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf) in FP64;
@@ -241,9 +243,7 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
         err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
-    } else if (n > 32 && getrf_large_supported(n) && (mode != 0 || n > 128)) {
-        err = getrf_large_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
-    } else {
+    } else {  // plain FP32 factors: the batched getrf's kernels
         aclblasStatus_t s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;
     }
@@ -412,9 +412,7 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
         err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
-    } else if (n > 32 && getrf_large_supported(n) && (mode != 0 || n > 128)) {
-        err = getrf_large_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
-    } else {
+    } else {  // plain FP32 factors: the batched getrf's kernels
         s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;
     }
