@@ -10,9 +10,9 @@
 // row order with every product rounded before it is added (no contraction), the order of the
 // CPU oracle they match bit for bit. Parity with the reference is its own test rule:
 // MIXED_TOLERANCE against LAPACK sgeqrf_.
-//   m, n <= 32 : geqrf_warp_kernel<N>, one warp per matrix, lane = row, the row in registers;
-//                the column sums go through a per-warp shared-memory transpose (lane c sums
-//                column c), the divisions run one per lane;
+//   m, n <= 32 : geqrf_col_kernel<M>, one warp per matrix, lane c = column c in registers (every
+//                sum local, in row order), the reflector published through shared memory with
+//                its divisions one row per lane, the column update in packed f32x2 operations;
 //   otherwise  : geqrf_generic_kernel, one CTA per matrix in global memory (correctness path):
 //                thread 0 forms the reflector, thread t updates columns i+1+t, i+1+t+256, ...
 #include <cuda_runtime.h>
@@ -25,26 +25,19 @@
 namespace opsblas {
 
 constexpr int kQrWarps = 8;
-constexpr int kQrStride = 33;  // row stride of the per-warp transpose buffer (conflict-free columns)
 
-// Reflector i of the warp's matrix (lane = row, the row in a[]); I is a template parameter so that
-// every register index is a compile-time constant.
-template <int N, int I>
-__device__ __forceinline__ void qr_warp_step(float (&a)[N], float& mytau, float* xw, float* cw, int lane, int m,
-                                             bool rv)
+// Reflector I of the warp's matrix. Lane c holds column c (rows in registers, M = m rows); every
+// sum runs locally in row order, so the arithmetic is the row-order restatement's. The reflector's
+// divisions are shared out one row per lane through the warp's shared-memory column buffer.
+template <int M, int I>
+__device__ __forceinline__ void qr_col_step(float (&col)[M], float& mytau, float* vb, int lane, int n)
 {
-    // sigma = sum_{r>i} A(r,i)^2 in row order (lane i)
-    cw[lane] = a[I];
-    __syncwarp();
+    // sigma = sum_{r>I} A(r,I)^2 (every lane forms it for its own column; lane I's is used)
     float sigma = 0.0f;
-    if (lane == I) {
-        for (int r = I + 1; r < m; r++) {
-            const float x = cw[r];
-            sigma = __fadd_rn(sigma, __fmul_rn(x, x));
-        }
-    }
+#pragma unroll
+    for (int r = I + 1; r < M; r++) sigma = __fadd_rn(sigma, __fmul_rn(col[r], col[r]));
     sigma = __shfl_sync(0xffffffffu, sigma, I);
-    const float x1 = __shfl_sync(0xffffffffu, a[I], I);
+    const float x1 = __shfl_sync(0xffffffffu, col[I], I);
     float t, alpha;
     if (sigma == 0.0f) {
         t = 0.0f;
@@ -55,70 +48,76 @@ __device__ __forceinline__ void qr_warp_step(float (&a)[N], float& mytau, float*
         t = __fdiv_rn(__fsub_rn(alpha, x1), alpha);
     }
     if (lane == I) mytau = t;
-    __syncwarp();  // column i read before the buffer is reused
-    if (t == 0.0f) return;  // A(i,i) stays x1 == alpha, no update
+    if (t == 0.0f) return;  // uniform: A(I,I) stays x1 == alpha, no update
     const float vscale = __fsub_rn(x1, alpha);
-    const bool below = rv && lane > I;
-    if (below) a[I] = __fdiv_rn(a[I], vscale);
-    if (lane == I) a[I] = alpha;
-    const float v = a[I];
-    // dot_c = A(i,c) + sum_{r>i} v_r A(r,c): row r's term at xw[r][c], lane c sums its column
+    // v_r = A(r,I) / vscale for r > I: lane I publishes its column, lane r divides row r
+    if (lane == I) {
 #pragma unroll
-    for (int c = I + 1; c < N; c++) xw[lane * kQrStride + c] = below ? __fmul_rn(v, a[c]) : (lane == I ? a[c] : 0.0f);
+        for (int r = I + 1; r < M; r++) vb[r] = col[r];
+    }
     __syncwarp();
-    float coef = 0.0f;
-    if (lane > I && lane < N) {
-        float dot = xw[I * kQrStride + lane];
-        for (int r = I + 1; r < m; r++) dot = __fadd_rn(dot, xw[r * kQrStride + lane]);
-        coef = __fmul_rn(t, dot);
-    }
+    if (lane > I && lane < M) vb[lane] = __fdiv_rn(vb[lane], vscale);
+    __syncwarp();
+    float v[M];
 #pragma unroll
-    for (int c = I + 1; c < N; c++) {
-        const float cc = __shfl_sync(0xffffffffu, coef, c);
-        if (below)
-            a[c] = __fsub_rn(a[c], __fmul_rn(cc, v));
-        else if (lane == I)
-            a[c] = __fsub_rn(a[c], cc);
+    for (int r = I + 1; r < M; r++) v[r] = vb[r];
+    if (lane == I) {
+        col[I] = alpha;
+#pragma unroll
+        for (int r = I + 1; r < M; r++) col[r] = v[r];
+    } else if (lane > I && lane < n) {
+        // dot = A(I,c) + sum_{r>I} v_r A(r,c) in row order, then A(r,c) -= coef v_r, A(I,c) -= coef
+        float dot = col[I];
+#pragma unroll
+        for (int r = I + 1; r < M; r++) dot = __fadd_rn(dot, __fmul_rn(v[r], col[r]));
+        const float coef = __fmul_rn(t, dot);
+        const float2 cc = make_float2(coef, coef);
+        int r = I + 1;
+#pragma unroll
+        for (; r + 1 < M; r += 2) {
+            const float2 p = __fmul2_rn(cc, make_float2(v[r], v[r + 1]));
+            const float2 q = __fadd2_rn(make_float2(col[r], col[r + 1]), make_float2(-p.x, -p.y));
+            col[r] = q.x;
+            col[r + 1] = q.y;
+        }
+        if (r < M) col[r] = __fsub_rn(col[r], __fmul_rn(coef, v[r]));
+        col[I] = __fsub_rn(col[I], coef);
     }
-    __syncwarp();  // sums read before the next step writes the buffer
+    __syncwarp();  // the buffer is read before the next reflector writes it
 }
 
-// Reflectors 0 .. min(m, n) - 1, one instantiation per column index.
-template <int N, int... I>
-__device__ __forceinline__ void qr_warp_all(float (&a)[N], float& mytau, float* xw, float* cw, int lane, int m, bool rv,
-                                            std::integer_sequence<int, I...>)
+// Reflectors 0 .. min(m, n) - 1, one instantiation per row index.
+template <int M, int... I>
+__device__ __forceinline__ void qr_col_all(float (&col)[M], float& mytau, float* vb, int lane, int n,
+                                           std::integer_sequence<int, I...>)
 {
-    ((I < m ? qr_warp_step<N, I>(a, mytau, xw, cw, lane, m, rv) : void()), ...);
+    ((I < n ? qr_col_step<M, I>(col, mytau, vb, lane, n) : void()), ...);
 }
 
-template <int N>
+template <int M>
 __global__ void __launch_bounds__(kQrWarps * 32)
-geqrf_warp_kernel(float* const* __restrict__ Aarray, int m, int lda, float* const* __restrict__ TauArray, int batch)
+geqrf_col_kernel(float* const* __restrict__ Aarray, int n, int lda, float* const* __restrict__ TauArray, int batch)
 {
-    __shared__ float xs[kQrWarps][32 * kQrStride];  // products of the current step, [row][column]
-    __shared__ float cs[kQrWarps][32];              // column i of the current step
+    __shared__ float vbuf[kQrWarps][32];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const long long b = (long long)blockIdx.x * kQrWarps + warp;
     if (b >= batch) return;  // warp-uniform
     float* A = Aarray[b];
     float* tau = TauArray[b];
-    float* xw = xs[warp];
-    float* cw = cs[warp];
-    const bool rv = lane < m;
-
-    float a[N];
+    const bool cv = lane < n;
+    float col[M];
+    const float* Ac = A + (long long)lane * lda;
 #pragma unroll
-    for (int c = 0; c < N; c++) a[c] = rv ? A[lane + (long long)c * lda] : 0.0f;
+    for (int r = 0; r < M; r++) col[r] = cv ? Ac[r] : 0.0f;
     float mytau = 0.0f;
-
-    qr_warp_all<N>(a, mytau, xw, cw, lane, m, rv, std::make_integer_sequence<int, N>{});
-
-    if (rv) {
+    qr_col_all<M>(col, mytau, vbuf[warp], lane, n, std::make_integer_sequence<int, M>{});
+    if (cv) {
+        float* Aw = A + (long long)lane * lda;
 #pragma unroll
-        for (int c = 0; c < N; c++) A[lane + (long long)c * lda] = a[c];
+        for (int r = 0; r < M; r++) Aw[r] = col[r];
     }
-    if (lane < m && lane < N) tau[lane] = mytau;
+    if (lane < M && lane < n) tau[lane] = mytau;
 }
 
 constexpr int kQrThreads = 256;
@@ -226,10 +225,10 @@ extern "C" aclblasStatus_t aclblasSgeqrfBatched(aclblasHandle_t handle, int m, i
     cudaStream_t st = handle->stream;
     if (m <= 32 && n <= 32) {
         const unsigned grid = (unsigned)((batchSize + kQrWarps - 1) / kQrWarps);
-        switch (n) {
-#define OPSBLAS_GEQRF_CASE(NN)                                                                                      \
-    case NN:                                                                                                        \
-        geqrf_warp_kernel<NN><<<grid, kQrWarps * 32, 0, st>>>(Aarray, m, lda, TauArray, batchSize);                 \
+        switch (m) {
+#define OPSBLAS_GEQRF_CASE(MM)                                                                                      \
+    case MM:                                                                                                        \
+        geqrf_col_kernel<MM><<<grid, kQrWarps * 32, 0, st>>>(Aarray, n, lda, TauArray, batchSize);                  \
         break;
             OPSBLAS_FOR_N_1_32(OPSBLAS_GEQRF_CASE)
 #undef OPSBLAS_GEQRF_CASE
