@@ -488,7 +488,7 @@ def section_gels(ob, h, dev, peak, reps=5, batch=65536):
     return {"workload": f"gels_32x16_nrhs2_b{batch}", "matrices_s": batch / (t * 1e-3), "ms": t,
             "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved_GB_s": alg / (t * 1e-3) / 1e9,
                          "frac": alg / (t * 1e-3) / 1e9 / peak},
-            "note": "one CTA per matrix with serial sums (correctness path)"}
+            "note": "warp per system (M >= N, M <= 32, N + nrhs <= 32), serial row-order sums"}
 
 
 def run_section(args):

@@ -12,13 +12,17 @@
 //   M <  N: LQ by row reflectors, forward substitution L y = c (same stop rule), rows M..N-1 of C
 //           zeroed, Q^T applied in reverse reflector order.
 // info is per matrix (device array), as the reference kernel writes it (its CPU golden keeps one
-// value for the batch). One CTA per matrix: thread 0 forms each reflector, threads take the
-// independent columns / rows / right-hand sides of every step, and every sum runs in index order
-// with each product rounded before it is added -- bit for bit the CPU oracle's restatement.
+// value for the batch). Small QR-path systems run a warp per system (gels_warp_kernel); the rest
+// one CTA per matrix: thread 0 forms each reflector, threads take the independent columns / rows /
+// right-hand sides of every step. Every sum runs in index order with each product rounded before
+// it is added -- bit for bit the CPU oracle's restatement, on both paths.
 // Parity with the reference is its tests' rule (MERE_MARE on the solution against LAPACK sgels_).
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "internal.h"
+#include "small_common.cuh"
 
 namespace opsblas {
 
@@ -195,6 +199,143 @@ gels_kernel(int trans, int m, int n, int nrhs, float* const* __restrict__ Aarray
     }
 }
 
+// Fast path, effective M >= N, M <= 32, N + nrhs <= 32: one warp per system. Lane c < N holds
+// column c of the (transposed, for trans T) matrix, lane N + j holds right-hand side j, rows in
+// registers. Reflector k is formed by lane k (norm, scale of v), published through shared memory
+// and applied by every later column lane and every right-hand-side lane in the same step -- the
+// reference applies Q^T to C after the factorisation, but each reflector meets the same column
+// state either way, so the bits agree. R then goes to shared memory and each right-hand-side lane
+// solves R x = c in row order (same stop rule as the CTA kernel).
+constexpr int kGelsWarps = 4;
+
+template <int M, int K>
+__device__ __forceinline__ void gels_warp_step(float (&col)[M], float* vb, int lane, int ncols, float& tau_k)
+{
+    // xnorm = ||A(K+1:, K)||, row order, formed by every lane for its own column (lane K's is used)
+    float ss = 0.0f;
+#pragma unroll
+    for (int r = K + 1; r < M; r++) ss = __fadd_rn(ss, __fmul_rn(col[r], col[r]));
+    const float xnorm = sqrtf(__shfl_sync(0xffffffffu, ss, K));
+    const float akk = __shfl_sync(0xffffffffu, col[K], K);
+    if (xnorm < 1.0e-30f && akk >= 0.0f) {
+        tau_k = 0.0f;
+        return;  // uniform
+    }
+    const float na = fabsf(akk);
+    const float sc = na > xnorm ? na : xnorm;
+    const float sa = __fdiv_rn(akk, sc), sx = __fdiv_rn(xnorm, sc);
+    const float nm = __fmul_rn(sc, sqrtf(__fadd_rn(__fmul_rn(sa, sa), __fmul_rn(sx, sx))));
+    const float beta = akk >= 0.0f ? -nm : nm;
+    const float t = __fdiv_rn(__fsub_rn(beta, akk), beta);
+    const float scalev = __fdiv_rn(1.0f, __fsub_rn(akk, beta));
+    tau_k = t;
+    if (lane == K) {
+        col[K] = beta;
+#pragma unroll
+        for (int r = K + 1; r < M; r++) {
+            col[r] = __fmul_rn(col[r], scalev);
+            vb[r] = col[r];
+        }
+    }
+    __syncwarp();
+    if (lane > K && lane < ncols) {
+        // w = v . a + a(K); a(K) -= t w; a += (-t w) v
+        float w = 0.0f;
+#pragma unroll
+        for (int r = K + 1; r < M; r++) w = __fadd_rn(w, __fmul_rn(vb[r], col[r]));
+        w = __fadd_rn(w, col[K]);
+        col[K] = __fsub_rn(col[K], __fmul_rn(t, w));
+        const float alpha = -__fmul_rn(t, w);
+#pragma unroll
+        for (int r = K + 1; r < M; r++) col[r] = __fadd_rn(col[r], __fmul_rn(alpha, vb[r]));
+    }
+    __syncwarp();  // v read before the next reflector writes it
+}
+
+template <int M, int... K>
+__device__ __forceinline__ void gels_warp_all(float (&col)[M], float* vb, int lane, int ncols, int N, float* tau,
+                                              std::integer_sequence<int, K...>)
+{
+    ((K < N ? gels_warp_step<M, K>(col, vb, lane, ncols, tau[K]) : void()), ...);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kGelsWarps * 32)
+gels_warp_kernel(int trans, int m, int n, int nrhs, float* const* __restrict__ Aarray, int lda,
+                 float* const* __restrict__ Carray, int ldc, int* __restrict__ info, int batch)
+{
+    __shared__ float vbuf[kGelsWarps][32];
+    __shared__ float rbuf[kGelsWarps][32 * 33];  // R (N x N), column c at rbuf[c * 33]
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const long long b = (long long)blockIdx.x * kGelsWarps + warp;
+    if (b >= batch) return;  // warp-uniform
+    float* A = Aarray[b];
+    float* C = Carray[b];
+    const int N = trans ? m : n;  // effective columns (M = effective rows)
+    const int ncols = N + nrhs;
+    float col[M];
+    if (lane < N) {
+#pragma unroll
+        for (int r = 0; r < M; r++) col[r] = trans ? A[lane + (long long)r * lda] : A[r + (long long)lane * lda];
+    } else if (lane < ncols) {
+        const float* c = C + (long long)(lane - N) * ldc;
+#pragma unroll
+        for (int r = 0; r < M; r++) col[r] = c[r];
+    } else {
+#pragma unroll
+        for (int r = 0; r < M; r++) col[r] = 0.0f;
+    }
+    float tau[32];
+    gels_warp_all<M>(col, vbuf[warp], lane, ncols, N, tau, std::make_integer_sequence<int, M>{});
+    // factors back (trans: the n x m transpose with leading dimension n, as the reference leaves it)
+    if (lane < N) {
+        if (trans) {
+            __syncwarp();  // every lane has read its row of A before any lane writes the transpose
+#pragma unroll
+            for (int r = 0; r < M; r++) A[r + (long long)lane * M] = col[r];
+        } else {
+#pragma unroll
+            for (int r = 0; r < M; r++) A[r + (long long)lane * lda] = col[r];
+        }
+    } else if (trans) {
+        __syncwarp();
+    }
+    // R to shared memory; the highest zero diagonal stops the first right-hand side there
+    float* R = rbuf[warp];
+    if (lane < N) {
+#pragma unroll
+        for (int r = 0; r < M; r++)
+            if (r < N) R[lane * 33 + r] = col[r];
+    }
+    __syncwarp();
+    int stop = -1;
+    for (int i = N - 1; i >= 0; i--)
+        if (R[i * 33 + i] == 0.0f) {
+            stop = i;
+            break;
+        }
+    const int j = lane - N;
+    if (j >= 0 && j < (stop >= 0 ? 1 : nrhs)) {
+#pragma unroll
+        for (int i = M - 1; i >= 0; i--) {
+            if (i < N && i > stop) {
+                float sum = 0.0f;
+#pragma unroll
+                for (int q = i + 1; q < M; q++)
+                    if (q < N) sum = __fadd_rn(sum, __fmul_rn(R[q * 33 + i], col[q]));
+                col[i] = __fdiv_rn(__fsub_rn(col[i], sum), R[i * 33 + i]);
+            }
+        }
+    }
+    if (j >= 0 && j < nrhs) {
+        float* c = C + (long long)j * ldc;
+#pragma unroll
+        for (int r = 0; r < M; r++) c[r] = col[r];
+    }
+    if (lane == 0) info[b] = stop >= 0 ? stop + 1 : 0;
+}
+
 size_t gels_smem_bytes(int trans, int m, int n, int lda)
 {
     const int k = m < n ? m : n;
@@ -242,6 +383,22 @@ extern "C" aclblasStatus_t aclblasSgelsBatched(aclblasHandle_t handle, aclblasOp
     if (m == 0 || n == 0 || nrhs == 0 || batchSize == 0) return ACLBLAS_STATUS_SUCCESS;
 
     const int t = trans == ACLBLAS_OP_T ? 1 : 0;
+    const int effM = t ? n : m, effN = t ? m : n;
+    if (effM >= effN && effM <= 32 && effN + nrhs <= 32) {
+        const unsigned grid = (unsigned)((batchSize + kGelsWarps - 1) / kGelsWarps);
+        switch (effM) {
+#define OPSBLAS_GELS_CASE(MM)                                                                                       \
+    case MM:                                                                                                        \
+        gels_warp_kernel<MM><<<grid, kGelsWarps * 32, 0, handle->stream>>>(t, m, n, nrhs, Aarray, lda, Carray, ldc,  \
+                                                                           devInfo, batchSize);                     \
+        break;
+            OPSBLAS_FOR_N_1_32(OPSBLAS_GELS_CASE)
+#undef OPSBLAS_GELS_CASE
+            default:
+                break;
+        }
+        return launch_status(kApi, cudaGetLastError());
+    }
     const size_t smem = gels_smem_bytes(t, m, n, lda);
     if (smem > kGelsMaxSmem) {
         log_error(kApi, "the transposed solve needs lda*n <= %zu floats of shared memory, got lda=%d n=%d",

@@ -57,6 +57,21 @@ def test_gels_singular_members(handle, shape):
     assert info[1] > 0
 
 
+@pytest.mark.parametrize("shape", [("N", 32, 16, 2), ("N", 32, 31, 1), ("N", 20, 3, 29), ("T", 9, 24, 8),
+                                   ("T", 1, 32, 3), ("N", 32, 1, 31), ("T", 16, 16, 16)])
+def test_gels_warp_path_shapes(handle, shape):
+    """Shapes of the warp-per-system path (M >= N, M <= 32, N + nrhs <= 32) with padding, singular
+    members and a batch that is not a multiple of the warps per CTA."""
+    t, m, n, nrhs = shape
+    lda, ldc, batch = m + 2, max(m, n) + 3, 23
+    rng = np.random.default_rng(m * 131 + n * 7 + nrhs)
+    a = rng.standard_normal((batch, n, lda)).astype(np.float32)
+    c = rng.standard_normal((batch, nrhs, ldc)).astype(np.float32)
+    a[4] = 0.0
+    a[5, 0, :] = 0.0
+    check(handle, t, a, c, m, n, nrhs, lda, ldc, f"{t} {m}x{n}x{nrhs}")
+
+
 def test_gels_large_batch(handle):
     row = ("big", "N", 32, 16, 2, 32, 32, 4096, "RANDOM", "-", "SUCCESS", "overdetermined")
     a, c = gels_inputs(row, 5)
