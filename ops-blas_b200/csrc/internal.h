@@ -83,9 +83,4 @@ void reg_default_shape(int n, int& rows, int& warps);
 cudaError_t getrf_reg_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch,
                              int rows, int warps);
 
-// getrf_medium.cu: 32 < n <= 128, matrix resident in shared memory.
-bool getrf_medium_supported(int n);
-cudaError_t getrf_medium_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info,
-                                int batch);
-
 }  // namespace opsblas

@@ -1,4 +1,4 @@
-// LU building blocks shared by the batched kernels (getrf.cu, getrf_medium.cu) and the grouped
+// LU building blocks shared by the batched kernels (getrf.cu, getrf_reg.cu) and the grouped
 // persistent kernel (grouped.cu). Each block restates the reference's unblocked right-looking
 // LU (sgetrf_batched_kernel.cpp:106-150): first-maximum pivot, whole-row interchange,
 // multipliers by true division, one fmaf per update in column order, stop at the first
@@ -428,232 +428,11 @@ __device__ __forceinline__ void reg_solve_global(const float* A, int lda, int n,
 }
 
 // =============================================================================================
-// Blocked LU of one matrix resident in shared memory (32 < n <= 128), run by a team of NT
-// threads (NT = 64 or 128; the team's first warp factors the panels). The reference's arithmetic
-// reorganised into panels of PB columns:
-//   1. panel: warp 0 factors columns k0..k0+PB-1 of the rows k0..n-1, up to 4 rows per lane
-//      in registers, first-maximum pivots by redux.sync, multipliers by division;
-//   2. U12: rows k0..k0+PB-1 right of the panel, forward substitution with the panel's unit
-//      L11 in order m = 0..PB-1 (what the reference's rank-1 updates do to those rows);
-//   3. A22 -= L21 * U12 with 4x4 register tiles whose accumulators start from A22 and add
-//      the PB products in order -- one fmaf per product, exactly the reference sequence.
-// Every element receives the same products in the same order for any PB, so PB and NT are free
-// tuning choices. Rows never move in shared memory: pivoting only updates a logical-to-physical
-// row map. On an exactly-zero pivot at column k the panel's columns before k are still applied
-// to the trailing columns (steps 2-3 with a narrower panel), so a singular matrix ends in the
-// reference's state too.
+// Triangular solve from factors held in shared memory (32 < n <= 128; the grouped kernel stages
+// its register-resident factors there for the right-hand sides).
 // =============================================================================================
 constexpr int kMedMaxN = 128;
-constexpr int kMedRows = kMedMaxN / 32;  // panel rows per lane
-
-struct MedLayout {
-    int ld;       // column stride of the resident matrix (odd: conflict-free row access)
-    int ls_ld;    // row stride of the staged L21 / U12 blocks (multiple of 4)
-    int mat;      // floats reserved for the matrix (multiple of 4: 16-byte aligned staging)
-    size_t bytes;
-    __host__ __device__ MedLayout(int n, int pb)
-    {
-        ld = n | 1;
-        ls_ld = (n + 3) & ~3;
-        mat = (ld * n + 3) & ~3;
-        bytes = (size_t)mat * 4               // matrix
-                + (size_t)2 * pb * ls_ld * 4  // staged L21 (transposed) and U12
-                + (size_t)n * 4               // row map
-                + (size_t)2 * 32 * 4          // pivot row broadcast (double buffered)
-                + 64;                         // scalars
-        bytes = (bytes + 15) & ~(size_t)15;
-    }
-};
-
-// Views of a team's shared-memory region laid out by MedLayout.
-struct MedSmem {
-    float* sa;    // resident matrix, column-major, ld
-    float* l21;   // [PB][lsd]: l21[m*lsd + i'] = L(r0+i', k0+m)
-    float* u12;   // [PB][lsd]: u12[m*lsd + j'] = U(k0+m, j0+j')
-    int* rmap;    // logical row -> physical row
-    float* prow;  // 2 x 32 floats
-    int* sc;      // scalars: [0] info, [1] panel columns applied
-    __device__ MedSmem(float* base, const MedLayout& L, int n, int pb)
-    {
-        sa = base;
-        l21 = sa + L.mat;
-        u12 = l21 + pb * L.ls_ld;
-        rmap = reinterpret_cast<int*>(u12 + pb * L.ls_ld);
-        prow = reinterpret_cast<float*>(rmap + n);
-        sc = reinterpret_cast<int*>(prow + 64);
-    }
-};
-
-// Factors the matrix in S.sa (loaded by the caller, rmap = identity, sc[0] = 0, pm zeroed when
-// pivoting). Returns info. tid is the thread's index within the team.
-template <bool PIVOT, int NT, int PB>
-__device__ __forceinline__ int med_getrf_core(const MedSmem& S, int n, int ld, int lsd, int* pm, int tid, int bar)
-{
-    float* sa = S.sa;
-    float* l21 = S.l21;
-    float* u12 = S.u12;
-    int* rmap = S.rmap;
-    float* prow = S.prow;
-    int* sc = S.sc;
-    const int lane = tid & 31, warp = tid >> 5;
-
-    for (int k0 = 0; k0 < n; k0 += PB) {
-        const int pb = min(PB, n - k0);
-        // ---------------------------------------------------------------- 1. panel --
-        if (warp == 0) {
-            float pr[kMedRows][PB];
-            int pos[kMedRows], phys[kMedRows];
-#pragma unroll
-            for (int t = 0; t < kMedRows; t++) {
-                const int i = k0 + lane + 32 * t;
-                pos[t] = i;
-                phys[t] = i < n ? rmap[i] : 0;
-#pragma unroll
-                for (int c = 0; c < PB; c++) pr[t][c] = (i < n && c < pb) ? sa[phys[t] + (k0 + c) * ld] : 0.0f;
-            }
-            int done = pb;
-            int inf = 0;
-#pragma unroll
-            for (int c = 0; c < PB; c++) {
-                if (c >= pb) break;
-                const int k = k0 + c;
-                float* buf = prow + 32 * (c & 1);
-                int ppos = k;
-                if (PIVOT) {
-                    // lane-local first maximum (ties to the lowest logical row), then warp-wide
-                    unsigned bkey = 0, bpos = 0xffffffffu;
-#pragma unroll
-                    for (int t = 0; t < kMedRows; t++) {
-                        const bool elig = pos[t] < n && pos[t] >= k;
-                        const float v = fabsf(pr[t][c]);
-                        const unsigned key = (elig && v > 0.0f) ? __float_as_uint(v) : 0u;
-                        if (elig && (key > bkey || (key == bkey && (unsigned)pos[t] < bpos))) {
-                            bkey = key;
-                            bpos = (unsigned)pos[t];
-                        }
-                    }
-                    ppos = (int)seg_argmax<32>(bkey, bpos, 0);
-                }
-                // the pivot row's owner publishes it
-#pragma unroll
-                for (int t = 0; t < kMedRows; t++) {
-                    if (pos[t] == ppos) {
-#pragma unroll
-                        for (int cc = 0; cc < PB; cc++) buf[cc] = pr[t][cc];
-                    }
-                }
-                __syncwarp();
-                const float pv = buf[c];
-                if (PIVOT && lane == 0) pm[k] = ppos + 1;
-                if (pv == 0.0f) {
-                    inf = k + 1;
-                    done = c;
-                    break;
-                }
-#pragma unroll
-                for (int t = 0; t < kMedRows; t++) {
-                    if (pos[t] == ppos)
-                        pos[t] = k;
-                    else if (pos[t] == k)
-                        pos[t] = ppos;
-                }
-#pragma unroll
-                for (int t = 0; t < kMedRows; t++) {
-                    if (pos[t] < n && pos[t] > k) {
-                        const float l = pr[t][c] / pv;
-                        pr[t][c] = l;
-#pragma unroll
-                        for (int cc = c + 1; cc < PB; cc++) pr[t][cc] = fmaf(-l, buf[cc], pr[t][cc]);
-                    }
-                }
-            }
-            // write the panel back in place, record the new logical order
-#pragma unroll
-            for (int t = 0; t < kMedRows; t++) {
-                if (k0 + lane + 32 * t < n) {
-#pragma unroll
-                    for (int c = 0; c < PB; c++)
-                        if (c < pb) sa[phys[t] + (k0 + c) * ld] = pr[t][c];
-                }
-            }
-            __syncwarp();
-#pragma unroll
-            for (int t = 0; t < kMedRows; t++)
-                if (k0 + lane + 32 * t < n) rmap[pos[t]] = phys[t];
-            if (lane == 0) {
-                sc[0] = inf;
-                sc[1] = done;
-            }
-        }
-        team_sync<NT>(bar);
-        const int w = sc[1];     // panel columns to apply (pb, or fewer after a zero pivot)
-        const int j0 = k0 + pb;  // first column right of the panel
-        const int r0 = k0 + w;   // first row of the trailing block
-        const int rest = n - j0;
-        if (w > 0 && rest > 0) {
-            // ------------------------------------------------ 2. U12 (+ staging) --
-            for (int jj = tid; jj < rest; jj += NT) {
-                const int j = j0 + jj;
-                float u[PB];
-#pragma unroll
-                for (int r = 0; r < PB; r++) u[r] = r < w ? sa[rmap[k0 + r] + j * ld] : 0.0f;
-#pragma unroll
-                for (int mm = 0; mm < PB; mm++) {
-                    if (mm < w) {
-#pragma unroll
-                        for (int r = mm + 1; r < PB; r++)
-                            if (r < w) u[r] = fmaf(-sa[rmap[k0 + r] + (k0 + mm) * ld], u[mm], u[r]);
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < PB; r++) {
-                    if (r < w) {
-                        sa[rmap[k0 + r] + j * ld] = u[r];
-                        u12[r * lsd + jj] = u[r];
-                    }
-                }
-            }
-            const int rows = n - r0;  // rows below the applied panel columns
-            for (int e = tid; e < rows * w; e += NT) {
-                const int ii = e % rows, mm = e / rows;
-                l21[mm * lsd + ii] = sa[rmap[r0 + ii] + (k0 + mm) * ld];
-            }
-            team_sync<NT>(bar);
-            // ------------------------------------------- 3. A22 -= L21 * U12 --
-            const int tr = (rows + 3) / 4, tc = (rest + 3) / 4;
-            for (int tile = tid; tile < tr * tc; tile += NT) {
-                const int bi = (tile % tr) * 4, bj = (tile / tr) * 4;
-                float acc[4][4];
-                int pr4[4];
-#pragma unroll
-                for (int a = 0; a < 4; a++) pr4[a] = (bi + a < rows) ? rmap[r0 + bi + a] : -1;
-#pragma unroll
-                for (int a = 0; a < 4; a++)
-#pragma unroll
-                    for (int b = 0; b < 4; b++)
-                        acc[a][b] = (pr4[a] >= 0 && bj + b < rest) ? sa[pr4[a] + (j0 + bj + b) * ld] : 0.0f;
-                for (int mm = 0; mm < w; mm++) {
-                    const float4 lv = *reinterpret_cast<const float4*>(l21 + mm * lsd + bi);
-                    const float4 uv = *reinterpret_cast<const float4*>(u12 + mm * lsd + bj);
-                    const float la[4] = {-lv.x, -lv.y, -lv.z, -lv.w};
-                    const float ub[4] = {uv.x, uv.y, uv.z, uv.w};
-#pragma unroll
-                    for (int a = 0; a < 4; a++)
-#pragma unroll
-                        for (int b = 0; b < 4; b++) acc[a][b] = fmaf(la[a], ub[b], acc[a][b]);
-                }
-#pragma unroll
-                for (int a = 0; a < 4; a++)
-#pragma unroll
-                    for (int b = 0; b < 4; b++)
-                        if (pr4[a] >= 0 && bj + b < rest) sa[pr4[a] + (j0 + bj + b) * ld] = acc[a][b];
-            }
-        }
-        team_sync<NT>(bar);
-        if (sc[0] != 0) break;
-    }
-    return sc[0];
-}
+constexpr int kMedRows = kMedMaxN / 32;  // rows per lane
 
 // Solves right-hand-side column y (n values, logical order after the interchanges: the lane's
 // rows i = lane + 32 t enter with y[t] = b[rmap[i]]) with the factors held in shared memory at
