@@ -370,63 +370,6 @@ __device__ __forceinline__ int reg_getrf_core(float (&a)[R][RegShape<R, NW>::CW]
     return info;
 }
 
-// Solves one right-hand side column bc (n values) with the factors already stored in logical
-// row order at A (leading dimension lda) and the team's lmap, in the reference getrs's order
-// (trans N): b permuted, unit-L forward sweep, U backward sweep with x_j = y_j / U(j,j), one
-// fmaf per update. Run by one warp; lane l handles logical rows l + 32 t.
-template <int R>
-__device__ __forceinline__ void reg_solve_global(const float* A, int lda, int n, float* bc, const int* lmap,
-                                                 int lane)
-{
-    float y[R];
-#pragma unroll
-    for (int t = 0; t < R; t++) {
-        const int i = lane + 32 * t;
-        y[t] = i < n ? bc[lmap[i]] : 0.0f;
-    }
-    __syncwarp();  // every lane has read its b before any lane writes x
-#pragma unroll
-    for (int kq = 0; kq < R; kq++) {
-#pragma unroll 4
-        for (int kl = 0; kl < 32; kl++) {
-            const int k = kq * 32 + kl;
-            if (k >= n) break;
-            const float yk = __shfl_sync(0xffffffffu, y[kq], kl);
-            const float* col = A + (long long)k * lda;
-#pragma unroll
-            for (int t = kq; t < R; t++) {
-                const int i = lane + 32 * t;
-                if (i > k && i < n) y[t] = fmaf(-col[i], yk, y[t]);
-            }
-        }
-    }
-#pragma unroll
-    for (int kq = R - 1; kq >= 0; kq--) {
-#pragma unroll 4
-        for (int kl = 31; kl >= 0; kl--) {
-            const int k = kq * 32 + kl;
-            if (k >= n) continue;
-            const float* col = A + (long long)k * lda;
-            const float t0 = (lane == kl) ? y[kq] / col[k] : 0.0f;
-            const float xk = __shfl_sync(0xffffffffu, t0, kl);
-#pragma unroll
-            for (int t = 0; t <= kq; t++) {
-                const int i = lane + 32 * t;
-                if (i == k)
-                    y[t] = xk;
-                else if (i < k)
-                    y[t] = fmaf(-col[i], xk, y[t]);
-            }
-        }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int t = 0; t < R; t++) {
-        const int i = lane + 32 * t;
-        if (i < n) bc[i] = y[t];
-    }
-}
-
 // =============================================================================================
 // Triangular solve from factors held in shared memory (32 < n <= 128; the grouped kernel stages
 // its register-resident factors there for the right-hand sides).
