@@ -8,7 +8,9 @@
 //   n <= 32, nrhs == 1 : getrs_small_kernel, rows of LU in registers, shuffle broadcasts;
 //   n <= 32, nrhs >= 2 : getrs_rhs_kernel, one lane per right-hand side, LU staged in shared
 //                        memory by cp.async;
-//   n  > 32, trans N   : getrs_blk_kernel (getrs_blk.cu), blocked, right-hand sides in shared memory;
+//   n  > 32, trans N   : getrs_trhs_kernel<false> (getrs_trhs.cu), one thread per right-hand side,
+//                        for n <= 128 with at least 65536 right-hand sides in the batch; otherwise
+//                        getrs_blk_kernel (getrs_blk.cu), blocked, right-hand sides in shared memory;
 //   n  > 32, trans T/C : getrs_trhs_kernel (getrs_trhs.cu), one thread per right-hand side;
 //   larger n than either handles: getrs_generic_kernel, one CTA per matrix in global memory.
 #include <cuda_runtime.h>
@@ -126,6 +128,8 @@ cudaError_t getrs_launch(cudaStream_t st, bool tr, int n, int nrhs, const float*
             getrs_small_dispatch_t(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
         else
             getrs_small_dispatch_n(n, st, Aarray, lda, devIpiv, Barray, ldb, nrhs, batchCount);
+    } else if (!tr && getrs_nrhs_preferred(n, nrhs, batchCount)) {
+        return getrs_nrhs_launch(st, n, nrhs, Aarray, lda, devIpiv, Barray, ldb, batchCount);
     } else if (!tr && getrs_blk_supported(n)) {
         return getrs_blk_launch(st, n, nrhs, Aarray, lda, devIpiv, Barray, ldb, batchCount);
     } else if (tr && getrs_trhs_supported(n)) {

@@ -53,6 +53,9 @@ cudaError_t getrs_blk_launch(cudaStream_t st, int n, int nrhs, const float* cons
 bool getrs_trhs_supported(int n);
 cudaError_t getrs_trhs_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda, const int* ipiv,
                               float* const* Barray, int ldb, int batch);
+bool getrs_nrhs_preferred(int n, int nrhs, int batch);
+cudaError_t getrs_nrhs_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda, const int* ipiv,
+                              float* const* Barray, int ldb, int batch);
 // C = alpha * op(A) * op(B) + beta * C, FP32 operands; round: 0 none, 1 TF32, 2 BF16.
 cudaError_t gemm_f32_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                             const float* const* A, int lda, const float* const* B, int ldb, float beta,
