@@ -21,7 +21,8 @@ Multi-GPU (torchrun): replicas only -- every rank runs its own batch, no collect
 data path; value = all ranks' matrices / max-over-ranks time.
 
 sections (single GPU, skipped with --no-sections): grouped uneven batch vs per-n launches,
-mixed precision + refinement vs plain FP32, adjoint, fused matinv, geqrf and gels; --section NAME
+mixed precision + refinement vs plain FP32, adjoint, fused matinv, geqrf, gels and complex GEMM;
+--section NAME
 [--small] runs one of them alone.
 """
 from __future__ import annotations
@@ -491,6 +492,62 @@ def section_gels(ob, h, dev, peak, reps=5, batch=65536):
             "note": "warp per system (M >= N, M <= 32, N + nrhs <= 32), serial row-order sums"}
 
 
+# FP32 FMA peak of the CUDA cores: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz (nominal; not measured)
+FP32_SIMT_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def section_cgemm(ob, h, dev, reps=5, batch=16384):
+    """aclblasCgemmBatched, 64 x 64 x 64 complex, alpha and beta complex (C read and written),
+    inputs in HBM (1.5 GiB, larger than L2). FP32 CUDA-core bound: 8 m n k FLOP per matrix.
+    Beside it, for context: torch.bmm on complex64 tensors of the same shape (cuBLAS), and the
+    reference golden's BLAS (scipy's OpenBLAS cgemm, one thread) on a host sample."""
+    import time
+
+    import torch
+
+    m = n = k = 64
+    g = torch.Generator(device=dev).manual_seed(17)
+    A = torch.randn((batch, k, m), dtype=torch.complex64, device=dev, generator=g)
+    B = torch.randn((batch, n, k), dtype=torch.complex64, device=dev, generator=g)
+    Cm = torch.randn((batch, n, m), dtype=torch.complex64, device=dev, generator=g)
+    pa, pb, pc = ob.ptr_array(A), ob.ptr_array(B), ob.ptr_array(Cm)
+    alpha, beta = 1.5 + 0.3j, 0.3 - 0.1j
+    t = _events_ms(lambda: h.cgemm("N", "N", m, n, k, alpha, A, m, B, k, beta, Cm, m, aptr=pa, bptr=pb, cptr=pc),
+                   reps)
+    D = torch.empty_like(Cm)
+    t_lib = _events_ms(lambda: torch.bmm(B, A, out=D), reps)  # (A B)^T = B^T A^T in row-major storage
+    flop = 8.0 * m * n * k * batch
+    out = {"workload": f"cgemm_64x64x64_b{batch}", "matrices_s": batch / (t * 1e-3), "ms": t,
+           "GFLOP_s": flop / (t * 1e-3) / 1e9,
+           "roofline": {"bound": "fp32_simt", "achieved_TFLOP_s": flop / (t * 1e-3) / 1e12,
+                        "peak_TFLOP_s": FP32_SIMT_TFLOPS, "frac": flop / (t * 1e-3) / 1e12 / FP32_SIMT_TFLOPS,
+                        "peak_note": "nominal 148 SMs x 128 FP32 lanes x 2 x 1965 MHz"},
+           "torch_bmm_complex64_ms": t_lib,
+           "torch_bmm_note": "cuBLAS complex GEMM of the same shape without alpha/beta, for context"}
+    try:
+        import numpy as np
+        from threadpoolctl import threadpool_limits
+
+        sys.path.insert(0, ROOT)
+        import oracle as O
+
+        ns = 2048
+        rng = np.random.default_rng(0)
+        a = (rng.standard_normal((ns, k, m)) + 1j * rng.standard_normal((ns, k, m))).astype(np.complex64)
+        b = (rng.standard_normal((ns, n, k)) + 1j * rng.standard_normal((ns, n, k))).astype(np.complex64)
+        c = (rng.standard_normal((ns, n, m)) + 1j * rng.standard_normal((ns, n, m))).astype(np.complex64)
+        with threadpool_limits(limits=1):
+            t0 = time.perf_counter()
+            O.ref_cgemm("N", "N", m, n, k, alpha, a, m, b, k, beta, c, m)
+            dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": ns / dt, "unit": "matrices/s", "cores": 1, "kind": "reference",
+                               "sample": f"{ns} matrices 64x64x64: the reference golden's cblas_cgemm (scipy "
+                                         f"OpenBLAS, one thread), {dt:.2f} s"}
+    except Exception as e:  # the baseline is reported, never required
+        out["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+    return out
+
+
 def run_section(args):
     """One measured section on its own (used for profiling captures with --small)."""
     import torch
@@ -509,6 +566,8 @@ def run_section(args):
         out = section_geqrf(ob, h, dev, peak, reps=2, batch=65536 if args.small else 131072)
     elif args.section == "matinv":
         out = section_matinv(ob, h, dev, peak, reps=2, batch=65536 if args.small else 131072)
+    elif args.section == "cgemm":
+        out = section_cgemm(ob, h, dev, reps=2, batch=4096 if args.small else 16384)
     else:
         out = section_adjoint(ob, h, dev, reps=2, batch=8192 if args.small else 65536)
     print(json.dumps({"section": args.section, "small": bool(args.small), **out}))
@@ -523,8 +582,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-sections", action="store_true", help="skip the section measurements (grouped, mixed, adjoint, matinv, geqrf, gels)")
-    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv", "geqrf", "gels"],
+    ap.add_argument("--no-sections", action="store_true", help="skip the section measurements (grouped, mixed, adjoint, matinv, geqrf, gels, cgemm)")
+    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv", "geqrf", "gels", "cgemm"],
                     help="run only this measured section (one JSON line) and exit")
     ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
     args = ap.parse_args()
@@ -706,7 +765,8 @@ def main():
         if world == 1 and not args.no_sections:
             line["sections"] = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
                                 "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak),
-                                "geqrf": section_geqrf(ob, h, dev, peak), "gels": section_gels(ob, h, dev, peak)}
+                                "geqrf": section_geqrf(ob, h, dev, peak), "gels": section_gels(ob, h, dev, peak),
+                                "cgemm": section_cgemm(ob, h, dev)}
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline()

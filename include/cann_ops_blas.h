@@ -157,6 +157,20 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgemmBatched(
     const float* alpha, const float* const Aarray[], int lda, const float* const Barray[], int ldb,
     const float* beta, float* const Carray[], int ldc, int batchCount);
 
+/* Replaces aclblasCgemmBatched (include/cann_ops_blas.h:423;
+ * blas/gemm_batched/arch35/gemm_batched_host.cpp:462-508, 767-819). C[i] = alpha * op(A[i]) *
+ * op(B[i]) + beta * C[i] in single-precision complex, op N, T or C (conjugate transpose), alpha
+ * and beta host values. The reference's decomposition: four FP32 sums T1 = sum Ar Br,
+ * T2 = sum Ai Bi, T3 = sum Ar Bi, T4 = sum Ai Br, then P = (T1 - T2, T3 + T4) and
+ * C = alpha P (+ beta C when beta != 0), each product and sum rounded separately. k == 0 or
+ * alpha == 0 takes P = 0 (beta == 1: C untouched). A null C[i] skips matrix i. Matrix pointers
+ * are 8-byte aligned (as cuComplex). Validation order of ValidateCgemmBatchedParams; every
+ * failure is INVALID_VALUE except the null handle. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasCgemmBatched(
+    aclblasHandle_t handle, aclblasOperation_t transa, aclblasOperation_t transb, int m, int n, int k,
+    const aclblasComplex* alpha, const aclblasComplex* const Aarray[], int lda, const aclblasComplex* const Barray[],
+    int ldb, const aclblasComplex* beta, aclblasComplex* const Carray[], int ldc, int batchCount);
+
 /* Replaces aclblasSmatinvBatched (include/cann_ops_blas.h:434;
  * blas/matinv_batched/arch35/matinv_batched_host.cpp:44-257). Ainv[i] = inverse of A[i] for
  * n <= 32, as aclblasSgetrfBatched on a copy of A followed by aclblasSgetriBatched (bit for

@@ -41,6 +41,13 @@ typedef enum aclblasOperation {
 } aclblasOperation_t;
 #endif
 
+/* Single-precision complex, real part first (include/cann_ops_blas_common.h:67-71); the layout
+ * of cuComplex / std::complex<float>. */
+typedef struct aclblasComplex {
+    float real;
+    float imag;
+} aclblasComplex;
+
 typedef enum aclblasComputeType {
     ACLBLAS_COMPUTE_16F = 0,
     ACLBLAS_COMPUTE_16F_PEDANTIC = 1,

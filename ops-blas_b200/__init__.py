@@ -62,6 +62,8 @@ SIGNATURES = {
                                       C.c_int]),
     "aclblasSgemmBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp,
                                       C.c_int, _vp, _vp, C.c_int, C.c_int]),
+    "aclblasCgemmBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, _vp,
+                                      C.c_int, _vp, _vp, C.c_int, C.c_int]),
     "aclblasGemmBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int,
                                        _vp, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "aclblasSgetrfsRefineBatchedEx": (C.c_int, [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp,
@@ -259,6 +261,19 @@ class Handle:
         check("aclblasSgemmBatched", lib().aclblasSgemmBatched(
             self.h, TRANS[transa], TRANS[transb], m, n, k, C.byref(al), aptr.data_ptr(), lda, bptr.data_ptr(), ldb,
             C.byref(be), cptr.data_ptr(), ldc, Cm.shape[0]))
+
+    def cgemm(self, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, aptr=None, bptr=None,
+              cptr=None):
+        """aclblasCgemmBatched over complex64 batch tensors A, B, C (column-major matrices);
+        alpha, beta Python complex values (aclblasComplex: real, then imaginary)."""
+        aptr = ptr_array(A) if aptr is None else aptr
+        bptr = ptr_array(B) if bptr is None else bptr
+        cptr = ptr_array(Cm) if cptr is None else cptr
+        al = (C.c_float * 2)(complex(alpha).real, complex(alpha).imag)
+        be = (C.c_float * 2)(complex(beta).real, complex(beta).imag)
+        check("aclblasCgemmBatched", lib().aclblasCgemmBatched(
+            self.h, TRANS[transa], TRANS[transb], m, n, k, al, aptr.data_ptr(), lda, bptr.data_ptr(), ldb,
+            be, cptr.data_ptr(), ldc, cptr.shape[0]))
 
     def geqrf(self, A, m, n, lda, tau=None, aptr=None, tptr=None):
         """In-place QR of every matrix of A (batch, n, lda); returns the tau tensor (batch, min(m,n))."""

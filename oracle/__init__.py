@@ -62,6 +62,9 @@ def lib():
         L.oracle_sgeqrf_batched.argtypes = [C.c_int, C.c_int, _f32p, C.c_int64, C.c_int, _f32p, C.c_int64, C.c_int]
         L.oracle_sgels_batched.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_int64, C.c_int, _f32p,
                                            C.c_int64, C.c_int, _i32p, C.c_int, _f32p]
+        L.oracle_cgemm_batched.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                           C.c_float, C.c_float, C.POINTER(_f32p), C.c_int, C.POINTER(_f32p),
+                                           C.c_int, C.POINTER(_f32p), C.c_int, C.c_int]
         L.case_matrix_batch.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_int]
         L.case_rhs_batch.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_uint32, C.c_int]
         _lib = L
@@ -171,7 +174,58 @@ def port_gels(trans, a, m, n, nrhs, lda, c, ldc):
     return info
 
 
+def _ptr_array(x, batch, skip=()):
+    """float* array over the matrices of x (batch, ncols, ld) complex64; None entries at ``skip``."""
+    arr = (_f32p * max(1, batch))()
+    for b in range(batch):
+        if b not in skip:
+            arr[b] = x[b].ctypes.data_as(_f32p)
+    return arr
+
+
+def port_cgemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, skip_c=()):
+    """C restatement of aclblasCgemmBatched, in place on c. a, b, c: complex64 arrays
+    (batch, ncols, ld); alpha, beta: Python complex; ta, tb in 'N', 'T', 'C'; matrices whose index
+    is in ``skip_c`` have a null C pointer."""
+    for x in (a, b, c):
+        assert x.dtype == np.complex64 and x.flags.c_contiguous and x.ndim == 3
+    batch = c.shape[0]
+    lib().oracle_cgemm_batched(TRANS[ta], TRANS[tb], m, n, k, alpha.real, alpha.imag, beta.real, beta.imag,
+                               _ptr_array(a, batch), lda, _ptr_array(b, batch), ldb,
+                               _ptr_array(c, batch, set(skip_c)), ldc, batch)
+
+
 # ----------------------------------------------------------------- reference golden path --
+
+def ref_cgemm(ta, tb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
+    """The reference's Cgemm golden (test/gemm_batched/cgemm_batched/cgemm_batched_golden.h:19-64)
+    over the BLAS it calls: alpha == 0 scales C by beta in FP32 (ApplyComplexAlphaZeroGolden),
+    every other case is cblas_cgemm -- here scipy's OpenBLAS cgemm, the same routine through its
+    Fortran interface. In place on c (complex64, (batch, ncols, ld))."""
+    from scipy.linalg import blas
+
+    if m == 0 or n == 0:
+        return
+    trans = {"N": 0, "T": 1, "C": 2}
+    br, bi = np.float32(beta.real), np.float32(beta.imag)
+    for i in range(c.shape[0]):
+        cm = c[i].T[:m, :n]  # column-major m x n view
+        if alpha == 0:
+            cr, ci = cm.real.copy(), cm.imag.copy()
+            cm.real = br * cr - bi * ci
+            cm.imag = br * ci + bi * cr
+            continue
+        ra, ca = (m, k) if ta == "N" else (k, m)
+        rb, cb = (k, n) if tb == "N" else (n, k)
+        if k == 0:
+            # BLAS with k == 0: C = beta C (zero when beta == 0)
+            cm[...] = 0 if beta == 0 else (np.complex64(beta) * cm)
+            continue
+        am = np.asfortranarray(a[i].T[:ra, :ca])
+        bm = np.asfortranarray(b[i].T[:rb, :cb])
+        out = blas.cgemm(np.complex64(alpha), am, bm, beta=np.complex64(beta), c=np.asfortranarray(cm),
+                         trans_a=trans[ta], trans_b=trans[tb])
+        cm[...] = out
 
 def ref_getrf(a, n, lda, pivot=True, nthreads=0):
     """aclblasSgetrfBatched_cpu in place; returns (piv, info)."""

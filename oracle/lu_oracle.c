@@ -436,3 +436,61 @@ ORACLE_API void oracle_sgels_batched(int trans, int m, int n, int nrhs, float* A
         oracle_sgels(trans, m, n, nrhs, A + (int64_t)b * strideA, lda, C + (int64_t)b * strideC, ldc, info + b,
                      scratch);
 }
+
+/* aclblasCgemmBatched (blas/gemm_batched/arch35/gemm_batched_host.cpp:438-819,
+ * gemm_batched_kernel.cpp:848-1110). Complex values are interleaved (real, imaginary) float
+ * pairs; op 0 = N, 1 = T, 2 = C (conjugate transpose: the imaginary part negated on the
+ * de-interleave). Per output the four real sums T1 = sum Ar Br, T2 = sum Ai Bi, T3 = sum Ar Bi,
+ * T4 = sum Ai Br (one fmaf per product, k in order, as this project's device kernel), then the
+ * reference's combine with every product and sum rounded on its own:
+ *   Pr = T1 - T2, Pi = T3 + T4, Cr = Pr aR - Pi aI, Ci = Pi aR + Pr aI;
+ *   beta != 0: Cr += Cor bR, Ci += Coi bR, Cr -= Coi bI, Ci += Cor bI.
+ * k == 0 or alpha == 0 combines zero sums (LaunchCgemmEarlyExit); with beta == 1 as well nothing
+ * is written. A null C pointer skips the matrix. m, n, batch == 0 return at once. */
+static void cg_elem(int op, const float* X, int ld, int r, int c, float* re, float* im)
+{
+    const int64_t idx = op == 0 ? (int64_t)r + (int64_t)c * ld : (int64_t)c + (int64_t)r * ld;
+    *re = X[2 * idx];
+    *im = op == 2 ? -X[2 * idx + 1] : X[2 * idx + 1];
+}
+
+ORACLE_API void oracle_cgemm_batched(int opa, int opb, int m, int n, int k, float alpha_re, float alpha_im,
+                                     float beta_re, float beta_im, const float* const* A, int lda,
+                                     const float* const* B, int ldb, float* const* C, int ldc, int batch)
+{
+    if (m == 0 || n == 0 || batch == 0) return;
+    const int zero_product = k == 0 || (alpha_re == 0.0f && alpha_im == 0.0f);
+    if (zero_product && beta_re == 1.0f && beta_im == 0.0f) return;
+    const int keff = zero_product ? 0 : k;
+    const int has_beta = beta_re != 0.0f || beta_im != 0.0f;
+    for (int b = 0; b < batch; b++) {
+        float* Cb = C[b];
+        if (Cb == NULL) continue;
+        for (int j = 0; j < n; j++)
+            for (int i = 0; i < m; i++) {
+                float t1 = 0.0f, t2 = 0.0f, t3 = 0.0f, t4 = 0.0f;
+                for (int p = 0; p < keff; p++) {
+                    float ar, ai, br, bi;
+                    cg_elem(opa, A[b], lda, i, p, &ar, &ai);
+                    cg_elem(opb, B[b], ldb, p, j, &br, &bi);
+                    t1 = fmaf(ar, br, t1);
+                    t2 = fmaf(ai, bi, t2);
+                    t3 = fmaf(ar, bi, t3);
+                    t4 = fmaf(ai, br, t4);
+                }
+                const float pr = t1 - t2, pi = t3 + t4;
+                float cr = pr * alpha_re - pi * alpha_im;
+                float ci = pi * alpha_re + pr * alpha_im;
+                float* c = Cb + 2 * ((int64_t)i + (int64_t)j * ldc);
+                if (has_beta) {
+                    const float cor = c[0], coi = c[1];
+                    cr = cr + cor * beta_re;
+                    ci = ci + coi * beta_re;
+                    cr = cr - coi * beta_im;
+                    ci = ci + cor * beta_im;
+                }
+                c[0] = cr;
+                c[1] = ci;
+            }
+    }
+}

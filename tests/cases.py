@@ -672,3 +672,213 @@ def gels_inputs(row, seed):
         rhs = op @ rng.standard_normal((batch, op.shape[2], nrhs))
     c[:, :nrhs, :rows_b] = np.swapaxes(rhs, 1, 2)
     return a, c
+
+
+# aclblasCgemmBatched rows of test/gemm_batched/cgemm_batched/arch35/cgemm_batched_test.csv
+# (duplicated rows once). Success rows: name transA transB m n k alpha(re;im) beta(re;im) lda ldb
+# ldc batch c_fill (R random, Z zero); 0 for a leading dimension means the CSV's default
+# (cgemm_batched_param.h:83-88: the stored rows of op's operand, ldc = m, at least 1).
+_CGEMM_OK = """
+L0_001 N N 0 128 128 1.0;0.0 0.0;0.0 0 0 128 4 Z
+L0_002 N N 128 0 128 1.0;0.0 0.0;0.0 0 0 128 4 Z
+L0_003 N N 128 128 0 1.0;0.0 0.0;0.0 0 0 128 4 Z
+L0_004 N N 128 128 128 1.0;0.0 0.0;0.0 0 0 128 0 Z
+G1_Msweep_021 N N 1 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Msweep_022 N N 3 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Msweep_023 N N 13 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Msweep_024 N N 32 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Msweep_025 N N 55 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Msweep_026 N N 64 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Msweep_027 N N 128 64 64 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G1_Msweep_028 N N 234 64 64 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G1_Msweep_029 N N 256 64 64 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G1_Msweep_030 N N 128 64 64 1.0;0.5 0.0;0.0 0 0 0 1 Z
+G1_Msweep_031 N N 591 64 64 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G1_Msweep_032 N N 512 64 64 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G1_Nsweep_033 N N 64 1 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_034 N N 64 3 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_035 N N 64 13 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_036 N N 64 32 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_037 N N 64 55 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_038 N N 64 128 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_039 N N 64 234 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_040 N N 64 256 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_041 N N 64 591 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Nsweep_042 N N 64 512 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_043 N N 64 64 1 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_044 N N 64 64 3 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_045 N N 64 64 13 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_046 N N 64 64 32 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_047 N N 64 64 55 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_048 N N 64 64 128 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_049 N N 64 64 234 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_050 N N 64 64 256 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_051 N N 64 64 591 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G1_Ksweep_052 N N 64 64 512 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G2_Mixed_053 N N 1 3 13 1.0;0.0 0.0;0.0 0 0 13 1 Z
+G2_Mixed_054 N N 32 55 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G2_Mixed_055 N N 128 234 256 1.0;0.0 0.0;0.0 0 0 256 1 Z
+G2_Mixed_056 N N 64 64 64 1.0;0.5 0.0;0.0 0 0 64 1 Z
+G2_Mixed_057 N N 64 64 64 0.5;0.3 0.0;0.0 0 0 64 1 Z
+G2_Mixed_058 N N 591 512 128 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G2_Mixed_059 N N 256 13 55 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G2_Mixed_060 N N 512 234 3 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G2_Mixed_061 N N 55 256 591 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G2_Mixed_062 N N 234 128 1 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G2_Mixed_063 N N 13 591 32 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G2_Mixed_064 N N 3 512 234 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G3_Trans_065 N N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_066 N T 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_067 N C 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_068 T N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_069 T T 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_070 T C 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_071 C N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_072 C T 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G3_Trans_073 C C 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G4_Alpha_074 N N 64 64 64 0.0;0.0 0.0;0.0 0 0 64 1 Z
+G4_Alpha_075 N N 64 64 64 0.3;0.0 0.0;0.0 0 0 64 1 Z
+G4_Alpha_076 N N 64 64 64 0.5;0.0 0.0;0.0 0 0 64 1 Z
+G4_Alpha_077 N N 64 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G4_Alpha_078 N N 64 64 64 1.0;0.5 0.0;0.0 0 0 64 1 Z
+G4_Alpha_079 N N 64 64 64 2.0;0.0 0.0;0.0 0 0 64 1 Z
+G4_Alpha_080 N N 64 64 64 2.3;0.0 0.0;0.0 0 0 64 1 Z
+G4_Alpha_081 N N 64 64 64 0.0;2.0 0.0;0.0 0 0 64 1 Z
+G4_Alpha_082 N N 64 64 64 1.5;0.7 0.0;0.0 0 0 64 1 Z
+G5_Beta_083 N N 64 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G5_Beta_084 N N 64 64 64 1.0;0.0 0.3;0.0 0 0 64 1 R
+G5_Beta_085 N N 64 64 64 1.0;0.0 0.5;0.0 0 0 64 1 R
+G5_Beta_086 N N 64 64 64 1.0;0.0 0.7;0.0 0 0 64 1 R
+G5_Beta_087 N N 64 64 64 1.0;0.0 1.0;0.0 0 0 64 1 R
+G5_Beta_088 N N 64 64 64 1.0;0.0 1.2;0.0 0 0 64 1 R
+G5_Beta_089 N N 64 64 64 1.0;0.0 1.7;0.0 0 0 64 1 R
+G5_Beta_090 N N 64 64 64 1.0;0.0 2.0;0.0 0 0 64 1 R
+G5_Beta_091 N N 64 64 64 1.0;0.0 2.3;0.0 0 0 64 1 R
+G6_AB_092 N N 64 64 64 0.0;0.0 0.3;0.0 0 0 64 1 R
+G6_AB_093 N N 64 64 64 0.3;0.5 1.7;0.2 0 0 64 1 R
+G6_AB_094 N N 64 64 64 0.5;0.3 0.5;0.7 0 0 64 1 R
+G6_AB_095 N N 64 64 64 0.7;0.2 2.0;0.5 0 0 64 1 R
+G6_AB_096 N N 64 64 64 1.0;0.0 0.0;0.0 0 0 64 1 Z
+G6_AB_097 N N 64 64 64 1.2;0.3 1.2;0.4 0 0 64 1 R
+G6_AB_098 N N 64 64 64 1.7;0.5 0.3;0.6 0 0 64 1 R
+G6_AB_099 N N 64 64 64 2.0;0.7 0.5;0.3 0 0 64 1 R
+G6_AB_100 N N 64 64 64 2.3;0.1 1.0;0.9 0 0 64 1 R
+G6_AB_101 N N 64 64 64 0.0;0.0 0.0;0.0 0 0 64 1 Z
+G7_Batch_102 N N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 1 R
+G7_Batch_103 N N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 2 R
+G7_Batch_104 N N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 3 R
+G7_Batch_105 N N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 4 R
+G7_Batch_106 N N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 8 R
+G8_Edge_107 N N 1 1 1 1.0;0.0 0.0;0.0 0 0 1 1 Z
+G8_Edge_108 N N 3 3 3 1.0;0.0 0.0;0.0 0 0 3 1 Z
+G8_Edge_109 N N 13 13 13 1.0;0.0 0.0;0.0 0 0 13 1 Z
+G8_Edge_110 N N 1 128 128 1.0;0.0 0.0;0.0 0 0 128 1 Z
+G8_Edge_111 N N 128 1 128 1.0;0.0 0.0;0.0 0 0 128 1 Z
+G8_Edge_112 N N 128 128 1 1.0;0.0 0.0;0.0 0 0 128 1 Z
+G8_Stress_113 T T 128 256 13 2.0;1.0 1.0;0.5 0 0 256 1 R
+G8_Stress_114 N T 256 128 55 1.7;0.7 0.7;0.3 0 0 0 1 R
+G8_Stress_115 N N 234 591 32 0.5;0.3 0.3;0.1 0 0 591 1 R
+G8_Stress_116 N N 128 128 128 1.0;0.0 0.0;0.0 0 0 128 1 Z
+G8_Stress_117 N N 128 128 128 1.5;0.3 0.3;0.0 0 0 128 1 Z
+G8_Stress_118 N N 256 256 128 1.0;0.5 0.5;0.2 0 0 256 1 R
+G8_Stress_119 N N 256 256 256 1.0;0.0 0.0;0.0 0 0 256 1 Z
+G8_Stress_120 N N 256 256 256 1.5;0.3 0.3;0.1 0 0 256 3 R
+G8_Stress_121 T N 128 128 128 0.7;1.7 1.7;0.3 0 0 128 3 R
+G8_Stress_122 N T 1 128 128 2.3;0.0 0.0;0.0 0 0 128 1 Z
+G8_Stress_123 N N 512 512 64 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G8_Stress_124 N N 512 512 512 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G8_Stress_125 N N 512 512 512 1.5;0.3 0.3;0.0 0 0 0 1 R
+G8_Stress_126 N N 591 591 591 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_127 N N 17 19 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_128 N T 17 19 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_129 T N 17 19 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_130 T T 17 19 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_131 N N 33 47 29 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_132 N T 33 47 29 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_133 T N 33 47 29 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_134 T T 33 47 29 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_135 N N 55 13 7 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_136 N T 55 13 7 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_137 T N 55 13 7 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_138 T T 55 13 7 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_139 N N 13 55 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_140 N T 13 55 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_141 T N 13 55 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G9_NonAligned_142 T T 13 55 23 1.0;0.0 0.0;0.0 0 0 0 1 Z
+G10_LdLarge_143 N N 128 128 128 1.0;0.0 0.0;0.0 0 0 128 4 Z
+G10_LdLarge_144 N N 128 128 128 1.0;0.0 0.0;0.0 256 128 128 4 Z
+G10_LdLarge_145 N N 128 128 128 1.0;0.0 0.0;0.0 128 256 128 4 Z
+G10_LdLarge_146 N N 128 128 128 1.0;0.0 0.0;0.0 128 128 256 4 Z
+G11_K0_beta0_147 N N 128 128 0 1.0;0.0 0.0;0.0 0 0 128 4 Z
+G11_K0_beta1_148 N N 128 128 0 1.0;0.0 1.0;0.0 0 0 128 4 R
+G11_K0_beta0p5_149 N N 128 128 0 1.0;0.0 0.5;0.0 0 0 128 4 R
+G11_A0_beta1_150 N N 128 128 128 0.0;0.0 1.0;0.0 0 0 128 4 R
+G11_A0_beta0_151 N N 128 128 128 0.0;0.0 0.0;0.0 0 0 128 4 Z
+G11_A0_betacplx_152 N N 128 128 128 0.0;0.0 0.5;0.3 0 0 128 4 R
+DIAG_M1_PP_NN N N 1 128 128 1.5;0.3 0.3;0.0 0 0 128 1 R
+DIAG_M1_PP_NN_b0 N N 1 128 128 2.0;0.0 0.0;0.0 0 0 128 1 Z
+DIAG_N1_PP_NN N N 128 1 128 1.5;0.3 0.3;0.0 0 0 128 1 R
+DIAG_M1_PP_NT N T 1 128 128 2.3;0.0 0.0;0.0 0 0 128 1 Z
+DIAG_M1_PP_TN T N 1 128 128 1.5;0.3 0.3;0.0 0 0 128 1 R
+DIAG_M3_PP_NN N N 3 128 128 1.5;0.3 0.3;0.0 0 0 128 1 R
+DIAG_M7_PP_NN N N 7 128 128 1.5;0.3 0.3;0.0 0 0 128 1 R
+DIAG_M8_PP_NN N N 8 128 128 1.5;0.3 0.3;0.0 0 0 128 1 R
+DIAG_M9_PP_NN N N 9 128 128 1.5;0.3 0.3;0.0 0 0 128 1 R
+G12_LargeBatch_153 N N 64 64 64 1.5;0.3 0.3;0.0 0 0 64 16 R
+G12_LargeBatch_154 N N 64 64 64 1.0;0.0 0.0;0.0 0 0 64 32 Z
+G12_LargeBatch_155 T T 32 32 32 1.7;0.7 0.7;0.3 0 0 32 16 R
+G12_LargeBatch_156 T T 32 32 32 1.7;0.7 0.7;0.3 0 0 32 64 R
+"""
+# Error rows: name transA transB m n k lda ldb ldc batch nulls(alpha beta A B C) null_handle status
+_CGEMM_ERR = """
+L0_005 N N 128 128 128 0 0 128 4 00000 1 HN
+L0_006 N N -1 128 128 0 0 128 4 00000 0 IV
+L0_007 N N 128 128 128 0 0 128 4 10000 0 IV
+L0_008 N N 128 128 128 0 0 128 4 01000 0 IV
+L0_009 N N 128 128 128 0 0 128 -1 00000 0 IV
+L0_010 N N 128 128 128 0 0 128 4 00100 0 IV
+L0_011 N N 128 128 128 0 0 128 4 00010 0 IV
+L0_012 N N 128 128 128 0 0 128 4 00001 0 IV
+L0_013 N N 128 128 128 64 128 128 4 00000 0 IV
+L0_014 N N 128 128 128 128 64 128 4 00000 0 IV
+L0_015 N N 128 128 128 128 128 64 4 00000 0 IV
+L0_016 T N 128 128 128 64 128 128 4 00000 0 IV
+L0_017 N N 128 -1 128 0 0 128 4 00000 0 IV
+L0_018 N N 128 128 -1 0 0 128 4 00000 0 IV
+L0_019 INVALID N 128 128 128 0 0 128 4 00000 0 IV
+L0_020 N INVALID 128 128 128 0 0 128 4 00000 0 IV
+"""
+
+
+def _cplx(v):
+    re, im = v.split(";")
+    return complex(float(re), float(im))
+
+
+def _cgemm_rows():
+    out = []
+    for line in _CGEMM_OK.split("\n"):
+        if not line.strip():
+            continue
+        name, ta, tb, m, n, k, alpha, beta, lda, ldb, ldc, batch, cfill = line.split()
+        m, n, k = int(m), int(n), int(k)
+        out.append((name, ta, tb, m, n, k, _cplx(alpha), _cplx(beta), _sgemm_ld(lda, m if ta == "N" else k),
+                    _sgemm_ld(ldb, k if tb == "N" else n), _sgemm_ld(ldc, m), int(batch), cfill))
+    return out
+
+
+def _cgemm_errors():
+    out = []
+    for line in _CGEMM_ERR.split("\n"):
+        if not line.strip():
+            continue
+        name, ta, tb, m, n, k, lda, ldb, ldc, batch, nulls, hn, status = line.split()
+        m, n, k = int(m), int(n), int(k)
+        out.append((name, ta, tb, m, n, k, _sgemm_ld(lda, m if ta == "N" else k),
+                    _sgemm_ld(ldb, k if tb == "N" else n), _sgemm_ld(ldc, m), int(batch),
+                    [c == "1" for c in nulls], hn == "1", {"IV": IV, "HN": HN}[status]))
+    return out
+
+
+CGEMM_CASES = _cgemm_rows()
+CGEMM_ERRORS = _cgemm_errors()

@@ -15,7 +15,8 @@ import re
 
 import pytest
 
-from cases import GELS_ROWS, GEQRF_ROWS, GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS, MATINV_ARG_ROWS, SGEMM_ERRORS
+from cases import (CGEMM_ERRORS, GELS_ROWS, GEQRF_ROWS, GETRF_ERRORS, GETRI_ERRORS, GETRS_ERRORS, MATINV_ARG_ROWS,
+                   SGEMM_ERRORS)
 from conftest import ROOT
 
 DUMMY = C.create_string_buffer(256)
@@ -180,6 +181,36 @@ def test_sgemm_batched_noops(ob):
     # k == 0 with beta == 1 leaves C untouched without a launch
     assert L.aclblasSgemmBatched(H, ob.OP_N, ob.OP_N, 8, 8, 0, C.byref(one), P, 8, P, 1, C.byref(one), P, 8,
                                  4) == ob.SUCCESS
+
+
+@pytest.mark.parametrize("row", CGEMM_ERRORS, ids=lambda r: r[0])
+def test_cgemm_batched_error_rows(ob, row):
+    name, ta, tb, m, n, k, lda, ldb, ldc, batch, nulls, null_h, status = row
+    one = (C.c_float * 2)(1.0, 0.0)
+    op = lambda t: 999 if t == "INVALID" else ob.TRANS[t]
+    ptr = lambda null, p: None if null else p
+    st = ob.lib().aclblasCgemmBatched(None if null_h else H, op(ta), op(tb), m, n, k, ptr(nulls[0], one),
+                                      ptr(nulls[2], P), lda, ptr(nulls[3], P), ldb, ptr(nulls[1], one),
+                                      ptr(nulls[4], P), ldc, batch)
+    assert ob.STATUS[st] == status
+
+
+def test_cgemm_batched_validation_order_and_noops(ob):
+    L = ob.lib()
+    one = (C.c_float * 2)(1.0, 0.0)
+    zero = (C.c_float * 2)(0.0, 0.0)
+    # alpha is checked before the dimensions, the operations before the leading dimensions
+    assert L.aclblasCgemmBatched(H, ob.OP_N, ob.OP_N, -1, 8, 8, None, P, 8, P, 8, one, P, 8, 1) == ob.INVALID_VALUE
+    assert L.aclblasCgemmBatched(H, 999, ob.OP_N, 8, 8, 8, one, P, 1, P, 8, one, P, 8, 1) == ob.INVALID_VALUE
+    # conjugate transpose takes its leading dimension from k, like T
+    assert L.aclblasCgemmBatched(H, ob.OP_C, ob.OP_N, 128, 8, 16, one, P, 15, P, 16, one, P, 128,
+                                 1) == ob.INVALID_VALUE
+    # m, n or batch zero: success before any array is read (gemm_batched_host.cpp:791-793)
+    assert L.aclblasCgemmBatched(H, ob.OP_N, ob.OP_N, 0, 128, 128, one, P, 1, P, 128, one, P, 1, 4) == ob.SUCCESS
+    assert L.aclblasCgemmBatched(H, ob.OP_N, ob.OP_N, 8, 8, 8, one, None, 8, None, 8, one, None, 8, 0) == ob.SUCCESS
+    # k == 0 or alpha == 0 with beta == 1 leaves C untouched without a launch (:801-804)
+    assert L.aclblasCgemmBatched(H, ob.OP_N, ob.OP_N, 8, 8, 0, one, P, 8, P, 1, one, P, 8, 4) == ob.SUCCESS
+    assert L.aclblasCgemmBatched(H, ob.OP_T, ob.OP_C, 8, 8, 8, zero, P, 8, P, 8, one, P, 8, 4) == ob.SUCCESS
 
 
 def _geqrf_expected_info(m, n, lda, batch, null_a, null_tau):
