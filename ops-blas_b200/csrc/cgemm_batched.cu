@@ -79,6 +79,26 @@ __device__ __forceinline__ void cg_fetch(const float2* A, int lda, const float2*
     }
 }
 
+// Stores this thread's fetched elements into one stage of the shared-memory planes.
+template <int OPA, int OPB>
+__device__ __forceinline__ void cg_store(float (*Ar)[kCgBM + 4], float (*Ai)[kCgBM + 4], float (*Br)[kCgBN + 4],
+                                         float (*Bi)[kCgBN + 4], int tid, const float2 (&pa)[kCgLoads],
+                                         const float2 (&pb)[kCgLoads])
+{
+#pragma unroll
+    for (int r = 0; r < kCgLoads; r++) {
+        const int e = tid + r * kCgThreads;
+        const int i = OPA == 0 ? e % kCgBM : e / kCgBK;
+        const int kk = OPA == 0 ? e / kCgBM : e % kCgBK;
+        Ar[kk][i] = pa[r].x;
+        Ai[kk][i] = pa[r].y;
+        const int kb = OPB == 0 ? e % kCgBK : e / kCgBN;
+        const int j = OPB == 0 ? e / kCgBK : e % kCgBN;
+        Br[kb][j] = pb[r].x;
+        Bi[kb][j] = pb[r].y;
+    }
+}
+
 // grid.x = (row tile, matrix) pairs, grid.y = column tiles. k == 0 computes P = 0 (the
 // reference's alpha == 0 / k == 0 path) without reading A or B.
 template <int OPA, int OPB>
@@ -86,10 +106,11 @@ __global__ void __launch_bounds__(kCgThreads, 2)
 cgemm_batched_kernel(int m, int n, int k, float2 alpha, float2 beta, const float2* const* Aarray, int lda,
                      const float2* const* Barray, int ldb, float2* const* Carray, int ldc)
 {
-    __shared__ __align__(16) float Ar[kCgBK][kCgBM + 4];
-    __shared__ __align__(16) float Ai[kCgBK][kCgBM + 4];
-    __shared__ __align__(16) float Br[kCgBK][kCgBN + 4];
-    __shared__ __align__(16) float Bi[kCgBK][kCgBN + 4];
+    // two stages of the operand slices: the multiply reads one while the next is stored into the other
+    __shared__ __align__(16) float Ar[2][kCgBK][kCgBM + 4];
+    __shared__ __align__(16) float Ai[2][kCgBK][kCgBM + 4];
+    __shared__ __align__(16) float Br[2][kCgBK][kCgBN + 4];
+    __shared__ __align__(16) float Bi[2][kCgBK][kCgBN + 4];
     const int tiles_m = (m + kCgBM - 1) / kCgBM;
     const long long b = blockIdx.x / tiles_m;
     float2* C = Carray[b];
@@ -105,34 +126,29 @@ cgemm_batched_kernel(int m, int n, int k, float2 alpha, float2 beta, const float
     if (k > 0) {
         const float2* A = Aarray[b];
         const float2* B = Barray[b];
-        // This thread's 4 elements of each operand slice; the next slice is fetched into
-        // registers while the current one is multiplied from shared memory.
+        // This thread's elements of the next operand slice are fetched into registers while the
+        // current one is multiplied from shared memory, then stored into the other stage; one
+        // barrier per slice (the barrier that ends slice t also ends every read of the stage that
+        // slice t + 1 stores into).
         float2 pa[kCgLoads], pb[kCgLoads];
         cg_fetch<OPA, OPB>(A, lda, B, ldb, m, n, k, m0, n0, 0, tid, pa, pb);
+        cg_store<OPA, OPB>(Ar[0], Ai[0], Br[0], Bi[0], tid, pa, pb);
+        __syncthreads();
+        int cur = 0;
         for (int k0 = 0; k0 < k; k0 += kCgBK) {
-#pragma unroll
-            for (int r = 0; r < kCgLoads; r++) {
-                const int e = tid + r * kCgThreads;
-                const int i = OPA == 0 ? e % kCgBM : e / kCgBK;
-                const int kk = OPA == 0 ? e / kCgBM : e % kCgBK;
-                Ar[kk][i] = pa[r].x;
-                Ai[kk][i] = pa[r].y;
-                const int kb = OPB == 0 ? e % kCgBK : e / kCgBN;
-                const int j = OPB == 0 ? e / kCgBK : e % kCgBN;
-                Br[kb][j] = pb[r].x;
-                Bi[kb][j] = pb[r].y;
-            }
-            __syncthreads();
-            if (k0 + kCgBK < k) cg_fetch<OPA, OPB>(A, lda, B, ldb, m, n, k, m0, n0, k0 + kCgBK, tid, pa, pb);
+            const bool more = k0 + kCgBK < k;
+            if (more) cg_fetch<OPA, OPB>(A, lda, B, ldb, m, n, k, m0, n0, k0 + kCgBK, tid, pa, pb);
             const int kn = min(kCgBK, k - k0);
             if (kn == kCgBK) {
 #pragma unroll
-                for (int kk = 0; kk < kCgBK; kk++) cg_step(Ar, Ai, Br, Bi, kk, tx, ty, s);
+                for (int kk = 0; kk < kCgBK; kk++) cg_step(Ar[cur], Ai[cur], Br[cur], Bi[cur], kk, tx, ty, s);
             } else {
                 // the last slice runs only its kn steps, so every sum holds exactly k products
-                for (int kk = 0; kk < kn; kk++) cg_step(Ar, Ai, Br, Bi, kk, tx, ty, s);
+                for (int kk = 0; kk < kn; kk++) cg_step(Ar[cur], Ai[cur], Br[cur], Bi[cur], kk, tx, ty, s);
             }
+            if (more) cg_store<OPA, OPB>(Ar[cur ^ 1], Ai[cur ^ 1], Br[cur ^ 1], Bi[cur ^ 1], tid, pa, pb);
             __syncthreads();
+            cur ^= 1;
         }
     }
 
