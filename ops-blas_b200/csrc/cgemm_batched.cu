@@ -6,11 +6,13 @@
 // (gemm_batched_kernel.cpp:1029-1110): Pr = T1 - T2, Pi = T3 + T4, Cr = Pr aR - Pi aI,
 // Ci = Pi aR + Pr aI, then, when beta != 0, Cr += Cor bR, Ci += Coi bR, Cr -= Coi bI,
 // Ci += Cor bI -- every product and sum rounded on its own. Here one kernel does all of it: each
-// CTA stages a 64 x 16 slice of op(A) and a 16 x 64 slice of op(B) in shared memory as separate
-// real and imaginary planes (the de-interleave, conjugation for op C included, happens on the
-// load), keeps the four sums of its 4 x 4 complex outputs per thread in registers (one fmaf per
-// product, k in order), and applies the combine in the reference's operation order in the
-// epilogue. No workspace, one launch, C read once (only when beta != 0) and written once.
+// CTA owns a 64 x 64 complex tile and walks k in slices of 8, staging op(A) and op(B) slices in
+// shared memory as separate real and imaginary planes (the de-interleave, conjugation for op C
+// included, happens on the load; the next slice is fetched into registers during the multiply and
+// stored into the second of two stages), keeps the four sums of its 4 x 4 complex outputs per
+// thread in registers (one fmaf per product, k in order), and applies the combine in the
+// reference's operation order in the epilogue. No workspace, one launch, C read once (only when
+// beta != 0) and written once.
 #include <climits>
 #include <cuda_runtime.h>
 
