@@ -79,16 +79,17 @@ gemm_batched_simt_kernel(bool transA, bool transB, int m, int n, int k, float al
     float acc[4][4] = {};
 
     for (int k0 = 0; k0 < k; k0 += kGemmBK) {
-        // op(A) tile: rows m0..m0+63, cols k0..k0+15 ; op(B) tile: rows k0.., cols n0..
+        // op(A) tile: rows m0..m0+63, cols k0..k0+15 ; op(B) tile: rows k0.., cols n0.. -- the
+        // fast index follows each operand's contiguous dimension (coalesced loads)
         for (int e = tid; e < kGemmBM * kGemmBK; e += kGemmThreads) {
-            const int i = e % kGemmBM, kk = e / kGemmBM;
+            const int i = transA ? e / kGemmBK : e % kGemmBM, kk = transA ? e % kGemmBK : e / kGemmBM;
             const int gi = m0 + i, gk = k0 + kk;
             float v = 0.0f;
             if (gi < m && gk < k) v = load_elem<TA>(A, transA ? (gk + (long long)gi * lda) : (gi + (long long)gk * lda));
             As[kk][i] = round_operand<R>(v);
         }
         for (int e = tid; e < kGemmBN * kGemmBK; e += kGemmThreads) {
-            const int kk = e % kGemmBK, j = e / kGemmBK;
+            const int kk = transB ? e / kGemmBN : e % kGemmBK, j = transB ? e % kGemmBN : e / kGemmBK;
             const int gj = n0 + j, gk = k0 + kk;
             float v = 0.0f;
             if (gj < n && gk < k) v = load_elem<TB>(B, transB ? (gj + (long long)gk * ldb) : (gk + (long long)gj * ldb));
@@ -108,16 +109,20 @@ gemm_batched_simt_kernel(bool transA, bool transB, int m, int n, int k, float al
         }
         __syncthreads();
     }
+    // The tile goes through shared memory so that C is read and written column by column (each
+    // warp a contiguous run of rows); the per-element epilogue is unchanged.
+    __shared__ float Cs[kGemmBN][kGemmBM + 1];
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int gi = m0 + tx * 4 + i;
-        if (gi >= m) continue;
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int gj = n0 + ty * 4 + j;
-            if (gj >= n) continue;
+        for (int j = 0; j < 4; j++) Cs[ty * 4 + j][tx * 4 + i] = acc[i][j];
+    __syncthreads();
+    for (int e = tid; e < kGemmBM * kGemmBN; e += kGemmThreads) {
+        const int i = e % kGemmBM, j = e / kGemmBM;
+        const int gi = m0 + i, gj = n0 + j;
+        if (gi < m && gj < n) {
             const long long idx = gi + (long long)gj * ldc;
-            float v = alpha * acc[i][j];
+            float v = alpha * Cs[j][i];
             if (beta != 0.0f) v = fmaf(beta, load_elem<TC>(C, idx), v);
             store_elem<TC>(C, idx, v);
         }
