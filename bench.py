@@ -42,6 +42,7 @@ N, BATCH, NRHS = 32, 131072, 4
 E2E_CHUNKS = 16  # e2e leg: chunks of the batch, pipelined over E2E_STREAMS streams
 E2E_STREAMS = 3
 FALLBACK_HBM_GBS = 6650.0
+DATA = "synthetic seeded: A ~ N(0,1), B ~ U(-1,1); fresh input copy per step, inputs (512 MiB) > L2"
 
 # Algorithmic bytes per matrix (reads + writes of each kernel):
 #   getrf  8n^2 + 4n + 12          A read and written, pivots, info, pointer
@@ -139,21 +140,38 @@ class ClockSampler:
                 "reasons": sorted(self.reasons - {"gpu_idle"}), "samples": len(self.samples)}
 
 
-def cpu_reference_rate(n_sample, nthreads=0, reps=1):
-    """Matrices/s of the reference's CPU golden chain (getrf, getrs N nrhs=4, getri) on a
-    sample of n_sample matrices of the workload's distribution; all host threads by default."""
+def chain_inputs(seed, batch=BATCH):
+    """The workload's inputs on the host: A (batch, N, N) i.i.d. N(0,1) and B (batch, NRHS, N) i.i.d.
+    U(-1,1), float32, column-major per matrix, from numpy's PCG64 seeded with `seed`. The GPU arm
+    and the reference arm factor these same bytes."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    a = rng.standard_normal((batch, N, N), dtype=np.float32)
+    b = rng.random((batch, NRHS, N), dtype=np.float32) * np.float32(2) - np.float32(1)
+    return a, b
+
+
+def workload_config(world):
+    """The config object of both arms' JSON lines."""
+    return {"workload": "lu_chain_n32_b131072", "n": N, "lda": N, "batch_per_gpu": BATCH, "nrhs": NRHS,
+            "ops": "getrf+getrs(N)+getri", "parallelism": f"replicas{world}", "seed": "1000 + rank",
+            "l2": "inputs larger than L2"}
+
+
+def cpu_reference_rate(a0, b0, nthreads=0, reps=1):
+    """Matrices/s of the reference's CPU golden chain (getrf, getrs N nrhs=4, getri) over the host
+    matrices a0 / b0 (fresh copies each rep, best of reps); all host threads by default."""
     import numpy as np
 
     sys.path.insert(0, ROOT)
     import oracle as O
 
-    rng = np.random.default_rng(123)
-    a = rng.standard_normal((n_sample, N, N)).astype(np.float32)
-    b = rng.uniform(-1, 1, (n_sample, NRHS, N)).astype(np.float32)
+    n_sample = a0.shape[0]
     best = None
     for _ in range(reps):
-        lu, x = a.copy(), b.copy()
-        c = np.empty_like(a)
+        lu, x = a0.copy(), b0.copy()
+        c = np.empty_like(a0)
         t0 = time.perf_counter()
         piv, _ = O.ref_getrf(lu, N, N, True, nthreads)
         O.ref_getrs("N", lu, N, N, piv, x, NRHS, N, nthreads)
@@ -164,17 +182,17 @@ def cpu_reference_rate(n_sample, nthreads=0, reps=1):
     return n_sample / best, cores, O.ref().ref_openblas_config().decode()
 
 
-def cpu_baseline(target_s=10.0):
-    """The reference golden chain sized to about target_s seconds of host time."""
-    rate, cores, cfg = cpu_reference_rate(2048)
-    sample = int(min(BATCH, max(2048, rate * target_s)))
-    rate, cores, cfg = cpu_reference_rate(sample)
+def cpu_baseline(a0, b0, reps=3):
+    """The reference golden chain on the workload's own host inputs (the whole batch), best of reps."""
+    rate, cores, cfg = cpu_reference_rate(a0, b0, reps=reps)
     return {"value": rate, "unit": "matrices/s", "cores": cores, "kind": "reference",
-            "sample": f"{sample} of the {BATCH} n=32 matrices (same distribution), getrf+getrs(nrhs=4)+getri, "
-                      f"reference golden headers over {cfg}, OpenMP over batch chunks"}
+            "sample": f"the workload's own {a0.shape[0]} n=32 matrices (same bytes as the GPU arm), best of {reps}, "
+                      f"getrf+getrs(nrhs=4)+getri, reference golden headers over {cfg}, OpenMP over batch chunks"}
 
 
 def run_reference_arm(args, rank):
+    """The reference's CPU golden path timed on the workload itself: every step factors fresh copies
+    of the same 131072 matrices the GPU arm factors (same generator and seed), all host threads."""
     if rank != 0:
         return None
     sys.path.insert(0, ROOT)
@@ -184,25 +202,24 @@ def run_reference_arm(args, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/librefgold.so (the reference's CPU "
                                                                "golden path) was not built on this machine"}))
         return None
-    rate, cores, cfg = cpu_reference_rate(2048)
-    sample = int(min(BATCH, max(1024, rate * 2.0)))  # about 2 s per step
+    a0, b0 = chain_inputs(1000 + rank)
     for _ in range(args.warmup):
-        cpu_reference_rate(sample)
+        cpu_reference_rate(a0, b0)
     times = []
+    cores, cfg = 0, ""
     for _ in range(args.steps):
-        r, cores, cfg = cpu_reference_rate(sample)
-        times.append(sample / r)
+        r, cores, cfg = cpu_reference_rate(a0, b0)
+        times.append(BATCH / r)
     total = sum(times)
-    value = sample * args.steps / total
+    value = BATCH * args.steps / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic seeded: A ~ N(0,1), B ~ U(-1,1)",
-        "config": {"workload": "lu_chain_n32_b131072", "n": N, "batch": BATCH, "nrhs": NRHS,
-                   "ops": "getrf+getrs(N)+getri", "step_sample": sample},
+        "data": DATA,
+        "config": workload_config(args.gpus),
         "cpu_baseline": {"value": value, "unit": "matrices/s", "cores": cores, "kind": "reference",
-                         "sample": f"{sample} matrices per step, reference golden headers over {cfg}"},
+                         "sample": f"all {BATCH} matrices per step, reference golden headers over {cfg}"},
         "e2e": {"value": value, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -548,6 +565,30 @@ def section_cgemm(ob, h, dev, reps=5, batch=16384):
     return out
 
 
+def section_chain(ob, h, dev, peak, reps=5, batch=BATCH):
+    """The headline chain (getrf -> getrs nrhs 4 -> getri at n = 32) on `batch` matrices, each kernel
+    timed on its own over fresh input copies; --small runs 32768 matrices (128 MiB, still larger
+    than L2) for profiling captures."""
+    import torch
+
+    a, b = chain_inputs(1000, batch)
+    A0, B0 = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    A, B, Cinv = torch.empty_like(A0), torch.empty_like(B0), torch.empty_like(A0)
+    pa, pb, pc = ob.ptr_array(A), ob.ptr_array(B), ob.ptr_array(Cinv)
+    piv = torch.empty((batch, N), dtype=torch.int32, device=dev)
+    info = torch.empty(batch, dtype=torch.int32, device=dev)
+    rinfo = torch.empty(batch, dtype=torch.int32, device=dev)
+    prep = lambda: (A.copy_(A0), B.copy_(B0))
+    t_f = _events_ms(lambda: h.getrf(A, N, N, piv=piv, info=info, aptr=pa), reps, prep)
+    t_s = _events_ms(lambda: h.getrs("N", A, N, N, piv, B, NRHS, N, aptr=pa, bptr=pb), reps, lambda: B.copy_(B0))
+    t_i = _events_ms(lambda: h.getri(A, N, N, piv, Cinv, N, info=rinfo, aptr=pa, cptr=pc), reps)
+    out = {"workload": f"lu_chain_n32_b{batch}"}
+    for k, t in (("getrf", t_f), ("getrs", t_s), ("getri", t_i)):
+        gbs = ALG_BYTES[k] * batch / (t * 1e-3) / 1e9
+        out[k] = {"ms": t, "GB_s": gbs, "frac_hbm": gbs / peak}
+    return out
+
+
 def run_section(args):
     """One measured section on its own (used for profiling captures with --small)."""
     import torch
@@ -556,7 +597,9 @@ def run_section(args):
     ob = load_package()
     h = ob.Handle()
     peak, _ = peaks()
-    if args.section == "grouped":
+    if args.section == "chain":
+        out = section_chain(ob, h, dev, peak, reps=2 if args.small else 5, batch=32768 if args.small else BATCH)
+    elif args.section == "grouped":
         out = section_grouped(ob, h, dev, peak, reps=2, instances=5000 if args.small else 50000)
     elif args.section == "mixed":
         out = section_mixed(ob, h, dev, reps=2, sizes=((256, 148), (512, 32)) if args.small else ((256, 2048), (512, 256)))
@@ -574,6 +617,36 @@ def run_section(args):
     h.close()
 
 
+def _r(x, d=4):
+    """x rounded to d significant digits (compact JSON)."""
+    return None if x is None else float(f"{x:.{d}g}")
+
+
+def metric_summary(kern, sections):
+    """The metric's own ratios (grouped and mixed + refinement against the plain FP32 path, with the
+    FP64 backward errors of both arms) and the headline kernel's HBM fraction, compact, as the last
+    key of the JSON line."""
+    out = {"getrf_frac_hbm": _r(kern["getrf"]["frac_hbm"], 3)}
+    g = sections.get("grouped")
+    if g:
+        out["grouped"] = {"speedup_vs_plain": _r(g["speedup_vs_plain"]),
+                          "graph_speedup_vs_plain": _r(g["ms"]["plain"] / g["ms"]["grouped_graph"]),
+                          "matrices_s": _r(g["grouped_matrices_s"]), "plain_matrices_s": _r(g["plain_matrices_s"]),
+                          "frac_hbm": _r(g["roofline"]["frac"], 3)}
+    m = sections.get("mixed_refine") or {}
+    for key, v in m.items():
+        n = key.split("_")[0]
+        e = {"plain_berr": _r(v["plain"]["berr_max"], 3), "plain_matrices_s": _r(v["plain"]["matrices_s"])}
+        for p in ("tf32", "bf16"):
+            if p in v:
+                e[p] = {"vs_plain": _r(v[p]["vs_plain"]), "berr": _r(v[p]["berr_max"], 3), "iters": v[p]["iters_max"]}
+        out[f"mixed_{n}"] = e
+    a = sections.get("adjoint")
+    if a:
+        out["adjoint_fwd_bwd_matrices_s"] = _r(a["fwd_bwd_matrices_s"])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -583,7 +656,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sections", action="store_true", help="skip the section measurements (grouped, mixed, adjoint, matinv, geqrf, gels, cgemm)")
-    ap.add_argument("--section", choices=["grouped", "mixed", "adjoint", "matinv", "geqrf", "gels", "cgemm"],
+    ap.add_argument("--section", choices=["chain", "grouped", "mixed", "adjoint", "matinv", "geqrf", "gels", "cgemm"],
                     help="run only this measured section (one JSON line) and exit")
     ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
     args = ap.parse_args()
@@ -616,9 +689,13 @@ def main():
     stream = torch.cuda.current_stream()
 
     nbuf = args.warmup + args.steps
-    g = torch.Generator(device=dev).manual_seed(1000 + rank)
-    A0 = [torch.randn((BATCH, N, N), device=dev, generator=g) for _ in range(nbuf)]
-    B0 = [torch.rand((BATCH, NRHS, N), device=dev, generator=g) * 2 - 1 for _ in range(nbuf)]
+    a_host, b_host = chain_inputs(1000 + rank)
+    A_first = torch.from_numpy(a_host).to(dev)
+    B_first = torch.from_numpy(b_host).to(dev)
+    # one fresh device copy of the inputs per step (getrf and getrs work in place)
+    A0 = [A_first.clone() for _ in range(nbuf)]
+    B0 = [B_first.clone() for _ in range(nbuf)]
+    del A_first, B_first
     aptr = [ob.ptr_array(a) for a in A0]
     bptr = [ob.ptr_array(b) for b in B0]
     Cinv = torch.empty((BATCH, N, N), device=dev)
@@ -670,8 +747,8 @@ def main():
     # e2e through the C ABI from pinned host memory
     hostA = torch.empty((BATCH, N, N), dtype=torch.float32).pin_memory()
     hostB = torch.empty((BATCH, NRHS, N), dtype=torch.float32).pin_memory()
-    hostA.copy_(A0[0].cpu())
-    hostB.copy_(B0[0].cpu())
+    hostA.copy_(torch.from_numpy(a_host))
+    hostB.copy_(torch.from_numpy(b_host))
     hostX = torch.empty_like(hostB).pin_memory()
     hostC = torch.empty_like(hostA).pin_memory()
     hostI = torch.empty(BATCH, dtype=torch.int32).pin_memory()
@@ -749,9 +826,8 @@ def main():
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32",
-            "data": "synthetic seeded: A ~ N(0,1), B ~ U(-1,1); fresh input copy per step, inputs (512 MiB) > L2",
-            "config": {"workload": "lu_chain_n32_b131072", "n": N, "lda": N, "batch_per_gpu": BATCH, "nrhs": NRHS,
-                       "ops": "getrf+getrs(N)+getri", "parallelism": f"replicas{world}", "l2": "inputs larger than L2"},
+            "data": DATA,
+            "config": workload_config(world),
             "kernels": kern,
             "roofline": {"kernel": dom, "bound": "hbm", "achieved": kern[dom]["GB_s"], "peak": peak,
                          "unit": "GB/s", "frac": kern[dom]["frac_hbm"], "peak_source": peak_kind,
@@ -762,16 +838,19 @@ def main():
             "gpu_launches": 3 * args.steps,
             "clocks": clocks.summary(),
         }
-        if world == 1 and not args.no_sections:
-            line["sections"] = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
-                                "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak),
-                                "geqrf": section_geqrf(ob, h, dev, peak), "gels": section_gels(ob, h, dev, peak),
-                                "cgemm": section_cgemm(ob, h, dev)}
         if world == 1 and not args.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_baseline()
+                line["cpu_baseline"] = cpu_baseline(a_host, b_host)
             except Exception as e:  # the baseline is reported, never required
                 line["cpu_baseline"] = {"value": None, "unavailable": str(e)[:200]}
+        if world == 1 and not args.no_sections:
+            sections = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
+                        "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak),
+                        "geqrf": section_geqrf(ob, h, dev, peak), "gels": section_gels(ob, h, dev, peak),
+                        "cgemm": section_cgemm(ob, h, dev)}
+            # the full sections on a line of their own (not JSON: the JSON line below stays the only one)
+            print("sections " + json.dumps(sections))
+            line["metric_summary"] = metric_summary(kern, sections)
         print(json.dumps(line))
     h.close()
     if dist:

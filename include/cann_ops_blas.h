@@ -224,7 +224,8 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
  * needs (n*nrhs*4 rounded up to 256 + 20) * batchCount + 512 bytes of it, and a larger request
  * returns ACLBLAS_STATUS_INVALID_VALUE without launching anything. The first call on each device
  * (with the handle's device current) sets up the scratch address; make it before any stream
- * capture. The scratch is shared by all handles and streams of the process: calls that overlap
+ * capture. The address is kept for the life of the process, so the entry point must not be used
+ * on a device after a cudaDeviceReset of that device. The scratch is shared by all handles and streams of the process: calls that overlap
  * in time on one device race on it; calls one after another on one stream are safe. Arguments,
  * results and status codes are otherwise those of aclblasSgetrfsRefineBatchedEx. */
 ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(

@@ -405,14 +405,8 @@ extern "C" aclblasStatus_t aclblasSgelsBatched(aclblasHandle_t handle, aclblasOp
                   kGelsMaxSmem / 4, lda, n);
         return ACLBLAS_STATUS_NOT_SUPPORTED;
     }
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(gels_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGelsMaxSmem);
-        if (e != cudaSuccess) return launch_status(kApi, e);
-        configured_device = dev;
-    }
+    const cudaError_t e = ensure_smem_limit(gels_kernel, (int)kGelsMaxSmem);
+    if (e != cudaSuccess) return launch_status(kApi, e);
     gels_kernel<<<(unsigned)batchSize, kGelsThreads, smem, handle->stream>>>(t, m, n, nrhs, Aarray, lda, Carray, ldc,
                                                                              devInfo);
     return launch_status(kApi, cudaGetLastError());

@@ -150,15 +150,8 @@ cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int
                            int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split)
 {
     if (m <= 0 || n <= 0 || batch <= 0) return cudaSuccess;
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)gemm_tc_smem_bytes());
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    const cudaError_t e = ensure_smem_limit(gemm_tc_kernel, (int)gemm_tc_smem_bytes());
+    if (e != cudaSuccess) return e;
     const int tm = (m + kTcTile - 1) / kTcTile, tn = (n + kTcTile - 1) / kTcTile;
     const long long blocks = (long long)tm * tn * batch;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;

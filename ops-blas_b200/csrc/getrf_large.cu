@@ -247,13 +247,10 @@ bool getrf_large_supported(int n) { return n > 32 && n <= kLgMaxN; }
 cudaError_t getrf_large_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int batch)
 {
     const LgLayout L(n);
-    static bool configured = false;
-    if (!configured) {
-        const int big = (int)LgLayout(kLgMaxN).bytes;
-        cudaFuncSetAttribute(getrf_large_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        cudaFuncSetAttribute(getrf_large_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-        configured = true;
-    }
+    const int big = (int)LgLayout(kLgMaxN).bytes;
+    const cudaError_t e = piv == nullptr ? ensure_smem_limit(getrf_large_kernel<false>, big)
+                                         : ensure_smem_limit(getrf_large_kernel<true>, big);
+    if (e != cudaSuccess) return e;
     const unsigned grid = (unsigned)batch;
     if (piv == nullptr)
         getrf_large_kernel<false><<<grid, kLgThreads, L.bytes, st>>>(Aarray, n, lda, nullptr, info);

@@ -395,18 +395,9 @@ bool getrf_tmem_supported(int n) { return n > 32 && n <= kTmMaxN; }
 cudaError_t getrf_tmem_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
                               int ldlu, int* piv, int* info, int batch, int prec)
 {
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(getrf_tmem_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)sizeof(TmSmem));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(getrf_tmem_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(TmSmem));
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    const cudaError_t e = prec == 2 ? ensure_smem_limit(getrf_tmem_kernel<2>, (int)sizeof(TmSmem))
+                                    : ensure_smem_limit(getrf_tmem_kernel<1>, (int)sizeof(TmSmem));
+    if (e != cudaSuccess) return e;
     if (prec == 2)
         getrf_tmem_kernel<2><<<(unsigned)batch, kTmThreads, sizeof(TmSmem), st>>>(Aarray, lda, LUarray, n, ldlu, piv,
                                                                                  info);

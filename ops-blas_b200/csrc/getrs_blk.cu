@@ -222,14 +222,8 @@ bool getrs_blk_supported(int n) { return n > 32 && getrs_blk_smem(n) <= 200 * 10
 cudaError_t getrs_blk_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda, const int* ipiv,
                              float* const* Barray, int ldb, int batch)
 {
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e = cudaFuncSetAttribute(getrs_blk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    const cudaError_t e = ensure_smem_limit(getrs_blk_kernel, 200 * 1024);
+    if (e != cudaSuccess) return e;
     getrs_blk_kernel<<<(unsigned)batch, kBsThreads, getrs_blk_smem(n), st>>>(Aarray, n, lda, ipiv, Barray, ldb, nrhs);
     return cudaGetLastError();
 }

@@ -159,15 +159,8 @@ template <bool TR>
 static cudaError_t thread_rhs_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda,
                                      const int* ipiv, float* const* Barray, int ldb, int batch)
 {
-    static int configured_device = -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (configured_device != dev) {
-        cudaError_t e =
-            cudaFuncSetAttribute(getrs_trhs_kernel<TR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        if (e != cudaSuccess) return e;
-        configured_device = dev;
-    }
+    const cudaError_t e = ensure_smem_limit(getrs_trhs_kernel<TR>, 200 * 1024);
+    if (e != cudaSuccess) return e;
     const long long chains = (long long)batch * nrhs;
     const long long blocks = (chains + kTrThreads - 1) / kTrThreads;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;

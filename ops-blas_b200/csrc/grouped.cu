@@ -482,8 +482,7 @@ extern "C" aclblasStatus_t aclblasSgetrfGetrsGroupedPlanCreate(aclblasHandle_t h
         if (err == cudaSuccess && !warp.empty())
             err = cudaMemcpy(p->d_warp, warp.data(), warp.size() * sizeof(GroupTask), cudaMemcpyHostToDevice);
         if (err == cudaSuccess)
-            err = cudaFuncSetAttribute(grouped_lu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)std::max<size_t>(p->smem, 1));
+            err = ensure_smem_limit(grouped_lu_kernel, (int)std::max<size_t>(p->smem, 1));
         int per_sm = 0;
         if (err == cudaSuccess)
             err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_lu_kernel, kGrpThreads, p->smem);

@@ -4,8 +4,10 @@
 // blas/common/helper/aclblas_logger_manager.cpp:19-48 of the reference, over CUDA.
 #include <cstdarg>
 #include <cstdio>
+#include <map>
 #include <mutex>
 #include <new>
+#include <utility>
 
 #include "internal.h"
 
@@ -77,6 +79,21 @@ int sm_count()
         cache[dev] = v;
     }
     return cache[dev];
+}
+
+cudaError_t ensure_smem_limit(const void* func, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> done;  // (device, kernel) -> limit set there
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = done.find({dev, func});
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    err = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (err == cudaSuccess) done[{dev, func}] = bytes;
+    return err;
 }
 
 aclblasStatus_t launch_status(const char* api, cudaError_t err)

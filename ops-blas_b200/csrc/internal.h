@@ -35,6 +35,18 @@ void log_info(const char* api, const char* fmt, ...) __attribute__((format(print
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on the current device. The
+// attribute is per device, so the set-up is remembered per (device, kernel) under a lock; the
+// result of cudaFuncSetAttribute is returned (a cached success afterwards). The record does not
+// survive a cudaDeviceReset of that device: the library must not be used across one.
+cudaError_t ensure_smem_limit(const void* func, int bytes);
+
+template <typename K>
+inline cudaError_t ensure_smem_limit(K* kernel, int bytes)
+{
+    return ensure_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
+}
+
 // Maps the error of a kernel launch to a status and logs it. SUCCESS when err == cudaSuccess.
 aclblasStatus_t launch_status(const char* api, cudaError_t err);
 

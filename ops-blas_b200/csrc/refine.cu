@@ -254,15 +254,12 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     const int rhs_chunk = nrhs < kResMaxRhs ? nrhs : kResMaxRhs;
     (void)rhs_chunk;
     const size_t rsm = (size_t)(n + 8) * kResMaxRhs * 8;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(refine_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        configured = true;
-    }
     if (rsm > 200 * 1024) {
         log_error(kApi, "n=%d exceeds the residual kernel's shared-memory limit", n);
         return ACLBLAS_STATUS_NOT_SUPPORTED;
     }
+    err = ensure_smem_limit(refine_residual_kernel, 200 * 1024);
+    if (err != cudaSuccess) return launch_status(kApi, err);
     for (int it = 0; it < maxIter; it++) {
         refine_residual_kernel<<<(unsigned)batchCount, kResThreads, rsm, st>>>(
             n, nrhs, Aarray, lda, Barray, ldb, Xarray, ldx, dptr, n, dact, tol, it, 0, done, berrArray, iterArray);
@@ -289,7 +286,9 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
 //
 // Set-up: the first call on each device (with that device current) looks up the scratch address
 // with cudaGetSymbolAddress and sets the residual kernel's shared-memory limit; later calls reuse
-// the cached address. Make that first call before any stream capture.
+// the cached address. Make that first call before any stream capture. The cached address does not
+// survive a cudaDeviceReset (the module is reloaded elsewhere): do not use the entry point on a
+// device after resetting it.
 //
 // Only the convergence flags must start at zero; every call clears them on its stream before use,
 // so the scratch may hold anything a previous call left there. There is one scratch array per
@@ -322,7 +321,7 @@ static aclblasStatus_t static_scratch_base(const char* api, int device, char** b
             log_error(api, "cannot resolve the static scratch on device %d: %s", device, cudaGetErrorString(err));
             return launch_status(api, err != cudaSuccess ? err : cudaErrorInvalidSymbol);
         }
-        err = cudaFuncSetAttribute(refine_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        err = ensure_smem_limit(refine_residual_kernel, 200 * 1024);
         if (err != cudaSuccess) return launch_status(api, err);
         g_static_base[device] = static_cast<char*>(p);
     }

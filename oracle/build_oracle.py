@@ -21,7 +21,9 @@ LIB_DIR = os.path.join(HERE, "lib")
 REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_LIB = os.path.join(LIB_DIR, "liboracle.so")
 REF_LIB = os.path.join(REF_DIR, "librefgold.so")
-REFERENCE_ROOT = os.environ.get("OPSBLAS_REFERENCE_ROOT", "/root/reference")
+# The reference tree: OPSBLAS_REFERENCE_ROOT, else a checkout named "reference" beside this repository.
+REFERENCE_ROOT = os.environ.get("OPSBLAS_REFERENCE_ROOT",
+                                os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference")))
 
 
 def _openblas_path() -> str:

@@ -297,13 +297,19 @@ def test_error_rows_with_real_handle(handle, ob):
     """The validation paths behave the same with a live handle."""
     import ctypes as C
 
+    import torch
+
     L = ob.lib()
-    assert L.aclblasSgetrfBatched(handle.h, 5, C.c_void_p(0x1000), 3, None, None, 4) == ob.INVALID_VALUE
+    # small real device buffers: the calls are rejected before they are read, and stay untouched
+    bufs = [torch.zeros(64, dtype=torch.float64, device="cuda") for _ in range(2)]
+    P = [C.c_void_p(t.data_ptr()) for t in bufs]
+    assert L.aclblasSgetrfBatched(handle.h, 5, P[0], 3, None, None, 4) == ob.INVALID_VALUE
     info = C.c_int(0)
     assert L.aclblasSgetrsBatched(handle.h, 999, 4, 1, None, 4, None, None, 4, C.byref(info), 1) == ob.INVALID_ENUM
     assert info.value == -2
-    assert L.aclblasSgetriBatched(handle.h, 4, C.c_void_p(0x1000), 4, None, C.c_void_p(0x1000), 4, None, 1) \
-        == ob.INVALID_VALUE
+    assert L.aclblasSgetriBatched(handle.h, 4, P[0], 4, None, P[1], 4, None, 1) == ob.INVALID_VALUE
+    torch.cuda.synchronize()
+    assert all(float(t.abs().sum()) == 0.0 for t in bufs)
 
 
 def test_handle_stream_and_workspace(ob, cuda):
