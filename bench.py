@@ -589,6 +589,42 @@ def section_chain(ob, h, dev, peak, reps=5, batch=BATCH):
     return out
 
 
+def section_gemm(ob, h, dev, reps=5, batch=2048, size=256):
+    """aclblasGemmBatchedEx on the tcgen05 tensor cores: size^3 per matrix, BF16 -> BF16, FP16 ->
+    FP16 and FP8 E4M3 -> FP16 (FP32 accumulation), plus FP32 with FAST_TF32; alpha = 1, beta = 0.
+    TFLOP/s against the measured cuBLAS BF16 peak (MEASURED_PEAKS.json); torch.bmm of the same
+    shape for context (BF16 / FP16)."""
+    import torch
+
+    m = n = k = size
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            bf16_peak, peak_kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        bf16_peak, peak_kind = 1590.0, "fallback"
+    g = torch.Generator(device=dev).manual_seed(19)
+    out = {"workload": f"gemm_batched_{size}^3_b{batch}", "peak_bf16_TFLOP_s": bf16_peak, "peak_source": peak_kind}
+    flop = 2.0 * m * n * k * batch
+    cases = (("bf16", torch.bfloat16, ob.ACL_BF16, torch.bfloat16, ob.ACL_BF16, ob.COMPUTE_32F),
+             ("f16", torch.float16, ob.ACL_FLOAT16, torch.float16, ob.ACL_FLOAT16, ob.COMPUTE_32F),
+             ("e4m3", torch.float8_e4m3fn, ob.ACL_FLOAT8_E4M3FN, torch.float16, ob.ACL_FLOAT16, ob.COMPUTE_32F),
+             ("tf32", torch.float32, ob.ACL_FLOAT, torch.float32, ob.ACL_FLOAT, ob.COMPUTE_32F_FAST_TF32))
+    for name, tin, ain, tout, aout, comp in cases:
+        A = torch.randn((batch, k, m), device=dev, generator=g).to(tin)
+        B = torch.randn((batch, n, k), device=dev, generator=g).to(tin)
+        Cm = torch.zeros((batch, n, m), device=dev, dtype=tout)
+        pa, pb, pc = ob.ptr_array(A), ob.ptr_array(B), ob.ptr_array(Cm)
+        t = _events_ms(lambda: h.gemm_batched_ex("N", "N", m, n, k, 1.0, A, ain, m, B, ain, k, 0.0, Cm, aout, m,
+                                                 compute=comp, aptr=pa, bptr=pb, cptr=pc), reps)
+        e = {"ms": t, "TFLOP_s": flop / (t * 1e-3) / 1e12, "frac_of_bf16_peak": flop / (t * 1e-3) / 1e12 / bf16_peak}
+        if name in ("bf16", "f16"):
+            D = torch.empty_like(Cm)
+            e["torch_bmm_ms"] = _events_ms(lambda: torch.bmm(B, A, out=D), reps)
+        out[name] = e
+        del A, B, Cm
+    return out
+
+
 def run_section(args):
     """One measured section on its own (used for profiling captures with --small)."""
     import torch
@@ -597,7 +633,9 @@ def run_section(args):
     ob = load_package()
     h = ob.Handle()
     peak, _ = peaks()
-    if args.section == "chain":
+    if args.section == "gemm":
+        out = section_gemm(ob, h, dev, reps=2 if args.small else 5, batch=256 if args.small else 2048)
+    elif args.section == "chain":
         out = section_chain(ob, h, dev, peak, reps=2 if args.small else 5, batch=32768 if args.small else BATCH)
     elif args.section == "grouped":
         out = section_grouped(ob, h, dev, peak, reps=2, instances=5000 if args.small else 50000)
@@ -656,7 +694,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sections", action="store_true", help="skip the section measurements (grouped, mixed, adjoint, matinv, geqrf, gels, cgemm)")
-    ap.add_argument("--section", choices=["chain", "grouped", "mixed", "adjoint", "matinv", "geqrf", "gels", "cgemm"],
+    ap.add_argument("--section", choices=["chain", "gemm", "grouped", "mixed", "adjoint", "matinv", "geqrf", "gels", "cgemm"],
                     help="run only this measured section (one JSON line) and exit")
     ap.add_argument("--small", action="store_true", help="with --section: reduced sizes (profiling captures)")
     args = ap.parse_args()
@@ -847,7 +885,7 @@ def main():
             sections = {"grouped": section_grouped(ob, h, dev, peak), "mixed_refine": section_mixed(ob, h, dev),
                         "adjoint": section_adjoint(ob, h, dev), "matinv": section_matinv(ob, h, dev, peak),
                         "geqrf": section_geqrf(ob, h, dev, peak), "gels": section_gels(ob, h, dev, peak),
-                        "cgemm": section_cgemm(ob, h, dev)}
+                        "cgemm": section_cgemm(ob, h, dev), "gemm": section_gemm(ob, h, dev)}
             # the full sections on a line of their own (not JSON: the JSON line below stays the only one)
             print("sections " + json.dumps(sections))
             line["metric_summary"] = metric_summary(kern, sections)

@@ -71,6 +71,16 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasLoggerConfigure(int logIsOn, int logToStdO
 ACLBLAS_EXPORT aclblasStatus_t aclblasSetLoggerCallback(aclblasLogCallback userCallback);
 ACLBLAS_EXPORT aclblasStatus_t aclblasGetLoggerCallback(aclblasLogCallback* userCallback);
 
+/* Extension (no counterpart in the reference, whose kernels have no waits that can give up).
+ * Every wait inside this library's kernels (on a bulk copy or on tensor-core MMAs) is bounded;
+ * a kernel whose wait gives up stops its work, lets its copies in flight land and sets a bit in
+ * the handle's device status word instead of faulting or hanging. This call synchronises the
+ * handle's stream, returns the bits set since the previous call in *flags and clears them:
+ * bit 0 a getrf bulk copy, bit 1 the mixed-precision TMEM LU, bit 2 the tcgen05 GEMM. It
+ * returns ACLBLAS_STATUS_EXECUTION_FAILED when any bit was set (the results of the calls since
+ * the previous check are then incomplete), else ACLBLAS_STATUS_SUCCESS. */
+ACLBLAS_EXPORT aclblasStatus_t aclblasGetDeviceStatus(aclblasHandle_t handle, unsigned int* flags);
+
 /* ------------------------------------------------------------------ batched LU chain --- */
 
 /* Replaces aclblasSgetrfBatched (include/cann_ops_blas.h:403;

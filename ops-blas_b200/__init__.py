@@ -46,6 +46,7 @@ SIGNATURES = {
     "aclblasLoggerConfigure": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_char_p]),
     "aclblasSetLoggerCallback": (C.c_int, [_vp]),
     "aclblasGetLoggerCallback": (C.c_int, [C.POINTER(_vp)]),
+    "aclblasGetDeviceStatus": (C.c_int, [_vp, C.POINTER(C.c_uint)]),
     "aclblasSgetrfBatched": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int]),
     "aclblasSgetrsBatched": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip,
                                        C.c_int]),
@@ -149,6 +150,13 @@ class Handle:
         s = torch.cuda.current_stream() if stream is None else stream
         check("aclblasSetStream", lib().aclblasSetStream(self.h, _vp(s.cuda_stream)))
         self.stream = s
+
+    def device_status(self):
+        """(status, flags) of aclblasGetDeviceStatus: synchronises the handle's stream, returns
+        the bits that kernels set when a bounded wait gave up (and clears them)."""
+        flags = C.c_uint(0)
+        st = lib().aclblasGetDeviceStatus(self.h, C.byref(flags))
+        return st, flags.value
 
     def close(self):
         if self.h:

@@ -19,8 +19,6 @@
 
 namespace opsblas {
 
-enum class GemmElem { F32, F16, BF16, E4M3, E5M2 };
-
 template <GemmElem T>
 __device__ __forceinline__ float load_elem(const void* p, long long idx)
 {
@@ -264,45 +262,30 @@ extern "C" aclblasStatus_t aclblasGemmBatchedEx(
         return launch_status(kApi, cudaGetLastError());
     }
 
+    // Every dtype of the reference's table runs on the tcgen05 tensor cores with FP32 accumulation
+    // (its cube unit's arithmetic); FP32 operands with COMPUTE_32F_PEDANTIC stay on the FP32
+    // CUDA-core kernel (plain FP32 products).
     cudaError_t err = cudaSuccess;
     using E = GemmElem;
-    using R = OperandRound;
+    auto tc = [&](TcIn ka, TcIn kb, E kc) {
+        return gemm_tc_typed_launch(st, ka, kb, kc, false, ta, tb, m, n, k, a, Aarray, 0, lda, Barray, 0, ldb, b,
+                                    Carray, 0, ldc, batchCount, handle->dstatus);
+    };
     switch (cb) {
-        case Combo::F16_F16_F16:
-            err = run_gemm<E::F16, E::F16, E::F16, R::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                           Carray, ldc, batchCount);
-            break;
-        case Combo::BF16_BF16_BF16:
-            err = run_gemm<E::BF16, E::BF16, E::BF16, R::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                              Carray, ldc, batchCount);
-            break;
-        case Combo::E4M3_E4M3_F16:
-            err = run_gemm<E::E4M3, E::E4M3, E::F16, R::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                             Carray, ldc, batchCount);
-            break;
-        case Combo::E5M2_E5M2_F16:
-            err = run_gemm<E::E5M2, E::E5M2, E::F16, R::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                             Carray, ldc, batchCount);
-            break;
-        case Combo::E4M3_E5M2_F16:
-            err = run_gemm<E::E4M3, E::E5M2, E::F16, R::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                             Carray, ldc, batchCount);
-            break;
-        case Combo::E5M2_E4M3_F16:
-            err = run_gemm<E::E5M2, E::E4M3, E::F16, R::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                             Carray, ldc, batchCount);
-            break;
+        case Combo::F16_F16_F16: err = tc(TcIn::F16, TcIn::F16, E::F16); break;
+        case Combo::BF16_BF16_BF16: err = tc(TcIn::BF16, TcIn::BF16, E::BF16); break;
+        case Combo::E4M3_E4M3_F16: err = tc(TcIn::E4M3, TcIn::E4M3, E::F16); break;
+        case Combo::E5M2_E5M2_F16: err = tc(TcIn::E5M2, TcIn::E5M2, E::F16); break;
+        case Combo::E4M3_E5M2_F16: err = tc(TcIn::E4M3, TcIn::E5M2, E::F16); break;
+        case Combo::E5M2_E4M3_F16: err = tc(TcIn::E5M2, TcIn::E4M3, E::F16); break;
         case Combo::F32_F32_F32:
-            if (computeType == ACLBLAS_COMPUTE_32F_FAST_TF32)  // tcgen05 tensor cores, TF32 operands
-                err = gemm_tc_launch(st, ta, tb, m, n, k, a, reinterpret_cast<const float* const*>(Aarray), 0, lda,
-                                     reinterpret_cast<const float* const*>(Barray), 0, ldb, b,
-                                     reinterpret_cast<float* const*>(Carray), 0, ldc, batchCount, 0);
+            if (computeType == ACLBLAS_COMPUTE_32F_FAST_TF32)
+                err = tc(TcIn::F32_TF32, TcIn::F32_TF32, E::F32);
             else if (computeType == ACLBLAS_COMPUTE_32F_FAST_16BF)
-                err = run_gemm<E::F32, E::F32, E::F32, R::BF16>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                               Carray, ldc, batchCount);
+                err = tc(TcIn::F32_BF16, TcIn::F32_BF16, E::F32);
             else
-                err = run_gemm<E::F32, E::F32, E::F32, R::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray, ldb, b,
-                                                               Carray, ldc, batchCount);
+                err = run_gemm<E::F32, E::F32, E::F32, OperandRound::None>(st, ta, tb, m, n, k, a, Aarray, lda, Barray,
+                                                                          ldb, b, Carray, ldc, batchCount);
             break;
         default:
             return ACLBLAS_STATUS_NOT_SUPPORTED;

@@ -21,11 +21,13 @@ namespace opsblas {
 // ---------------------------------------------------------------------------------------
 // n <= 32: one warp segment per matrix, rows in registers (small_getrf_core, lu_core.cuh).
 // The lane of row r loads it with coalesced column-wise loads and stores it at its final
-// position.
+// position. LD = N compiles the contiguous case (lda == n) with constant strides; with one
+// matrix per warp (n > 16) a warp past the batch leaves at once, so no per-lane validity state
+// is carried through the factorisation.
 // ---------------------------------------------------------------------------------------
-template <int N, bool PIVOT>
+template <int N, bool PIVOT, int LD>
 __global__ void __launch_bounds__(kSmallWarps * 32, N > 16 ? 4 : (N > 8 ? 5 : 6))
-getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__ piv, int* __restrict__ info,
+getrf_small_kernel(float* const* __restrict__ Aarray, int lda_rt, int* __restrict__ piv, int* __restrict__ info,
                    int batch)
 {
     using S = SmallShape<N>;
@@ -37,8 +39,10 @@ getrf_small_kernel(float* const* __restrict__ Aarray, int lda, int* __restrict__
     const int seg = lane / S::SEG;
     const int r = lane % S::SEG;
     const long long m = ((long long)blockIdx.x * kSmallWarps + warp) * S::MPW + seg;
-    const bool mvalid = m < batch;
+    if (S::SEG == 32 && m >= batch) return;  // warp-uniform: the warp's only matrix is past the batch
+    const bool mvalid = S::SEG == 32 ? true : m < batch;
     const bool rvalid = mvalid && r < N;
+    const int lda = LD > 0 ? LD : lda_rt;
 
     // Row r in registers as float4 chunks (contiguous quads: published with one 16-byte store,
     // updated two columns per packed fma); padding entries stay zero.
@@ -190,12 +194,20 @@ extern "C" aclblasStatus_t aclblasSgetrfBatched(
     case NN: {                                                                                                      \
         constexpr int per_cta = kSmallWarps * SmallShape<NN>::MPW;                                                  \
         const unsigned grid = (unsigned)((batchSize + per_cta - 1) / per_cta);                                      \
-        if (pivot)                                                                                                  \
-            getrf_small_kernel<NN, true><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, PivotArray, infoArray,     \
-                                                                            batchSize);                             \
+        constexpr int ld_c = NN > 16 ? NN : 0; /* contiguous variant for one matrix per warp */                      \
+        if (ld_c > 0 && lda == NN) {                                                                                \
+            if (pivot)                                                                                              \
+                getrf_small_kernel<NN, true, ld_c><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, PivotArray,      \
+                                                                                     infoArray, batchSize);         \
+            else                                                                                                    \
+                getrf_small_kernel<NN, false, ld_c><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, nullptr,        \
+                                                                                      infoArray, batchSize);        \
+        } else if (pivot)                                                                                           \
+            getrf_small_kernel<NN, true, 0><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, PivotArray, infoArray,  \
+                                                                               batchSize);                          \
         else                                                                                                        \
-            getrf_small_kernel<NN, false><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, nullptr, infoArray,       \
-                                                                             batchSize);                            \
+            getrf_small_kernel<NN, false, 0><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, nullptr, infoArray,    \
+                                                                                batchSize);                         \
         break;                                                                                                      \
     }
             OPSBLAS_FOR_N_1_32(OPSBLAS_GETRF_CASE)

@@ -18,7 +18,9 @@
 //      the final U12 rows are written to global memory while the MMAs of step 4 run;
 //   4. one thread issues A22 += (-L21) * U12 as tcgen05.mma (kind::tf32, hi*hi + hi*lo + lo*hi)
 //      accumulating straight into the TMEM-resident trailing matrix, and commits to an mbarrier
-//      that the CTA waits on (bounded) before the next panel reads TMEM.
+//      that the CTA waits on (bounded) before the next panel reads TMEM. If that wait gives up,
+//      the CTA waits (bounded) for the MMAs in flight, sets kStatusTmemLuTimeout in the handle's
+//      status word and info = -1, and stops.
 // At the end every row is written to global memory at its final position: the columns left of
 // and inside its pivot panel from TMEM, the rest was written in step 3. HBM traffic is one read
 // and one write of the matrix. Rows that are not below a panel get zero A-operand rows, so the MMA
@@ -39,8 +41,6 @@ constexpr int kTmMaxN = 256;
 constexpr int kTmPB = 32;                // panel width = the MMA's K slice
 constexpr int kTmPart = 128 * kTmPB;     // floats of one 128-row operand part
 constexpr uint32_t kTmWaitLimit = 1u << 24;
-
-__device__ unsigned int g_tmem_lu_timeouts;
 
 struct TmSmem {
     float a_hi[2][kTmPart];  // -L21, rows of block b (physical rows 128b..), K-major UMMA layout
@@ -189,7 +189,7 @@ __device__ __forceinline__ bool tm_panel(float (&p)[kTmPB], int& pos, bool valid
 template <int PREC>
 __global__ void __launch_bounds__(kTmThreads, 1)
 getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* __restrict__ LUarr, int n, int ldlu,
-                  int* __restrict__ piv, int* __restrict__ info)
+                  int* __restrict__ piv, int* __restrict__ info, unsigned* __restrict__ status, unsigned polls)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
     TmSmem& S = *reinterpret_cast<TmSmem*>(smraw);
@@ -356,16 +356,19 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
         // the final U12 rows go to global memory while the tensor cores run (coalesced columns)
         for (int jj = warp; jj < rest; jj += kTmWarps)
             if (lane < nr) LU[(k0 + lane) + (long long)(j0 + jj) * ldlu] = S.u12[lane][jj];
-        const bool waited = mbar_wait_bounded(&S.mbar, phase, kTmWaitLimit);
-        phase ^= 1u;
-        tc_fence_after_sync();
+        const bool waited = mbar_wait_bounded(&S.mbar, phase, polls);
         if (__syncthreads_or(!waited)) {
+            // give up: the MMAs in flight finish first (bounded), the status word reports it
+            mbar_wait_bounded(&S.mbar, phase, kTmWaitLimit);
+            tc_fence_after_sync();
             if (tid == 0) {
-                atomicAdd(&g_tmem_lu_timeouts, 1u);
+                atomicOr(status, kStatusTmemLuTimeout);
                 S.info = -1;
             }
             break;
         }
+        phase ^= 1u;
+        tc_fence_after_sync();
     }
 
     // ---- store: row at its final position; columns right of its pivot panel were written as U12 ----
@@ -393,17 +396,18 @@ getrf_tmem_kernel(const float* const* __restrict__ Ain, int lda, float* const* _
 bool getrf_tmem_supported(int n) { return n > 32 && n <= kTmMaxN; }
 
 cudaError_t getrf_tmem_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
-                              int ldlu, int* piv, int* info, int batch, int prec)
+                              int ldlu, int* piv, int* info, int batch, int prec, unsigned* status)
 {
+    const unsigned polls = wait_limit(kTmWaitLimit);
     const cudaError_t e = prec == 2 ? ensure_smem_limit(getrf_tmem_kernel<2>, (int)sizeof(TmSmem))
                                     : ensure_smem_limit(getrf_tmem_kernel<1>, (int)sizeof(TmSmem));
     if (e != cudaSuccess) return e;
     if (prec == 2)
         getrf_tmem_kernel<2><<<(unsigned)batch, kTmThreads, sizeof(TmSmem), st>>>(Aarray, lda, LUarray, n, ldlu, piv,
-                                                                                 info);
+                                                                                 info, status, polls);
     else
         getrf_tmem_kernel<1><<<(unsigned)batch, kTmThreads, sizeof(TmSmem), st>>>(Aarray, lda, LUarray, n, ldlu, piv,
-                                                                                 info);
+                                                                                 info, status, polls);
     return cudaGetLastError();
 }
 

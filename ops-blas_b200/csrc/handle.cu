@@ -2,6 +2,7 @@
 //
 // Semantics follow blas/common/helper/aclblas_auxiliary.cpp:24-148 and
 // blas/common/helper/aclblas_logger_manager.cpp:19-48 of the reference, over CUDA.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <map>
@@ -81,6 +82,14 @@ int sm_count()
     return cache[dev];
 }
 
+static std::atomic<unsigned> g_wait_limit_override{0xffffffffu};
+
+unsigned wait_limit(unsigned def)
+{
+    const unsigned v = g_wait_limit_override.load(std::memory_order_relaxed);
+    return v == 0xffffffffu ? def : v;
+}
+
 cudaError_t ensure_smem_limit(const void* func, int bytes)
 {
     static std::mutex mu;
@@ -157,6 +166,15 @@ aclblasStatus_t aclblasCreate(aclblasHandle_t* handle)
         log_error("aclblasCreate", "cannot allocate the %zu-byte default workspace", opsblas::kDefaultWorkspaceBytes);
         return st;
     }
+    if (cudaMalloc(&h->dstatus, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(h->dstatus, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        if (h->dstatus) cudaFree(h->dstatus);
+        free_library_workspace(h);
+        delete h;
+        log_error("aclblasCreate", "cannot allocate the device status word");
+        return ACLBLAS_STATUS_ALLOC_FAILED;
+    }
     *handle = h;
     return ACLBLAS_STATUS_SUCCESS;
 }
@@ -169,8 +187,40 @@ aclblasStatus_t aclblasDestroy(aclblasHandle_t handle)
         return ACLBLAS_STATUS_EXECUTION_FAILED;
     }
     free_library_workspace(handle);
+    if (handle->dstatus) cudaFree(handle->dstatus);
     delete handle;
     return ACLBLAS_STATUS_SUCCESS;
+}
+
+aclblasStatus_t aclblasGetDeviceStatus(aclblasHandle_t handle, unsigned int* flags)
+{
+    static const char* kApi = "aclblasGetDeviceStatus";
+    if (handle == nullptr) return ACLBLAS_STATUS_HANDLE_IS_NULLPTR;
+    if (flags == nullptr) {
+        log_error(kApi, "flags must not be nullptr");
+        return ACLBLAS_STATUS_INVALID_VALUE;
+    }
+    unsigned v = 0;
+    cudaError_t err = cudaMemcpyAsync(&v, handle->dstatus, sizeof(v), cudaMemcpyDeviceToHost, handle->stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(handle->dstatus, 0, sizeof(unsigned), handle->stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(handle->stream);
+    if (err != cudaSuccess) {
+        log_error(kApi, "reading the device status failed: %s", cudaGetErrorString(err));
+        return ACLBLAS_STATUS_EXECUTION_FAILED;
+    }
+    *flags = v;
+    if (v != 0) {
+        log_error(kApi, "a kernel gave up a bounded wait (flags 0x%x); its results are incomplete", v);
+        return ACLBLAS_STATUS_EXECUTION_FAILED;
+    }
+    return ACLBLAS_STATUS_SUCCESS;
+}
+
+// Test hook for the failure path (not part of the API): every bounded device wait launched after
+// this call polls at most `polls` times (0 = gives up at once); 0xffffffff restores the defaults.
+__attribute__((visibility("default"))) void opsblas_test_set_wait_limit(unsigned int polls)
+{
+    opsblas::g_wait_limit_override.store(polls, std::memory_order_relaxed);
 }
 
 aclblasStatus_t aclblasSetStream(aclblasHandle_t handle, aclrtStream stream)

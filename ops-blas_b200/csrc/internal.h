@@ -22,6 +22,9 @@ struct _aclblas_handle {
     WorkspaceOwner owner = WorkspaceOwner::Library;
     size_t library_workspace_size = 0;
     int device = 0;
+    // Device status word (4 bytes of device memory owned by the handle): kernels launched through
+    // this handle OR in a kStatus* bit when a bounded wait of theirs gives up.
+    unsigned* dstatus = nullptr;
 };
 
 namespace opsblas {
@@ -31,6 +34,15 @@ constexpr size_t kDefaultWorkspaceBytes = 32u * 1024u * 1024u;
 // Logging through the aclblasLoggerConfigure / aclblasSetLoggerCallback configuration.
 void log_error(const char* api, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
 void log_info(const char* api, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+
+// Bits of the handle's device status word (aclblasGetDeviceStatus).
+constexpr unsigned kStatusBulkCopyTimeout = 1u << 0;  // getrf: a bulk copy of a matrix did not land
+constexpr unsigned kStatusTmemLuTimeout = 1u << 1;    // TMEM LU: the trailing-update MMAs did not complete
+constexpr unsigned kStatusTcGemmTimeout = 1u << 2;    // tcgen05 GEMM: the MMAs of a tile did not complete
+
+// Polls of a bounded device wait: `def`, unless a test has set an override
+// (opsblas_test_set_wait_limit) to make the waits give up.
+unsigned wait_limit(unsigned def);
 
 // Number of SMs of the current device (cached per device).
 int sm_count();
@@ -68,24 +80,38 @@ cudaError_t getrs_trhs_launch(cudaStream_t st, int n, int nrhs, const float* con
 bool getrs_nrhs_preferred(int n, int nrhs, int batch);
 cudaError_t getrs_nrhs_launch(cudaStream_t st, int n, int nrhs, const float* const* Aarray, int lda, const int* ipiv,
                               float* const* Barray, int ldb, int batch);
+// Element types of the batched GEMMs' operands in global memory.
+enum class GemmElem { F32, F16, BF16, E4M3, E5M2 };
+
+// Operand kinds of the tcgen05 GEMM: native FP16 / BF16 / FP8 (E4M3, E5M2), and FP32 operands
+// rounded to TF32 (optionally split into TF32 high and low parts) or converted to BF16.
+enum class TcIn { F16, BF16, E4M3, E5M2, F32_TF32, F32_BF16 };
+
 // C = alpha * op(A) * op(B) + beta * C, FP32 operands; round: 0 none, 1 TF32, 2 BF16.
 cudaError_t gemm_f32_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                             const float* const* A, int lda, const float* const* B, int ldb, float beta,
                             float* const* C, int ldc, int batch, int round);
 
-// gemm_tc.cu: C = alpha * op(A) * op(B) + beta * C on the tcgen05 tensor cores (TF32 operands;
-// split = 1 adds the low-part products for about FP32 accuracy). *_off are element offsets added
-// to every matrix pointer.
+// gemm_tc.cu: C = alpha * op(A) * op(B) + beta * C on the tcgen05 tensor cores, FP32 accumulation.
+// *_off are element offsets added to every matrix pointer; status: the handle's status word.
+// Typed form: A / B of kinds ta / tb (both FP8, or equal), C of type tc (F32 for FP32 operands,
+// F16 for FP16 and FP8, BF16 for BF16).
+cudaError_t gemm_tc_typed_launch(cudaStream_t st, TcIn ta, TcIn tb, GemmElem tc, bool split, bool transA,
+                                 bool transB, int m, int n, int k, float alpha, const void* const* A, long long a_off,
+                                 int lda, const void* const* B, long long b_off, int ldb, float beta, void* const* C,
+                                 long long c_off, int ldc, int batch, unsigned* status);
+// FP32 operands rounded to TF32; split = 1 adds the low-part products for about FP32 accuracy.
 cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                            const float* const* A, long long a_off, int lda, const float* const* B, long long b_off,
-                           int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split);
+                           int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split,
+                           unsigned* status);
 
 // getrf_tmem.cu: 32 < n <= 256, mixed-precision LU with the matrix resident in TMEM.
 bool getrf_tmem_supported(int n);
 // Reads A (lda), writes the factors to LU (ldlu); A may equal LU. prec 1: TF32 split update,
 // 2: BF16 split update.
 cudaError_t getrf_tmem_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
-                              int ldlu, int* piv, int* info, int batch, int prec);
+                              int ldlu, int* piv, int* info, int batch, int prec, unsigned* status);
 
 // getrf_large.cu: 32 < n <= 640, matrix in global memory, the reference's operation order.
 bool getrf_large_supported(int n);

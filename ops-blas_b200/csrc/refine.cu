@@ -242,7 +242,8 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
-        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
+        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode,
+                                handle->dstatus);
     } else {  // plain FP32 factors: the batched getrf's kernels
         aclblasStatus_t s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;
@@ -410,7 +411,8 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
     err = cudaGetLastError();
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
-        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode);
+        err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode,
+                                handle->dstatus);
     } else {  // plain FP32 factors: the batched getrf's kernels
         s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;

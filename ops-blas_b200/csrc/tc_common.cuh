@@ -115,6 +115,51 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t parit
     return false;
 }
 
+// ---- bulk copies (the TMA engine's non-tensor form), completion on an mbarrier / bulk group ----
+
+// The next phase of mbar completes when this thread's arrival and `bytes` of transactions land.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes)
+                 : "memory");
+}
+
+// Global -> shared copy of `bytes` (multiple of 16, both addresses 16-byte aligned), counted on mbar.
+__device__ __forceinline__ void bulk_load(void* smem_dst, const void* gsrc, uint32_t bytes, uint64_t* mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem_dst)),
+                 "l"(gsrc), "r"(bytes), "r"(smem_u32(mbar))
+                 : "memory");
+}
+
+// Shared -> global copy of `bytes` (multiple of 16, both addresses 16-byte aligned) in a bulk group.
+__device__ __forceinline__ void bulk_store(void* gdst, const void* smem_src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(smem_src)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// Until this thread's committed bulk stores have read their shared-memory source.
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
+// Until this thread's committed bulk stores are complete (written to global memory).
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// mbar_wait_bounded that also gives up as soon as *abort (shared, set by another thread of the
+// CTA) is non-zero; checked every 32 polls.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* mbar, uint32_t parity, uint32_t limit, const int* abort)
+{
+    for (uint32_t i = 0; i < limit; i++) {
+        if (mbar_try_wait(mbar, parity)) return true;
+        if ((i & 31u) == 31u && *(const volatile int*)abort) return false;
+    }
+    return false;
+}
+
 // 16 consecutive accumulator columns of this warp's 32 TMEM lanes (lane i of the warp gets row
 // 32 * (warp % 4) + i).
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])

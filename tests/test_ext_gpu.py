@@ -51,6 +51,18 @@ GEMM_CASES = [
     ("T", "T", 129, 257, 33, -2.0, 0.0, "F32", "F32", "F32", 6, 2e-3),
     ("N", "T", 128, 128, 8, 1.0, 1.0, "F32", "F32", "F32", 6, 2e-3),
     ("N", "T", 64, 64, 32, 1.0, 0.0, "F32", "F32", "F32", 5, 2e-2),
+    # tcgen05 pipeline: several K tiles (more than the pipeline's stages), every orientation,
+    # ragged edges, beta != 0 in the C type, and leading dimensions that are not 16-byte multiples
+    # (register path instead of cp.async)
+    ("N", "N", 200, 136, 520, 1.0, 0.0, "F16", "F16", "F16", 2, 4e-3),
+    ("T", "T", 130, 250, 300, 0.75, -0.5, "F16", "F16", "F16", 2, 4e-3),
+    ("T", "N", 256, 256, 256, 1.0, 1.0, "BF16", "BF16", "BF16", 2, 2e-2),
+    ("N", "T", 77, 91, 333, -1.0, 0.25, "BF16", "BF16", "BF16", 2, 2e-2),
+    ("T", "N", 160, 144, 512, 1.0, 0.0, "E4M3", "E4M3", "F16", 2, 4e-3),
+    ("N", "T", 129, 130, 257, 1.0, 0.5, "E5M2", "E4M3", "F16", 2, 4e-3),
+    ("T", "T", 96, 100, 200, 1.0, 0.0, "E4M3", "E5M2", "F16", 2, 4e-3),
+    ("N", "N", 257, 129, 300, 1.0, 0.0, "F32", "F32", "F32", 6, 2e-3),
+    ("T", "T", 140, 70, 130, 1.0, -1.0, "F32", "F32", "F32", 5, 2e-2),
 ]
 DT = {"F32": 0, "F16": 1, "BF16": 27, "E5M2": 35, "E4M3": 36}
 
