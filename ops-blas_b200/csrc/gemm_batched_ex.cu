@@ -269,7 +269,7 @@ extern "C" aclblasStatus_t aclblasGemmBatchedEx(
     using E = GemmElem;
     auto tc = [&](TcIn ka, TcIn kb, E kc) {
         return gemm_tc_typed_launch(st, ka, kb, kc, false, ta, tb, m, n, k, a, Aarray, 0, lda, Barray, 0, ldb, b,
-                                    Carray, 0, ldc, batchCount, handle->dstatus);
+                                    Carray, 0, ldc, batchCount, handle->dstatus, handle->tmslots);
     };
     switch (cb) {
         case Combo::F16_F16_F16: err = tc(TcIn::F16, TcIn::F16, E::F16); break;

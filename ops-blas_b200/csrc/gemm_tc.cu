@@ -3,34 +3,39 @@
 //   C[b] = alpha * op(A[b]) * op(B[b]) + beta * C[b]   (column-major, pointer arrays, element
 //   offsets a_off / b_off / c_off added to every matrix pointer)
 //
-// One CTA per 128 x 128 tile of C, five warps:
+// Persistent: one CTA per SM walks the 128 x 128 tiles of C (matrix by matrix), nine warps:
 //   * warps 0-3 produce: per K tile (128 bytes of K: 64 FP16/BF16, 128 FP8 or 32 TF32 values) they
-//     fill a pipeline stage with op(A) rows m0..m0+127 and op(B)^T rows n0..n0+127 in the
-//     canonical no-swizzle UMMA layout of the operand's own orientation in global memory, so that
-//     every 16-byte run of the source is one 16-byte shared-memory row of a core matrix:
-//       K-major source (K contiguous: A with op T, B with op N): core matrix = 8 MN-rows x 16 B
-//         of K; K-adjacent core matrices 128 B apart (LBO), 8-row groups 1024 B apart (SBO);
-//       MN-major source (A with op N, B with op T): core matrix = 8 K-rows x 16 B of MN;
-//         MN-adjacent core matrices 128 B apart (SBO), 8-row K groups 128 * (16 B groups along
-//         MN) apart (LBO) -- except TF32 operands, which are always staged K-major.
+//     fill a stage of a ring that runs across tile boundaries with op(A) rows m0..m0+127 and
+//     op(B)^T rows n0..n0+127 in the 128-byte swizzled canonical UMMA layout of the operand's
+//     own orientation in global memory (TcLayout below): K-major for a K-contiguous source (A
+//     with op T, B with op N), MN-major for an MN-contiguous one (A with op N, B with op T) --
+//     except TF32 operands, which are always staged K-major.
 //     Native FP16 / BF16 / FP8 operands whose matrix and leading dimension are 16-byte aligned
-//     move by cp.async (16 bytes per copy, zero fill at the edges, no registers held); FP32
-//     operands (rounded to TF32 or BF16, or split into TF32 high and low parts) and unaligned
-//     matrices go through registers. A stage is handed over with an mbarrier (full[s]);
+//     move by cp.async (16 bytes per copy, zero fill at the edges, no registers held), and each
+//     producer thread's cp.async.mbarrier.arrive lets full[s] complete once its copies have
+//     landed, so the producers never wait for their own copies; FP32 operands (rounded to TF32 or
+//     BF16, or split into TF32 high and low parts, 16-byte loads in 4 x 4 blocks) and unaligned
+//     matrices go through registers and a proxy fence before the arrival;
 //   * warp 4 issues the MMAs (one elected thread): per stage four K steps of 32 bytes,
-//     tcgen05.mma kind::f16 / kind::f8f6f4 / kind::tf32 into a 128 x 128 FP32 accumulator in
-//     TMEM (three products hi*hi + hi*lo + lo*hi with SPLIT), then tcgen05.commit frees the stage
-//     (empty[s]) when its MMAs are done; a last commit signals the epilogue;
-//   * warps 0-3 then read their 32 accumulator rows each (tcgen05.ld) and apply alpha / beta to C
-//     in C's type, coalesced along the columns.
-// Every mbarrier wait is bounded. A wait that gives up sets the CTA's abort flag and
-// kStatusTcGemmTimeout in the handle's status word; no further loads or MMAs are issued, the
-// copies and MMAs already in flight are waited for (bounded), C is left as it was and the TMEM is
-// released.
+//     tcgen05.mma kind::f16 / kind::f8f6f4 / kind::tf32 (three products hi*hi + hi*lo + lo*hi
+//     with SPLIT) into one of two 128 x 128 FP32 accumulators in TMEM (256 columns), alternating
+//     per tile; tcgen05.commit frees each stage (empty[s]) and, after a tile's last stage, hands
+//     the accumulator to the epilogue (acc_full[b]);
+//   * warps 5-8 drain the other accumulator meanwhile: each reads its TMEM lane quarter
+//     (tcgen05.ld, 32 rows), releases the accumulator (acc_empty[b]) and applies alpha / beta to
+//     C in C's type, coalesced along the columns.
+// Every mbarrier wait is bounded. A wait that gives up sets the CTA's abort flag (every role then
+// stops) and kStatusTcGemmTimeout in the handle's status word; the copies and MMAs already in
+// flight are waited for (bounded) before the TMEM is released, and the tiles not finished keep
+// their old C.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
+
+#include <mutex>
+#include <type_traits>
 
 #include "internal.h"
 #include "small_common.cuh"
@@ -40,7 +45,8 @@ namespace opsblas {
 
 constexpr int kTcTile = 128;                       // M and N of a CTA tile (one MMA: 128 x 128)
 constexpr int kTcProducers = 128;                  // warps 0-3
-constexpr int kTcThreads = kTcProducers + 32;      // + the MMA warp
+constexpr int kTcEpilogue = 128;                   // warps 5-8
+constexpr int kTcThreads = kTcProducers + 32 + kTcEpilogue;  // + the MMA warp (warp 4)
 constexpr int kTcOperandBytes = kTcTile * 128;     // one operand tile of one stage: 16 KB
 constexpr unsigned kTcWaitPolls = 1u << 24;
 
@@ -85,22 +91,32 @@ __device__ __forceinline__ void umma_issue(uint32_t d, uint64_t a, uint64_t b, u
     }
 }
 
-// Byte offset of 16-byte chunk `c16` (along the contiguous dimension) of line `ln` (the other
-// dimension) in an operand tile, and the descriptor fields, for each source orientation.
-//   K-major:  line = MN row (0..127), chunk = 16 B of K (0..7)
-//   MN-major: line = K index (0..BK-1), chunk = 16 B of MN (0..8*es-1)
+// Operand tiles use the 128-byte swizzled canonical UMMA layouts (1024-byte atoms of 8 lines x
+// 128 bytes, the 16-byte chunk c of line r stored at chunk position c ^ (r % 8)), so that a warp
+// copies four whole 128-byte lines of the source per instruction without bank conflicts.
+//   K-major:  line = MN row (0..127), chunk = 16 B of K (0..7): atoms of 8 rows 1024 B apart
+//             (SBO); a K step of 32 bytes moves the start address by 32 bytes inside the atom;
+//   MN-major: line = K index (0..BK-1), chunk = 16 B of MN (0..8*es-1): 8-row K groups 1024 B
+//             apart (SBO), 128-byte MN atoms (BK / 8) * 1024 B apart (LBO).
 template <int ES>
 struct TcLayout {
-    static constexpr int BK = 128 / ES;                // K values per stage
-    static constexpr int MN_CHUNKS = kTcTile * ES / 16;  // 16-byte groups along MN
-    static constexpr uint32_t MN_LBO = MN_CHUNKS * 128;  // bytes between 8-row K groups
-    __device__ static __forceinline__ uint32_t kmaj(int row, int c16) { return (row >> 3) * 1024 + c16 * 128 + (row & 7) * 16; }
-    __device__ static __forceinline__ uint32_t mnmaj(int k, int c16) { return c16 * 128 + (k >> 3) * MN_LBO + (k & 7) * 16; }
+    static constexpr int BK = 128 / ES;                  // K values per stage
+    static constexpr int MN_CHUNKS = kTcTile * ES / 16;  // 16-byte chunks along MN
+    static constexpr uint32_t MN_LBO = (BK / 8) * 1024;  // bytes between 128-byte MN atoms
+    __device__ static __forceinline__ uint32_t kmaj(int row, int c16)
+    {
+        return (row >> 3) * 1024 + (row & 7) * 128 + ((c16 ^ (row & 7)) << 4);
+    }
+    __device__ static __forceinline__ uint32_t mnmaj(int k, int c16)
+    {
+        return (c16 >> 3) * MN_LBO + (k >> 3) * 1024 + (k & 7) * 128 + (((c16 & 7) ^ (k & 7)) << 4);
+    }
     // descriptor of K step s (32 bytes of K)
     __device__ static __forceinline__ uint64_t desc(uint32_t base, bool mn, int s)
     {
-        return mn ? umma_smem_desc(base + (uint32_t)s * (4 / ES > 0 ? 4 / ES : 1) * MN_LBO, MN_LBO, 128)
-                  : umma_smem_desc(base + (uint32_t)s * 256, 128, 1024);
+        constexpr uint64_t kSw128 = (uint64_t)2 << 61;
+        return mn ? (umma_smem_desc(base + (uint32_t)s * (4 / ES > 0 ? 4 / ES : 1) * 1024, MN_LBO, 1024) | kSw128)
+                  : (umma_smem_desc(base + (uint32_t)s * 32, 16, 1024) | kSw128);
     }
 };
 
@@ -181,12 +197,51 @@ __device__ __forceinline__ void tc_store_c(void* C, long long idx, float v)
     if constexpr (TC == GemmElem::BF16) static_cast<__nv_bfloat16*>(C)[idx] = __float2bfloat16_rn(v);
 }
 
+// C[idx .. idx + n) = a[0 .. n) (+ beta * C) in C's type, n <= 4: with vec (a 16-byte (FP32) or
+// 8-byte (FP16 / BF16) aligned run) and n == 4 one vector load and store, else element by element.
+template <GemmElem TC>
+__device__ __forceinline__ void tc_store_run(void* C, long long idx, const float4& a, float beta, int n, bool vec)
+{
+    const float av[4] = {a.x, a.y, a.z, a.w};
+    if (vec && n == 4) {
+        if constexpr (TC == GemmElem::F32) {
+            float4* p = reinterpret_cast<float4*>(static_cast<float*>(C) + idx);
+            float4 r = a;
+            if (beta != 0.0f) {
+                const float4 c = *p;
+                r = make_float4(fmaf(beta, c.x, a.x), fmaf(beta, c.y, a.y), fmaf(beta, c.z, a.z), fmaf(beta, c.w, a.w));
+            }
+            *p = r;
+        } else {
+            using H = typename std::conditional<TC == GemmElem::F16, __half, __nv_bfloat16>::type;
+            H* p = static_cast<H*>(C) + idx;
+            float r[4] = {av[0], av[1], av[2], av[3]};
+            if (beta != 0.0f) {
+                const uint2 cw = *reinterpret_cast<const uint2*>(p);
+                const H* ch = reinterpret_cast<const H*>(&cw);
+#pragma unroll
+                for (int e = 0; e < 4; e++) r[e] = fmaf(beta, tc_load_c<TC>(ch, e), av[e]);
+            }
+            uint2 ow;
+            H* oh = reinterpret_cast<H*>(&ow);
+#pragma unroll
+            for (int e = 0; e < 4; e++) tc_store_c<TC>(oh, e, r[e]);
+            *reinterpret_cast<uint2*>(p) = ow;
+        }
+        return;
+    }
+    for (int e = 0; e < n && e < 4; e++)
+        tc_store_c<TC>(C, idx + e, beta == 0.0f ? av[e] : fmaf(beta, tc_load_c<TC>(C, idx + e), av[e]));
+}
+
 template <bool SPLIT>
 struct TcStages {
-    static constexpr int S = SPLIT ? 2 : 3;
+    static constexpr int S = SPLIT ? 3 : 4;
     static constexpr int PARTS = SPLIT ? 2 : 1;                     // hi (+ lo)
     static constexpr int STAGE_BYTES = 2 * PARTS * kTcOperandBytes;  // A and B
-    static constexpr size_t SMEM = (size_t)S * STAGE_BYTES + 256;  // + barriers, flags, alignment slack
+    static constexpr int EPI_BYTES = 4 * 32 * 32 * 4;                 // epilogue staging, 4 KB per warp
+    // stages | barriers (0..511) | tensor maps (512..767) | staging (from 1024) | alignment slack
+    static constexpr size_t SMEM = (size_t)S * STAGE_BYTES + 1024 + EPI_BYTES + 1024;
 };
 
 // Fills stage `st` with K tile kt of one operand (rows r0.. of op(X), X's leading dimension ld).
@@ -212,19 +267,24 @@ __device__ __forceinline__ bool tc_fill_operand(uint32_t s_hi, uint32_t s_lo, co
     const bool native = T != TcIn::F32_TF32 && T != TcIn::F32_BF16;
     const bool mn = tc_smem_mn<T>(src_mn);          // shared-memory orientation
     const bool across = src_mn && !mn;              // K-major chunks read across an MN-major source
+    const bool copy = native && vec;
+    uint4 hv[8], lv[8];
+    uint32_t offs[8];
+    // phase 1: every chunk's copy is issued (cp.async) or its elements are loaded into registers
+    // before anything is stored, so that the loads of all chunks are in flight together
 #pragma unroll
     for (int it = 0; it < 8; it++) {
         const int combo = warp * 8 + it;  // 32 combos of (high line, high chunk) over the 4 warps
         int ln, c16;
-        if (!mn) {  // line = row (0..127), chunk along K (0..7): lanes cover 8 rows x 4 chunks
-            ln = (combo >> 1) * 8 + (lane & 7);
-            c16 = (combo & 1) * 4 + (lane >> 3);
-        } else {  // line = k (0..BK-1), chunk along MN (0..MN_CHUNKS-1): lanes cover 8 k x 4 chunks
-            constexpr int CH_HI = L::MN_CHUNKS / 4;
-            ln = (combo / CH_HI) * 8 + (lane & 7);
-            c16 = (combo % CH_HI) * 4 + (lane >> 3);
+        if (!mn) {  // line = row (0..127), chunk along K (0..7): a warp copies 4 whole rows
+            ln = combo * 4 + (lane >> 3);
+            c16 = lane & 7;
+        } else {  // line = k (0..BK-1), chunk along MN: a warp copies one 128-byte atom row of 4 k
+            constexpr int ATOMS = L::MN_CHUNKS / 8;
+            ln = (combo / ATOMS) * 4 + (lane >> 3);
+            c16 = (combo % ATOMS) * 8 + (lane & 7);
         }
-        const uint32_t off = mn ? L::mnmaj(ln, c16) : L::kmaj(ln, c16);
+        offs[it] = mn ? L::mnmaj(ln, c16) : L::kmaj(ln, c16);
         // the chunk's first element: (row, k) of op(X)
         const int row = mn ? r0 + c16 * NE : r0 + ln;
         const int k = mn ? k0 + ln : k0 + c16 * NE;
@@ -232,29 +292,180 @@ __device__ __forceinline__ bool tc_fill_operand(uint32_t s_hi, uint32_t s_lo, co
         const int left = mn ? rows - row : K - k;  // elements left along the chunk's dimension
         const int n = line_ok ? (left < 0 ? 0 : (left > NE ? NE : left)) : 0;
         const long long gidx = src_mn ? (row + (long long)k * ld) : (k + (long long)row * ld);
-        if (native && vec) {
-            cp_async16_zfill(s_hi + off, n > 0 ? (const void*)(X + gidx) : (const void*)X, n * ES);
-        } else {
-            uint4 h, l;
-            tc_chunk_regs<T, SPLIT>(X + (n > 0 ? gidx : 0), across ? ld : 1, n, h, l);
-            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(s_hi + off), "r"(h.x), "r"(h.y), "r"(h.z),
-                         "r"(h.w)
+        if (copy)
+            cp_async16_zfill(s_hi + offs[it], n > 0 ? (const void*)(X + gidx) : (const void*)X, n * ES);
+        else
+            tc_chunk_regs<T, SPLIT>(X + (n > 0 ? gidx : 0), across ? ld : 1, n, hv[it], lv[it]);
+    }
+    // phase 2: register chunks into shared memory
+    if (!copy) {
+#pragma unroll
+        for (int it = 0; it < 8; it++) {
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(s_hi + offs[it]), "r"(hv[it].x),
+                         "r"(hv[it].y), "r"(hv[it].z), "r"(hv[it].w)
                          : "memory");
             if (SPLIT)
-                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(s_lo + off), "r"(l.x), "r"(l.y),
-                             "r"(l.z), "r"(l.w)
+                asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(s_lo + offs[it]), "r"(lv[it].x),
+                             "r"(lv[it].y), "r"(lv[it].z), "r"(lv[it].w)
                              : "memory");
         }
     }
-    return native && vec;
+    return copy;
 }
 
+__device__ __forceinline__ void sts_v4(uint32_t a, uint32_t x, uint32_t y, uint32_t z, uint32_t w)
+{
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(a), "r"(x), "r"(y), "r"(z), "r"(w) : "memory");
+}
+
+__device__ __forceinline__ void sts_v2(uint32_t a, uint32_t x, uint32_t y)
+{
+    asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(a), "r"(x), "r"(y) : "memory");
+}
+
+__device__ __forceinline__ uint32_t bf16x2_bits(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);  // a in the low half (lower address)
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// FP32 operands (TF32 rounding / TF32 high + low split / BF16 conversion): the stage is moved in
+// blocks of 4 rows x 4 K values per thread, read with 16-byte loads along the source's contiguous
+// dimension (transposed in registers when that is MN) and written as 16-byte (TF32) or 8-byte
+// (BF16) shared-memory rows of the operand layout. Blocks that cross the matrix edge, and matrices
+// that are not 16-byte aligned (vec4 false), are read element by element.
+template <TcIn T, bool SPLIT>
+__device__ __forceinline__ void tc_fill_f32(uint32_t s_hi, uint32_t s_lo, const float* X, long long ld, bool src_mn,
+                                            int rows, int K, int r0, int k0, bool vec4, int tid)
+{
+    constexpr int ES = tc_esize(T);  // 4 (TF32) or 2 (BF16)
+    using L = TcLayout<ES>;
+    constexpr int BK = L::BK;
+    constexpr int KB = BK / 4;           // 4-wide K blocks per stage
+    constexpr int NB = (kTcTile / 4) * KB;  // blocks per operand tile
+    const bool smn = tc_smem_mn<T>(src_mn);
+    float v[NB / kTcProducers][4][4];  // [block][row][k]
+#pragma unroll
+    for (int i = 0; i < NB / kTcProducers; i++) {
+        const int bi = tid + i * kTcProducers;
+        // consecutive threads walk the source's contiguous dimension
+        const int rb = src_mn ? bi % (kTcTile / 4) : bi / KB;
+        const int kb = src_mn ? bi / (kTcTile / 4) : bi % KB;
+        const int row = r0 + rb * 4, k = k0 + kb * 4;
+        if (vec4 && row + 3 < rows && k + 3 < K) {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float4 f = src_mn ? *reinterpret_cast<const float4*>(X + row + (long long)(k + j) * ld)
+                                        : *reinterpret_cast<const float4*>(X + k + (long long)(row + j) * ld);
+                const float e[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (src_mn)
+                        v[i][q][j] = e[q];
+                    else
+                        v[i][j][q] = e[q];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++)
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const bool ok = row + rr < rows && k + kk < K;
+                    const long long idx = src_mn ? (row + rr + (long long)(k + kk) * ld) : (k + kk + (long long)(row + rr) * ld);
+                    v[i][rr][kk] = ok ? X[idx] : 0.0f;
+                }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < NB / kTcProducers; i++) {
+        const int bi = tid + i * kTcProducers;
+        const int rb = src_mn ? bi % (kTcTile / 4) : bi / KB;
+        const int kb = src_mn ? bi / (kTcTile / 4) : bi % KB;
+        if constexpr (T == TcIn::F32_TF32) {  // K-major, one 16-byte chunk row per block row
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++) {
+                uint32_t h[4], l[4];
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) {
+                    const float x = v[i][rr][kk];
+                    const float hi = tf32_rne(x);
+                    h[kk] = __float_as_uint(hi);
+                    l[kk] = __float_as_uint(tf32_rne(x - hi));
+                }
+                const uint32_t off = L::kmaj(rb * 4 + rr, kb);
+                sts_v4(s_hi + off, h[0], h[1], h[2], h[3]);
+                if (SPLIT) sts_v4(s_lo + off, l[0], l[1], l[2], l[3]);
+            }
+        } else if (!smn) {  // BF16, K-major: half a chunk row (4 K values) per block row
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++)
+                sts_v2(s_hi + L::kmaj(rb * 4 + rr, kb >> 1) + (kb & 1) * 8, bf16x2_bits(v[i][rr][0], v[i][rr][1]),
+                       bf16x2_bits(v[i][rr][2], v[i][rr][3]));
+        } else {  // BF16, MN-major: half a chunk row (4 MN values) per block K value
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++)
+                sts_v2(s_hi + L::mnmaj(kb * 4 + kk, rb >> 1) + (rb & 1) * 8, bf16x2_bits(v[i][0][kk], v[i][1][kk]),
+                       bf16x2_bits(v[i][2][kk], v[i][3][kk]));
+        }
+    }
+}
+
+// ---- TMA with per-matrix tensor maps ----
+__device__ __forceinline__ void tma_load_2d(uint32_t smem_dst, const CUtensorMap* map, int c0, int c1, uint64_t* mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_dst),
+        "l"(map), "r"(c0), "r"(c1), "r"(smem_u32(mbar))
+        : "memory");
+}
+
+// Points the tensor map held in shared memory at another matrix.
+__device__ __forceinline__ void tmap_replace_address(CUtensorMap* smap, const void* ptr)
+{
+    asm volatile("tensormap.replace.tile.global_address.shared::cta.b1024.b64 [%0], %1;" ::"r"(smem_u32(smap)),
+                 "l"(ptr)
+                 : "memory");
+}
+
+// Copies a tensor map from shared to global memory with the release fence the TMA unit needs
+// (whole warp, converged).
+__device__ __forceinline__ void tmap_publish(CUtensorMap* gmap, const CUtensorMap* smap)
+{
+    asm volatile(
+        "tensormap.cp_fenceproxy.global.shared::cta.tensormap::generic.release.gpu.sync.aligned [%0], [%1], 128;" ::"l"(
+            gmap),
+        "r"(smem_u32(smap))
+        : "memory");
+}
+
+__device__ __forceinline__ void tmap_acquire(const CUtensorMap* gmap)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(gmap) : "memory");
+}
+
+// OR of p over the 128 producer threads (named barrier 1); every producer thread must call it.
+__device__ __forceinline__ bool producers_any(bool p)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred q, o;\n\tsetp.ne.b32 q, %1, 0;\n\tbarrier.red.or.pred o, 1, %2, q;\n\tselp.b32 %0, 1, 0, o;\n\t}"
+        : "=r"(r)
+        : "r"((int)p), "n"(kTcProducers)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kTcProducers) : "memory"); }
+
 template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT>
-__global__ void __launch_bounds__(kTcThreads)
+__global__ void __launch_bounds__(kTcThreads, 1)
 gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__ Aarr, long long a_off, int lda,
                int tA, const void* const* __restrict__ Barr, long long b_off, int ldb, int tB, float beta,
-               void* const* __restrict__ Carr, long long c_off, int ldc, int tiles_m, int tiles_n,
-               unsigned* __restrict__ status, unsigned polls)
+               void* const* __restrict__ Carr, long long c_off, int ldc, int tiles_m, int tiles_n, long long total,
+               unsigned* __restrict__ status, unsigned polls, const __grid_constant__ CUtensorMap tmA,
+               const __grid_constant__ CUtensorMap tmB, CUtensorMap* __restrict__ gslots, int use_tma)
 {
     static_assert(tc_esize(TA) == tc_esize(TB), "A and B share the MMA kind");
     constexpr int ES = tc_esize(TA);
@@ -264,37 +475,41 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
     using SA = typename TcSrc<TA>::type;
     using SB = typename TcSrc<TB>::type;
 
-    // no-swizzle operand layouts need 16-byte alignment only; 128 keeps every tile on its own lines
-    extern __shared__ __align__(128) unsigned char smraw[];
-    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 127) & ~(uintptr_t)127);
+    // swizzled operand tiles start on 1024-byte boundaries (the swizzle pattern's period)
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    unsigned char* sm =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(sm + S * ST::STAGE_BYTES);
     uint64_t* empty = full + S;
-    uint64_t* done = empty + S;
-    uint32_t* taddr_s = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* acc_full = empty + S;
+    uint64_t* acc_empty = acc_full + 2;
+    uint64_t* drain = acc_empty + 2;
+    uint32_t* taddr_s = reinterpret_cast<uint32_t*>(drain + 1);
     int* abort_s = reinterpret_cast<int*>(taddr_s + 1);
+    CUtensorMap* smap = reinterpret_cast<CUtensorMap*>(sm + S * ST::STAGE_BYTES + 512);  // A, B (128-aligned)
+    float* epi = reinterpret_cast<float*>(sm + S * ST::STAGE_BYTES + 1024);             // epilogue staging
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles = tiles_m * tiles_n;
-    const long long bidx = blockIdx.x / tiles;
-    const int tile = blockIdx.x % tiles;
-    const int m0 = (tile % tiles_m) * kTcTile, n0 = (tile / tiles_m) * kTcTile;
-    const SA* A = static_cast<const SA*>(Aarr[bidx]) + a_off;
-    const SB* B = static_cast<const SB*>(Barr[bidx]) + b_off;
     const bool amn = tA == 0;  // op(A) = A: M contiguous
     const bool bmn = tB != 0;  // op(B)^T rows = B's columns when transposed: N contiguous
     const bool amn_s = tc_smem_mn<TA>(amn), bmn_s = tc_smem_mn<TB>(bmn);  // orientation in shared memory
     const int KT = (K + L::BK - 1) / L::BK;
 
     if (warp == 0) {
-        tmem_alloc(taddr_s, kTcTile);
+        tmem_alloc(taddr_s, 2 * kTcTile);
         tmem_relinquish();
     }
     if (tid == 0) {
-        for (int s = 0; s < S; s++) {
-            mbar_init(&full[s], kTcProducers);
-            mbar_init(&empty[s], 1);
+        for (int q = 0; q < S; q++) {
+            mbar_init(&full[q], 1);  // one arrival: the TMA issuer's expect_tx, or producer 0 after a sync
+            mbar_init(&empty[q], 1);
         }
-        mbar_init(done, 1);
+        for (int q = 0; q < 2; q++) {
+            mbar_init(&acc_full[q], 1);
+            mbar_init(&acc_empty[q], kTcEpilogue);
+        }
+        mbar_init(drain, 1);
         *abort_s = 0;
         fence_mbar_init();
     }
@@ -303,140 +518,303 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
     tc_fence_after_sync();
     const uint32_t tacc = *taddr_s;
     const uint32_t sbase = smem_u32(sm);
-    auto a_hi = [&](int s) { return sbase + (uint32_t)(s * ST::STAGE_BYTES); };
-    auto b_hi = [&](int s) { return sbase + (uint32_t)(s * ST::STAGE_BYTES + kTcOperandBytes); };
-    auto a_lo = [&](int s) { return sbase + (uint32_t)(s * ST::STAGE_BYTES + 2 * kTcOperandBytes); };
-    auto b_lo = [&](int s) { return sbase + (uint32_t)(s * ST::STAGE_BYTES + 3 * kTcOperandBytes); };
+    auto a_hi = [&](int q) { return sbase + (uint32_t)(q * ST::STAGE_BYTES); };
+    auto b_hi = [&](int q) { return sbase + (uint32_t)(q * ST::STAGE_BYTES + kTcOperandBytes); };
+    auto a_lo = [&](int q) { return sbase + (uint32_t)(q * ST::STAGE_BYTES + 2 * kTcOperandBytes); };
+    auto b_lo = [&](int q) { return sbase + (uint32_t)(q * ST::STAGE_BYTES + 3 * kTcOperandBytes); };
+    auto aborted = [&]() { return *(volatile int*)abort_s != 0; };
+    auto give_up = [&]() { atomicExch(abort_s, 1); };
 
     if (warp < 4) {
         // ---------------------------------------------------------------- producers
-        const bool avec = (reinterpret_cast<uintptr_t>(A) & 15) == 0 && ((long long)lda * ES) % 16 == 0;
-        const bool bvec = (reinterpret_cast<uintptr_t>(B) & 15) == 0 && ((long long)ldb * ES) % 16 == 0;
-        bool pending = false;  // cp.async group of the previous tile not yet handed over
-        int prev_s = 0;
-        for (int kt = 0; kt < KT; kt++) {
-            const int s = kt % S;
-            if (kt >= S) {
-                const bool ok = mbar_wait_or_abort(&empty[s], (uint32_t)((kt / S - 1) & 1), polls, abort_s);
-                if (!ok) atomicExch(abort_s, 1);
-            }
-            if (*(volatile int*)abort_s) break;
-            const bool ca = tc_fill_operand<TA, SPLIT>(a_hi(s), a_lo(s), A, lda, amn, M, K, m0, kt * L::BK, avec, tid);
-            const bool cb = tc_fill_operand<TB, SPLIT>(b_hi(s), b_lo(s), B, ldb, bmn, N, K, n0, kt * L::BK, bvec, tid);
-            if (ca || cb) {
-                cp_async_commit();
-                if (pending) {  // hand over the previous stage once its copies have landed
-                    cp_async_wait_group<1>();
-                    fence_async_smem();
-                    mbar_arrive(&full[prev_s]);
-                }
-                pending = true;
-                prev_s = s;
-            } else {
-                if (pending) {
-                    cp_async_wait_all();
-                    fence_async_smem();
-                    mbar_arrive(&full[prev_s]);
-                    pending = false;
-                }
-                fence_async_smem();
-                mbar_arrive(&full[s]);
+        CUtensorMap* gA = gslots + 2 * (long long)blockIdx.x;
+        CUtensorMap* gB = gA + 1;
+        if (use_tma && tid == 0) {  // the templates into shared memory, to be pointed at each matrix
+            const uint4* pa = reinterpret_cast<const uint4*>(&tmA);
+            const uint4* pb = reinterpret_cast<const uint4*>(&tmB);
+            uint4* da = reinterpret_cast<uint4*>(&smap[0]);
+            uint4* db = reinterpret_cast<uint4*>(&smap[1]);
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                da[i] = pa[i];
+                db[i] = pb[i];
             }
         }
-        if (pending) {
-            cp_async_wait_all();
-            fence_async_smem();
-            mbar_arrive(&full[prev_s]);
+        long long g = 0;          // K tiles issued by this CTA (the ring position)
+        long long issued = 0;     // K tiles whose loads were actually issued (warp 0 tracks it)
+        long long mapped = -1;    // the matrix the global maps point at
+        for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+            // every producer thread takes the same path through every tile (named barrier 1)
+            if (producers_any(aborted())) break;
+            const long long bidx = t / tiles;
+            const int tile = (int)(t % tiles);
+            const int m0 = (tile % tiles_m) * kTcTile, n0 = (tile / tiles_m) * kTcTile;
+            const SA* A = static_cast<const SA*>(Aarr[bidx]) + a_off;
+            const SB* B = static_cast<const SB*>(Barr[bidx]) + b_off;
+            const bool avec = (reinterpret_cast<uintptr_t>(A) & 15) == 0 && ((long long)lda * ES) % 16 == 0;
+            const bool bvec = (reinterpret_cast<uintptr_t>(B) & 15) == 0 && ((long long)ldb * ES) % 16 == 0;
+            const bool tma = use_tma && avec && bvec;
+            if (tma) {
+                // one thread of warp 0 issues a TMA load per operand (two for 16-bit MN-major A or B)
+                if (warp == 0) {
+                    if (bidx != mapped) {
+                        if (lane == 0) {
+                            tmap_replace_address(&smap[0], A);
+                            tmap_replace_address(&smap[1], B);
+                            // loads still in flight must have read the maps before they change
+                            bulk_commit();
+                            bulk_wait_read_all();
+                        }
+                        __syncwarp();
+                        tmap_publish(gA, &smap[0]);
+                        tmap_publish(gB, &smap[1]);
+                        tmap_acquire(gA);
+                        tmap_acquire(gB);
+                        mapped = bidx;
+                    }
+                    long long gl = g;
+                    for (int kt = 0; kt < KT; kt++, gl++) {
+                        const int q = (int)(gl % S);
+                        bool ok = gl < S || mbar_wait_or_abort(&empty[q], (uint32_t)((gl / S - 1) & 1), polls, abort_s);
+                        ok = __all_sync(0xffffffffu, ok && !aborted());
+                        if (!ok) {
+                            if (lane == 0) give_up();
+                            break;
+                        }
+                        if (lane == 0) {
+                            const int k0 = kt * L::BK;
+                            mbar_arrive_expect_tx(&full[q], 2 * kTcOperandBytes);
+                            if (amn_s) {
+                                for (int a = 0; a < ES; a++)
+                                    tma_load_2d(a_hi(q) + a * L::MN_LBO, gA, m0 + a * (128 / ES), k0, &full[q]);
+                            } else {
+                                tma_load_2d(a_hi(q), gA, k0, m0, &full[q]);
+                            }
+                            if (bmn_s) {
+                                for (int a = 0; a < ES; a++)
+                                    tma_load_2d(b_hi(q) + a * L::MN_LBO, gB, n0 + a * (128 / ES), k0, &full[q]);
+                            } else {
+                                tma_load_2d(b_hi(q), gB, k0, n0, &full[q]);
+                            }
+                        }
+                        __syncwarp();
+                    }
+                    issued = gl;
+                }
+                g += KT;
+                continue;
+            }
+            for (int kt = 0; kt < KT; kt++, g++) {
+                const int q = (int)(g % S);
+                const bool ok = g < S || mbar_wait_or_abort(&empty[q], (uint32_t)((g / S - 1) & 1), polls, abort_s);
+                if (producers_any(!ok || aborted())) {
+                    give_up();
+                    break;
+                }
+                bool ca = false, cb = false;
+                if constexpr (TA == TcIn::F32_TF32 || TA == TcIn::F32_BF16) {
+                    const bool a4 = (reinterpret_cast<uintptr_t>(A) & 15) == 0 && lda % 4 == 0;
+                    const bool b4 = (reinterpret_cast<uintptr_t>(B) & 15) == 0 && ldb % 4 == 0;
+                    tc_fill_f32<TA, SPLIT>(a_hi(q), a_lo(q), reinterpret_cast<const float*>(A), lda, amn, M, K, m0,
+                                           kt * L::BK, a4, tid);
+                    tc_fill_f32<TB, SPLIT>(b_hi(q), b_lo(q), reinterpret_cast<const float*>(B), ldb, bmn, N, K, n0,
+                                           kt * L::BK, b4, tid);
+                } else {
+                    ca = tc_fill_operand<TA, SPLIT>(a_hi(q), a_lo(q), A, lda, amn, M, K, m0, kt * L::BK, avec, tid);
+                    cb = tc_fill_operand<TB, SPLIT>(b_hi(q), b_lo(q), B, ldb, bmn, N, K, n0, kt * L::BK, bvec, tid);
+                }
+                // hand the stage over once every producer's copies and stores are in place
+                if (ca || cb) cp_async_wait_all();
+                fence_async_smem();
+                producers_sync();
+                if (tid == 0) mbar_arrive(&full[q]);
+                issued = g + 1;
+            }
         }
         cp_async_wait_all();  // nothing of this thread is still writing shared memory
-    } else if (lane == 0) {
+        if (use_tma && tid == 0) {
+            // no TMA load may still be writing shared memory when the CTA ends (after a give-up
+            // some stages were never consumed): wait for the last phase of every stage used
+            for (long long gg = issued > S ? issued - S : 0; gg < issued; gg++)
+                mbar_wait_bounded(&full[gg % S], (uint32_t)((gg / S) & 1), kTcWaitPolls);
+        }
+    } else if (warp == 4) {
         // ---------------------------------------------------------------- MMA issue
-        const uint32_t idesc =
-            tc_idesc(tc_format(TA), tc_format(TB), amn_s ? 1u : 0u, bmn_s ? 1u : 0u, kTcTile, kTcTile);
-        for (int kt = 0; kt < KT; kt++) {
-            const int s = kt % S;
-            if (!mbar_wait_or_abort(&full[s], (uint32_t)((kt / S) & 1), polls, abort_s)) {
-                atomicExch(abort_s, 1);
+        if (lane == 0) {
+            const uint32_t idesc =
+                tc_idesc(tc_format(TA), tc_format(TB), amn_s ? 1u : 0u, bmn_s ? 1u : 0u, kTcTile, kTcTile);
+            long long g = 0;
+            long long i = 0;  // local tile count
+            for (long long t = blockIdx.x; t < total; t += gridDim.x, i++) {
+                const int b = (int)(i & 1);
+                if (i >= 2 && !mbar_wait_or_abort(&acc_empty[b], (uint32_t)((i / 2 - 1) & 1), polls, abort_s)) {
+                    give_up();
+                    break;
+                }
+                const uint32_t dacc = tacc + (uint32_t)(b * kTcTile);
+                bool ok = true;
+                for (int kt = 0; kt < KT; kt++, g++) {
+                    const int q = (int)(g % S);
+                    if (!mbar_wait_or_abort(&full[q], (uint32_t)((g / S) & 1), polls, abort_s)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after_sync();
+#pragma unroll
+                    for (int st = 0; st < 4; st++) {
+                        const uint64_t ah = L::desc(a_hi(q), amn_s, st), bh = L::desc(b_hi(q), bmn_s, st);
+                        umma_issue<TA>(dacc, ah, bh, idesc, (kt > 0 || st > 0) ? 1 : 0);
+                        if (SPLIT) {
+                            const uint64_t al = L::desc(a_lo(q), amn_s, st), bl = L::desc(b_lo(q), bmn_s, st);
+                            umma_issue<TA>(dacc, ah, bl, idesc, 1);
+                            umma_issue<TA>(dacc, al, bh, idesc, 1);
+                        }
+                    }
+                    umma_commit(&empty[q]);
+                }
+                if (!ok) {
+                    give_up();
+                    break;
+                }
+                umma_commit(&acc_full[b]);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------------------- epilogue (warps 5-8)
+        const int quarter = warp & 3;  // TMEM lane quarter this warp may read
+        long long i = 0;
+        for (long long t = blockIdx.x; t < total; t += gridDim.x, i++) {
+            const int b = (int)(i & 1);
+            if (!mbar_wait_or_abort(&acc_full[b], (uint32_t)((i / 2) & 1), polls, abort_s)) {
+                give_up();
                 break;
             }
             tc_fence_after_sync();
-#pragma unroll
-            for (int st = 0; st < 4; st++) {
-                const uint64_t ah = L::desc(a_hi(s), amn_s, st), bh = L::desc(b_hi(s), bmn_s, st);
-                umma_issue<TA>(tacc, ah, bh, idesc, (kt > 0 || st > 0) ? 1 : 0);
-                if (SPLIT) {
-                    const uint64_t al = L::desc(a_lo(s), amn_s, st), bl = L::desc(b_lo(s), bmn_s, st);
-                    umma_issue<TA>(tacc, ah, bl, idesc, 1);
-                    umma_issue<TA>(tacc, al, bh, idesc, 1);
+            const long long bidx = t / tiles;
+            const int tile = (int)(t % tiles);
+            const int m0 = (tile % tiles_m) * kTcTile, n0 = (tile / tiles_m) * kTcTile;
+            void* C = static_cast<void*>(static_cast<char*>(Carr[bidx]) + c_off * (TC == GemmElem::F32 ? 4 : 2));
+            const uint32_t row_addr = tacc + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kTcTile);
+            constexpr int CES = TC == GemmElem::F32 ? 4 : 2;
+            const bool cvec = (reinterpret_cast<uintptr_t>(C) & (4 * CES - 1)) == 0 && ((long long)ldc * CES) % (4 * CES) == 0;
+            float* stg = epi + quarter * 32 * 32;  // this warp's 32 columns x 32 rows, column-major
+            for (int c0 = 0; c0 < kTcTile; c0 += 32) {
+                if (n0 + c0 >= N) break;  // uniform
+                float v[32];
+                tmem_ld32(row_addr + (uint32_t)c0, v);
+                if (c0 + 32 >= kTcTile || n0 + c0 + 32 >= N) {
+                    // the accumulator is in registers: the MMA warp may start the next tile here
+                    tc_fence_before_sync();
+                    mbar_arrive(&acc_empty[b]);
                 }
-            }
-            umma_commit(&empty[s]);
-        }
-        umma_commit(done);  // completes when every MMA issued above has
-    }
-    if (warp == 4) __syncwarp();
-
-    // ---------------------------------------------------------------- epilogue (warps 0-3)
-    if (warp < 4) {
-        bool ok = mbar_wait_bounded(done, 0, polls);
-        if (!ok) {
-            atomicExch(abort_s, 1);
-            ok = mbar_wait_bounded(done, 0, kTcWaitPolls);  // the MMAs in flight finish first
-        }
-        tc_fence_after_sync();
-        const bool skip = *(volatile int*)abort_s != 0 || K <= 0;
-        void* C = static_cast<void*>(static_cast<char*>(Carr[bidx]) + c_off * (TC == GemmElem::F32 ? 4 : 2));
-        const int gi = m0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < kTcTile; c0 += 16) {
-            if (n0 + c0 >= N) break;
-            float v[16];
-            tmem_ld16(tacc + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-            if (!skip && gi < M) {
+                // lane = row: stage alpha * D column by column, then every lane writes 4-row runs
+                // of C (coalesced along the columns) with one vector access each
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const int gj = n0 + c0 + j;
-                    if (gj < N) {
-                        const long long idx = gi + (long long)gj * ldc;
-                        const float d = alpha * v[j];
-                        tc_store_c<TC>(C, idx, beta == 0.0f ? d : fmaf(beta, tc_load_c<TC>(C, idx), d));
+                for (int j = 0; j < 32; j++) stg[j * 32 + lane] = alpha * v[j];
+                __syncwarp();
+                if (K > 0) {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const int idx = lane + 32 * i;
+                        const int jj = idx >> 3, rg = idx & 7;
+                        const int gj = n0 + c0 + jj;
+                        const int gr = m0 + quarter * 32 + rg * 4;
+                        if (gj >= N || gr >= M) continue;
+                        const float4 a = *reinterpret_cast<const float4*>(&stg[jj * 32 + rg * 4]);
+                        tc_store_run<TC>(C, gr + (long long)gj * ldc, a, beta, M - gr < 4 ? M - gr : 4, cvec);
                     }
                 }
+                __syncwarp();
             }
         }
     }
-    tc_fence_before_sync();
+
+    // ---------------------------------------------------------------- teardown
+    if (tid == 4 * 32) umma_commit(drain);  // completes once every MMA issued by this CTA has
     __syncthreads();
-    if (tid == 0 && *(volatile int*)abort_s) atomicOr(status, kStatusTcGemmTimeout);
-    if (warp == 0) tmem_dealloc(tacc, kTcTile);
+    if (!mbar_wait_bounded(drain, 0, kTcWaitPolls)) give_up();
+    tc_fence_after_sync();
+    __syncthreads();
+    if (tid == 0 && aborted()) atomicOr(status, kStatusTcGemmTimeout);
+    if (warp == 0) tmem_dealloc(tacc, 2 * kTcTile);
+}
+
+using TmapEncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static TmapEncodeFn tmap_encoder()
+{
+    static TmapEncodeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<TmapEncodeFn>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// Template tensor map of one operand: 2D, 128-byte swizzle, zero fill outside, the box of one TMA
+// load (K-major: BK x 128 rows; MN-major: 128 bytes of MN x BK). The base address is a placeholder
+// that every CTA replaces with the matrix it loads from.
+template <TcIn T>
+static bool tmap_encode(CUtensorMap* map, void* placeholder, bool mn, int rows, int K, int ld)
+{
+    constexpr int ES = tc_esize(T);
+    TmapEncodeFn enc = tmap_encoder();
+    if (enc == nullptr || ((long long)ld * ES) % 16 != 0) return false;
+    const CUtensorMapDataType dt = ES == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+                                           : (T == TcIn::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                              : CU_TENSOR_MAP_DATA_TYPE_FLOAT16);
+    const cuuint64_t dims[2] = {(cuuint64_t)(mn ? rows : K), (cuuint64_t)(mn ? K : rows)};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * ES};
+    const cuuint32_t box[2] = {(cuuint32_t)(mn ? 128 / ES : 128 / ES), (cuuint32_t)(mn ? 128 / ES : kTcTile)};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, dt, 2, placeholder, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT>
 static cudaError_t tc_launch_t(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                                const void* const* A, long long a_off, int lda, const void* const* B, long long b_off,
                                int ldb, float beta, void* const* C, long long c_off, int ldc, int batch,
-                               unsigned* status)
+                               unsigned* status, void* tmslots)
 {
     const size_t smem = TcStages<SPLIT>::SMEM;
     const cudaError_t e = ensure_smem_limit(gemm_tc_kernel<TA, TB, TC, SPLIT>, (int)smem);
     if (e != cudaSuccess) return e;
     const int tm = (m + kTcTile - 1) / kTcTile, tn = (n + kTcTile - 1) / kTcTile;
-    const long long blocks = (long long)tm * tn * batch;
-    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    gemm_tc_kernel<TA, TB, TC, SPLIT><<<(unsigned)blocks, kTcThreads, smem, st>>>(
+    const long long total = (long long)tm * tn * batch;
+    const long long grid = total < sm_count() ? total : sm_count();  // persistent: one CTA per SM
+    CUtensorMap ma{}, mb{};
+    bool use_tma = false;
+    constexpr bool native = TA != TcIn::F32_TF32 && TA != TcIn::F32_BF16;
+    if (native && tmslots != nullptr && grid * 2 * sizeof(CUtensorMap) <= kTensorMapSlotBytes) {
+        // op(A) rows = M (MN-major when A is not transposed); op(B)^T rows = N (MN-major when B is)
+        use_tma = tmap_encode<TA>(&ma, tmslots, !transA, m, k, lda) && tmap_encode<TB>(&mb, tmslots, transB, n, k, ldb);
+    }
+    gemm_tc_kernel<TA, TB, TC, SPLIT><<<(unsigned)grid, kTcThreads, smem, st>>>(
         m, n, k, alpha, A, a_off, lda, transA ? 1 : 0, B, b_off, ldb, transB ? 1 : 0, beta, C, c_off, ldc, tm, tn,
-        status, wait_limit(kTcWaitPolls));
+        total, status, wait_limit(kTcWaitPolls), ma, mb, static_cast<CUtensorMap*>(tmslots), use_tma ? 1 : 0);
     return cudaGetLastError();
 }
 
 cudaError_t gemm_tc_typed_launch(cudaStream_t st, TcIn ta_kind, TcIn tb_kind, GemmElem tc_kind, bool split,
                                  bool transA, bool transB, int m, int n, int k, float alpha, const void* const* A,
                                  long long a_off, int lda, const void* const* B, long long b_off, int ldb, float beta,
-                                 void* const* C, long long c_off, int ldc, int batch, unsigned* status)
+                                 void* const* C, long long c_off, int ldc, int batch, unsigned* status, void* tmslots)
 {
     if (m <= 0 || n <= 0 || batch <= 0) return cudaSuccess;
 #define OPSBLAS_TC(TA_, TB_, TC_, SP_)                                                                               \
     return tc_launch_t<TA_, TB_, TC_, SP_>(st, transA, transB, m, n, k, alpha, A, a_off, lda, B, b_off, ldb, beta, C, \
-                                           c_off, ldc, batch, status)
+                                           c_off, ldc, batch, status, tmslots)
     using E = GemmElem;
     if (ta_kind == TcIn::F32_TF32) {
         if (tc_kind != E::F32) return cudaErrorInvalidValue;
@@ -464,7 +842,7 @@ cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int
     return gemm_tc_typed_launch(st, TcIn::F32_TF32, TcIn::F32_TF32, GemmElem::F32, split != 0, transA, transB, m, n,
                                 k, alpha, reinterpret_cast<const void* const*>(A), a_off, lda,
                                 reinterpret_cast<const void* const*>(B), b_off, ldb, beta,
-                                reinterpret_cast<void* const*>(C), c_off, ldc, batch, status);
+                                reinterpret_cast<void* const*>(C), c_off, ldc, batch, status, nullptr);
 }
 
 }  // namespace opsblas

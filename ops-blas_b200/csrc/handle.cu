@@ -167,12 +167,14 @@ aclblasStatus_t aclblasCreate(aclblasHandle_t* handle)
         return st;
     }
     if (cudaMalloc(&h->dstatus, sizeof(unsigned)) != cudaSuccess ||
-        cudaMemset(h->dstatus, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaMemset(h->dstatus, 0, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&h->tmslots, opsblas::kTensorMapSlotBytes) != cudaSuccess) {
         cudaGetLastError();
         if (h->dstatus) cudaFree(h->dstatus);
+        if (h->tmslots) cudaFree(h->tmslots);
         free_library_workspace(h);
         delete h;
-        log_error("aclblasCreate", "cannot allocate the device status word");
+        log_error("aclblasCreate", "cannot allocate the device status word and tensor-map slots");
         return ACLBLAS_STATUS_ALLOC_FAILED;
     }
     *handle = h;
@@ -188,6 +190,7 @@ aclblasStatus_t aclblasDestroy(aclblasHandle_t handle)
     }
     free_library_workspace(handle);
     if (handle->dstatus) cudaFree(handle->dstatus);
+    if (handle->tmslots) cudaFree(handle->tmslots);
     delete handle;
     return ACLBLAS_STATUS_SUCCESS;
 }

@@ -25,11 +25,15 @@ struct _aclblas_handle {
     // Device status word (4 bytes of device memory owned by the handle): kernels launched through
     // this handle OR in a kStatus* bit when a bounded wait of theirs gives up.
     unsigned* dstatus = nullptr;
+    // Device memory for the tcgen05 GEMM's per-CTA TMA tensor maps (kTensorMapSlotBytes): each
+    // persistent CTA rewrites its maps' base address there when it moves to another matrix.
+    void* tmslots = nullptr;
 };
 
 namespace opsblas {
 
 constexpr size_t kDefaultWorkspaceBytes = 32u * 1024u * 1024u;
+constexpr size_t kTensorMapSlotBytes = 512u * 2u * 128u;  // up to 512 CTAs x (A, B) x 128-byte map
 
 // Logging through the aclblasLoggerConfigure / aclblasSetLoggerCallback configuration.
 void log_error(const char* api, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
@@ -96,10 +100,12 @@ cudaError_t gemm_f32_launch(cudaStream_t st, bool transA, bool transB, int m, in
 // *_off are element offsets added to every matrix pointer; status: the handle's status word.
 // Typed form: A / B of kinds ta / tb (both FP8, or equal), C of type tc (F32 for FP32 operands,
 // F16 for FP16 and FP8, BF16 for BF16).
+// tmslots: the handle's tensor-map slots (native FP16 / BF16 / FP8 operands then arrive by TMA),
+// or nullptr (copies by cp.async).
 cudaError_t gemm_tc_typed_launch(cudaStream_t st, TcIn ta, TcIn tb, GemmElem tc, bool split, bool transA,
                                  bool transB, int m, int n, int k, float alpha, const void* const* A, long long a_off,
                                  int lda, const void* const* B, long long b_off, int ldb, float beta, void* const* C,
-                                 long long c_off, int ldc, int batch, unsigned* status);
+                                 long long c_off, int ldc, int batch, unsigned* status, void* tmslots);
 // FP32 operands rounded to TF32; split = 1 adds the low-part products for about FP32 accuracy.
 cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                            const float* const* A, long long a_off, int lda, const float* const* B, long long b_off,
