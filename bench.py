@@ -610,13 +610,16 @@ def section_gemm(ob, h, dev, reps=5, batch=2048, size=256):
              ("e4m3", torch.float8_e4m3fn, ob.ACL_FLOAT8_E4M3FN, torch.float16, ob.ACL_FLOAT16, ob.COMPUTE_32F),
              ("tf32", torch.float32, ob.ACL_FLOAT, torch.float32, ob.ACL_FLOAT, ob.COMPUTE_32F_FAST_TF32))
     for name, tin, ain, tout, aout, comp in cases:
-        A = torch.randn((batch, k, m), device=dev, generator=g).to(tin)
+        ta_ = "T" if name == "tf32" else "N"  # FP32 operands arrive by TMA when K-contiguous
+        A = torch.randn((batch, k, m), device=dev, generator=g).to(tin)  # m == k: either orientation
         B = torch.randn((batch, n, k), device=dev, generator=g).to(tin)
         Cm = torch.zeros((batch, n, m), device=dev, dtype=tout)
         pa, pb, pc = ob.ptr_array(A), ob.ptr_array(B), ob.ptr_array(Cm)
-        t = _events_ms(lambda: h.gemm_batched_ex("N", "N", m, n, k, 1.0, A, ain, m, B, ain, k, 0.0, Cm, aout, m,
+        t = _events_ms(lambda: h.gemm_batched_ex(ta_, "N", m, n, k, 1.0, A, ain, m, B, ain, k, 0.0, Cm, aout, m,
                                                  compute=comp, aptr=pa, bptr=pb, cptr=pc), reps)
-        e = {"ms": t, "TFLOP_s": flop / (t * 1e-3) / 1e12, "frac_of_bf16_peak": flop / (t * 1e-3) / 1e12 / bf16_peak}
+        e_ = {"op": ta_ + "N"}
+        e = {**e_, "ms": t, "TFLOP_s": flop / (t * 1e-3) / 1e12,
+             "frac_of_bf16_peak": flop / (t * 1e-3) / 1e12 / bf16_peak}
         if name in ("bf16", "f16"):
             D = torch.empty_like(Cm)
             e["torch_bmm_ms"] = _events_ms(lambda: torch.bmm(B, A, out=D), reps)

@@ -216,7 +216,11 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasGemmBatchedEx(
  * matrices whose error is <= tol stop, the others add LU \ r to X. berrArray (double),
  * iterArray (refinement steps used; maxIter if not converged) and infoArray are device arrays.
  * Needs n*nrhs*4 (rounded up to 256) + 20 bytes per matrix (+ 512) of handle workspace
- * (aclblasSetWorkspace); EXECUTION_FAILED if it is smaller. */
+ * (aclblasSetWorkspace); EXECUTION_FAILED if it is smaller. With _FAST_TF32 and 256 < n <= 1024
+ * the factorization is blocked (FP32 panels of 32 columns, split-TF32 tensor-core trailing
+ * updates) when the workspace holds, after that amount rounded up to 256, another P + 16 bytes
+ * per matrix + 512, P = the sum of 2*(n-32)*128, 3*(n-32)*128 and 4*n, each rounded up to 256;
+ * with less, and for _FAST_16BF above n = 256, the factors are plain FP32. */
 ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     aclblasHandle_t handle, int n, int nrhs, const float* const Aarray[], int lda, float* const LUarray[], int ldlu,
     int* PivotArray, const float* const Barray[], int ldb, float* const Xarray[], int ldx,

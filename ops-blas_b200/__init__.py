@@ -227,6 +227,10 @@ class Handle:
         berr = torch.empty(batch, dtype=torch.float64, device=dev)
         iters = torch.empty(batch, dtype=torch.int32, device=dev)
         need = (((n * nrhs * 4 + 255) // 256) * 256 + 20) * batch + 512
+        if 256 < n <= 1024:  # scratch of the blocked tensor-core LU (TF32 mode), after the refinement's part
+            plane = (n - 32) * 32 * 4
+            per = sum((x + 255) // 256 * 256 for x in (2 * plane, 3 * plane, 4 * n))
+            need = (need + 255) // 256 * 256 + per * batch + batch * 16 + 512
         if self._ws is None or self._ws.numel() < need:
             self._ws = torch.empty(max(need, 32 << 20), dtype=torch.uint8, device=dev)
             check("aclblasSetWorkspace", lib().aclblasSetWorkspace(self.h, _vp(self._ws.data_ptr()),

@@ -3,7 +3,9 @@
 //   C[b] = alpha * op(A[b]) * op(B[b]) + beta * C[b]   (column-major, pointer arrays, element
 //   offsets a_off / b_off / c_off added to every matrix pointer)
 //
-// Persistent: one CTA per SM walks the 128 x 128 tiles of C (matrix by matrix), nine warps:
+// Persistent: one CTA per SM walks the 128 x 128 tiles of C (tile t, t + #CTAs, ...: the CTAs
+// work on neighbouring tiles of the same matrices at the same time, which share operands in L2),
+// nine warps:
 //   * warps 0-3 produce: per K tile (128 bytes of K: 64 FP16/BF16, 128 FP8 or 32 TF32 values) they
 //     fill a stage of a ring that runs across tile boundaries with op(A) rows m0..m0+127 and
 //     op(B)^T rows n0..n0+127 in the 128-byte swizzled canonical UMMA layout of the operand's
@@ -197,50 +199,61 @@ __device__ __forceinline__ void tc_store_c(void* C, long long idx, float v)
     if constexpr (TC == GemmElem::BF16) static_cast<__nv_bfloat16*>(C)[idx] = __float2bfloat16_rn(v);
 }
 
-// C[idx .. idx + n) = a[0 .. n) (+ beta * C) in C's type, n <= 4: with vec (a 16-byte (FP32) or
-// 8-byte (FP16 / BF16) aligned run) and n == 4 one vector load and store, else element by element.
+// Four C values of column gj at rows src.x..src.w (n of them exist): one vector load when vec
+// (a 16-byte (FP32) or 8-byte (FP16 / BF16) aligned run of consecutive rows), else one at a time.
 template <GemmElem TC>
-__device__ __forceinline__ void tc_store_run(void* C, long long idx, const float4& a, float beta, int n, bool vec)
+__device__ __forceinline__ float4 tc_load_run(const void* C, int4 src, int gj, int ldc, int n, bool vec)
 {
-    const float av[4] = {a.x, a.y, a.z, a.w};
+    const long long col = (long long)gj * ldc;
     if (vec && n == 4) {
         if constexpr (TC == GemmElem::F32) {
-            float4* p = reinterpret_cast<float4*>(static_cast<float*>(C) + idx);
-            float4 r = a;
-            if (beta != 0.0f) {
-                const float4 c = *p;
-                r = make_float4(fmaf(beta, c.x, a.x), fmaf(beta, c.y, a.y), fmaf(beta, c.z, a.z), fmaf(beta, c.w, a.w));
-            }
-            *p = r;
+            return *reinterpret_cast<const float4*>(static_cast<const float*>(C) + src.x + col);
         } else {
             using H = typename std::conditional<TC == GemmElem::F16, __half, __nv_bfloat16>::type;
-            H* p = static_cast<H*>(C) + idx;
-            float r[4] = {av[0], av[1], av[2], av[3]};
-            if (beta != 0.0f) {
-                const uint2 cw = *reinterpret_cast<const uint2*>(p);
-                const H* ch = reinterpret_cast<const H*>(&cw);
+            const uint2 w = *reinterpret_cast<const uint2*>(static_cast<const H*>(C) + src.x + col);
+            const H* h = reinterpret_cast<const H*>(&w);
+            return make_float4(tc_load_c<TC>(h, 0), tc_load_c<TC>(h, 1), tc_load_c<TC>(h, 2), tc_load_c<TC>(h, 3));
+        }
+    }
+    const int sr[4] = {src.x, src.y, src.z, src.w};
+    float v[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                for (int e = 0; e < 4; e++) r[e] = fmaf(beta, tc_load_c<TC>(ch, e), av[e]);
-            }
+    for (int e = 0; e < 4; e++)
+        if (e < n) v[e] = tc_load_c<TC>(C, sr[e] + col);
+    return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// C[idx .. idx + n) = r[0 .. n) in C's type: one vector store when vec and n == 4.
+template <GemmElem TC>
+__device__ __forceinline__ void tc_store_vals(void* C, long long idx, const float4& r, int n, bool vec)
+{
+    if (vec && n == 4) {
+        if constexpr (TC == GemmElem::F32) {
+            *reinterpret_cast<float4*>(static_cast<float*>(C) + idx) = r;
+        } else {
+            using H = typename std::conditional<TC == GemmElem::F16, __half, __nv_bfloat16>::type;
             uint2 ow;
             H* oh = reinterpret_cast<H*>(&ow);
-#pragma unroll
-            for (int e = 0; e < 4; e++) tc_store_c<TC>(oh, e, r[e]);
-            *reinterpret_cast<uint2*>(p) = ow;
+            tc_store_c<TC>(oh, 0, r.x);
+            tc_store_c<TC>(oh, 1, r.y);
+            tc_store_c<TC>(oh, 2, r.z);
+            tc_store_c<TC>(oh, 3, r.w);
+            *reinterpret_cast<uint2*>(static_cast<H*>(C) + idx) = ow;
         }
         return;
     }
-    for (int e = 0; e < n && e < 4; e++)
-        tc_store_c<TC>(C, idx + e, beta == 0.0f ? av[e] : fmaf(beta, tc_load_c<TC>(C, idx + e), av[e]));
+    const float rv[4] = {r.x, r.y, r.z, r.w};
+    for (int e = 0; e < n && e < 4; e++) tc_store_c<TC>(C, idx + e, rv[e]);
 }
 
 template <bool SPLIT>
 struct TcStages {
-    static constexpr int S = SPLIT ? 3 : 4;
+    static constexpr int S = SPLIT ? 2 : 4;
     static constexpr int PARTS = SPLIT ? 2 : 1;                     // hi (+ lo)
     static constexpr int STAGE_BYTES = 2 * PARTS * kTcOperandBytes;  // A and B
-    static constexpr int EPI_BYTES = 4 * 32 * 32 * 4;                 // epilogue staging, 4 KB per warp
-    // stages | barriers (0..511) | tensor maps (512..767) | staging (from 1024) | alignment slack
+    // epilogue staging: three 128 x 32 FP32 chunks of C (the TMA epilogue), or 4 KB per warp
+    static constexpr int EPI_BYTES = 3 * kTcTile * 32 * 4;
+    // stages | barriers (0..511) | tensor maps (512..895) | staging (from 1024) | alignment slack
     static constexpr size_t SMEM = (size_t)S * STAGE_BYTES + 1024 + EPI_BYTES + 1024;
 };
 
@@ -459,13 +472,61 @@ __device__ __forceinline__ bool producers_any(bool p)
 
 __device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kTcProducers) : "memory"); }
 
+// Shared -> global tile copies of the TMA epilogue (bulk groups of the issuing thread).
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int c0, int c1, uint32_t smem_src)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map),
+                 "r"(c0), "r"(c1), "r"(smem_src)
+                 : "memory");
+}
+
+// Until at most N of this thread's committed bulk stores have not yet read their source.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read_n()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// OR over the four epilogue warps (5-8, named barrier 3) / their barrier.
+__device__ __forceinline__ bool epilogue_any(bool p)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred q, o;\n\tsetp.ne.b32 q, %1, 0;\n\tbarrier.red.or.pred o, 3, %2, q;\n\tselp.b32 %0, 1, 0, o;\n\t}"
+        : "=r"(r)
+        : "r"((int)p), "n"(kTcEpilogue)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void epilogue_sync() { asm volatile("bar.sync 3, %0;" ::"n"(kTcEpilogue) : "memory"); }
+
+// The same over the three converter warps (1-3) of an FP32 TMA tile (named barrier 2).
+__device__ __forceinline__ bool converters_any(bool p)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred q, o;\n\tsetp.ne.b32 q, %1, 0;\n\tbarrier.red.or.pred o, 2, %2, q;\n\tselp.b32 %0, 1, 0, o;\n\t}"
+        : "=r"(r)
+        : "r"((int)p), "n"(kTcProducers - 32)
+        : "memory");
+    return r != 0;
+}
+
+__device__ __forceinline__ void converters_sync()
+{
+    asm volatile("bar.sync 2, %0;" ::"n"(kTcProducers - 32) : "memory");
+}
+
 template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT>
 __global__ void __launch_bounds__(kTcThreads, 1)
 gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__ Aarr, long long a_off, int lda,
                int tA, const void* const* __restrict__ Barr, long long b_off, int ldb, int tB, float beta,
                void* const* __restrict__ Carr, long long c_off, int ldc, int tiles_m, int tiles_n, long long total,
                unsigned* __restrict__ status, unsigned polls, const __grid_constant__ CUtensorMap tmA,
-               const __grid_constant__ CUtensorMap tmB, CUtensorMap* __restrict__ gslots, int use_tma)
+               const __grid_constant__ CUtensorMap tmB, CUtensorMap* __restrict__ gslots, int use_tma,
+               const int* __restrict__ rowsrc, long long rs_stride, int presplit, int a_lo_rows, int b_lo_rows,
+               const __grid_constant__ CUtensorMap tmC, int epi_mode)
 {
     static_assert(tc_esize(TA) == tc_esize(TB), "A and B share the MMA kind");
     constexpr int ES = tc_esize(TA);
@@ -481,12 +542,14 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(sm + S * ST::STAGE_BYTES);
     uint64_t* empty = full + S;
-    uint64_t* acc_full = empty + S;
+    uint64_t* ready = empty + S;  // FP32 operands: the stage converted to TF32 (high and low parts)
+    uint64_t* acc_full = ready + S;
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* drain = acc_empty + 2;
-    uint32_t* taddr_s = reinterpret_cast<uint32_t*>(drain + 1);
+    uint64_t* cload = drain + 1;  // TMA epilogue: the three staging buffers' loads of C
+    uint32_t* taddr_s = reinterpret_cast<uint32_t*>(cload + 3);
     int* abort_s = reinterpret_cast<int*>(taddr_s + 1);
-    CUtensorMap* smap = reinterpret_cast<CUtensorMap*>(sm + S * ST::STAGE_BYTES + 512);  // A, B (128-aligned)
+    CUtensorMap* smap = reinterpret_cast<CUtensorMap*>(sm + S * ST::STAGE_BYTES + 512);  // A, B, C (128-aligned)
     float* epi = reinterpret_cast<float*>(sm + S * ST::STAGE_BYTES + 1024);             // epilogue staging
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -495,6 +558,11 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
     const bool bmn = tB != 0;  // op(B)^T rows = B's columns when transposed: N contiguous
     const bool amn_s = tc_smem_mn<TA>(amn), bmn_s = tc_smem_mn<TB>(bmn);  // orientation in shared memory
     const int KT = (K + L::BK - 1) / L::BK;
+    // FP32 operands arriving by TMA are converted in shared memory (round to TF32, low parts)
+    // before the MMAs: the MMA warp then waits on ready[] instead of full[]
+    // (operands that arrive already split into TF32 high and low planes, presplit, need nothing)
+    const bool CONVERT = TA == TcIn::F32_TF32 && !presplit;
+    uint64_t* hand = CONVERT ? ready : full;
 
     if (warp == 0) {
         tmem_alloc(taddr_s, 2 * kTcTile);
@@ -504,12 +572,14 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
         for (int q = 0; q < S; q++) {
             mbar_init(&full[q], 1);  // one arrival: the TMA issuer's expect_tx, or producer 0 after a sync
             mbar_init(&empty[q], 1);
+            mbar_init(&ready[q], 1);
         }
         for (int q = 0; q < 2; q++) {
             mbar_init(&acc_full[q], 1);
             mbar_init(&acc_empty[q], kTcEpilogue);
         }
         mbar_init(drain, 1);
+        for (int q = 0; q < 3; q++) mbar_init(&cload[q], 1);
         *abort_s = 0;
         fence_mbar_init();
     }
@@ -527,7 +597,7 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
 
     if (warp < 4) {
         // ---------------------------------------------------------------- producers
-        CUtensorMap* gA = gslots + 2 * (long long)blockIdx.x;
+        CUtensorMap* gA = gslots + 3 * (long long)blockIdx.x;
         CUtensorMap* gB = gA + 1;
         if (use_tma && tid == 0) {  // the templates into shared memory, to be pointed at each matrix
             const uint4* pa = reinterpret_cast<const uint4*>(&tmA);
@@ -581,7 +651,14 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                             if (lane == 0) give_up();
                             break;
                         }
-                        if (lane == 0) {
+                        if (lane == 0 && presplit) {  // high and low planes of both operands
+                            const int k0 = kt * L::BK;
+                            mbar_arrive_expect_tx(&full[q], 4 * kTcOperandBytes);
+                            tma_load_2d(a_hi(q), gA, k0, m0, &full[q]);
+                            tma_load_2d(a_lo(q), gA, k0, m0 + a_lo_rows, &full[q]);
+                            tma_load_2d(b_hi(q), gB, k0, n0, &full[q]);
+                            tma_load_2d(b_lo(q), gB, k0, n0 + b_lo_rows, &full[q]);
+                        } else if (lane == 0) {
                             const int k0 = kt * L::BK;
                             mbar_arrive_expect_tx(&full[q], 2 * kTcOperandBytes);
                             if (amn_s) {
@@ -600,6 +677,41 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                         __syncwarp();
                     }
                     issued = gl;
+                } else if (CONVERT && warp > 0) {
+                    // warps 1-3: each landed stage to TF32 in place (round to nearest even), plus
+                    // the low parts x - hi with SPLIT, then hand it to the MMA warp
+                    const int ctid = tid - 32;
+                    long long gl = g;
+                    for (int kt = 0; kt < KT; kt++, gl++) {
+                        const int q = (int)(gl % S);
+                        const bool ok = mbar_wait_or_abort(&full[q], (uint32_t)((gl / S) & 1), polls, abort_s);
+                        if (converters_any(!ok || aborted())) {
+                            if (ctid == 0) give_up();
+                            break;
+                        }
+                        for (int c = ctid; c < 2 * kTcOperandBytes / 16; c += kTcProducers - 32) {
+                            const uint32_t off = (uint32_t)(c % (kTcOperandBytes / 16)) * 16;
+                            const uint32_t hi_a = (c < kTcOperandBytes / 16 ? a_hi(q) : b_hi(q)) + off;
+                            const uint32_t lo_a = (c < kTcOperandBytes / 16 ? a_lo(q) : b_lo(q)) + off;
+                            uint32_t x[4];
+                            asm volatile("ld.shared.v4.b32 {%0, %1, %2, %3}, [%4];"
+                                         : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3])
+                                         : "r"(hi_a));
+                            uint32_t h[4], l[4];
+#pragma unroll
+                            for (int e = 0; e < 4; e++) {
+                                const float f = __uint_as_float(x[e]);
+                                const float hf = tf32_rne(f);
+                                h[e] = __float_as_uint(hf);
+                                l[e] = __float_as_uint(tf32_rne(f - hf));
+                            }
+                            sts_v4(hi_a, h[0], h[1], h[2], h[3]);
+                            if (SPLIT) sts_v4(lo_a, l[0], l[1], l[2], l[3]);
+                        }
+                        fence_async_smem();
+                        converters_sync();
+                        if (ctid == 0) mbar_arrive(&ready[q]);
+                    }
                 }
                 g += KT;
                 continue;
@@ -627,7 +739,7 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                 if (ca || cb) cp_async_wait_all();
                 fence_async_smem();
                 producers_sync();
-                if (tid == 0) mbar_arrive(&full[q]);
+                if (tid == 0) mbar_arrive(&hand[q]);
                 issued = g + 1;
             }
         }
@@ -655,7 +767,7 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                 bool ok = true;
                 for (int kt = 0; kt < KT; kt++, g++) {
                     const int q = (int)(g % S);
-                    if (!mbar_wait_or_abort(&full[q], (uint32_t)((g / S) & 1), polls, abort_s)) {
+                    if (!mbar_wait_or_abort(&hand[q], (uint32_t)((g / S) & 1), polls, abort_s)) {
                         ok = false;
                         break;
                     }
@@ -683,51 +795,227 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
     } else {
         // ---------------------------------------------------------------- epilogue (warps 5-8)
         const int quarter = warp & 3;  // TMEM lane quarter this warp may read
+        float* stg = epi + quarter * 32 * 32;  // this warp's 32 columns x 32 rows, column-major
+        constexpr int CES = TC == GemmElem::F32 ? 4 : 2;
+        CUtensorMap* gC = gslots + 3 * (long long)blockIdx.x + 2;
+        const int issuer = kTcProducers + 32;  // warp 5, lane 0: every TMA store of C
+        long long mapped_c = -1;
+        bool prev_tma = false;
+        long long gch = 0;      // TMA epilogue chunks so far (the staging buffer ring position)
+        uint32_t cphase = 0;    // bit k: the phase to wait for on cload[k]
+        if (epi_mode != 0 && tid == issuer) {
+            const uint4* pc = reinterpret_cast<const uint4*>(&tmC);
+            uint4* dc = reinterpret_cast<uint4*>(&smap[2]);
+#pragma unroll
+            for (int k = 0; k < 8; k++) dc[k] = pc[k];
+        }
         long long i = 0;
         for (long long t = blockIdx.x; t < total; t += gridDim.x, i++) {
             const int b = (int)(i & 1);
-            if (!mbar_wait_or_abort(&acc_full[b], (uint32_t)((i / 2) & 1), polls, abort_s)) {
+            const long long bidx = t / tiles;
+            const int tile = (int)(t % tiles);
+            const int m0 = (tile % tiles_m) * kTcTile, n0 = (tile / tiles_m) * kTcTile;
+            void* C = static_cast<void*>(static_cast<char*>(Carr[bidx]) + c_off * CES);
+            const bool cvec = (reinterpret_cast<uintptr_t>(C) & (4 * CES - 1)) == 0 && ((long long)ldc * CES) % (4 * CES) == 0;
+            const int* rs = rowsrc != nullptr ? rowsrc + bidx * rs_stride : nullptr;
+            const int gi = m0 + quarter * 32 + lane;  // this lane's row
+            if (epi_mode != 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0) {
+                // ---- TMA epilogue in 128 x 32 chunks through three rotating staging buffers:
+                // beta = 0: alpha * D staged and stored by TMA; otherwise the chunk of C is loaded
+                // by TMA (the first one before the accumulator is ready, each next one while the
+                // current one is combined), combined in place (beta * C + alpha * D) and stored.
+                // Rows that the row map takes from other rows read those rows' values directly.
+                if (bidx != mapped_c) {
+                    if (warp == kTcProducers / 32 + 1) {
+                        if (lane == 0) {
+                            tmap_replace_address(&smap[2], C);
+                            bulk_commit();
+                            bulk_wait_read_all();  // earlier stores must have read the old map
+                        }
+                        __syncwarp();
+                        tmap_publish(gC, &smap[2]);
+                        tmap_acquire(gC);
+                    }
+                    mapped_c = bidx;
+                }
+                // a row that the row map takes from another row reads that row's C itself (32
+                // independent loads per chunk, issued before the chunk's waits) in place of the
+                // staged values of its own row
+                int srow = gi;
+                if (epi_mode == 2 && rs != nullptr && gi < M) srow = rs[gi];
+                const bool mv = srow != gi;
+                const int nchunks = (N - n0) < kTcTile ? (N - n0 + 31) / 32 : kTcTile / 32;
+                epilogue_sync();
+                // chunk gcc's load of C into buffer gcc % 3, whose last store was chunk gcc - 3's
+                // (stores are issued up to the current chunk - 1: `lookahead` loads run one ahead)
+                auto load_chunk_tma = [&](long long gcc, int c0, bool lookahead) {  // issuer only
+                    const int bf = (int)(gcc % 3);
+                    if (lookahead)
+                        bulk_wait_read_n<1>();
+                    else
+                        bulk_wait_read_n<2>();
+                    mbar_arrive_expect_tx(&cload[bf], (uint32_t)(kTcTile * 32 * CES));
+                    tma_load_2d(smem_u32(epi) + (uint32_t)(bf * kTcTile * 32 * 4), gC, m0, n0 + c0, &cload[bf]);
+                };
+                // after a give-up: loads of C still in flight land before the CTA ends
+                auto drain_load = [&](long long gcc) {
+                    const int bf = (int)(gcc % 3);
+                    mbar_wait_bounded(&cload[bf], (cphase >> bf) & 1u, kTcWaitPolls);
+                };
+                if (epi_mode == 2 && tid == issuer) load_chunk_tma(gch, 0, false);
+                const bool ok = mbar_wait_or_abort(&acc_full[b], (uint32_t)((i / 2) & 1), polls, abort_s);
+                if (epilogue_any(!ok)) {
+                    if (tid == issuer) {
+                        give_up();
+                        if (epi_mode == 2) drain_load(gch);
+                    }
+                    break;
+                }
+                tc_fence_after_sync();
+                const uint32_t row_addr = tacc + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kTcTile);
+                bool stop = false;
+                for (int c = 0; c < nchunks; c++, gch++) {
+                    const int c0 = c * 32;
+                    const int bf = (int)(gch % 3);
+                    if (epi_mode == 2 && tid == issuer && c + 1 < nchunks) load_chunk_tma(gch + 1, c0 + 32, true);
+                    float cm[32];
+                    if (mv) {
+#pragma unroll
+                        for (int j = 0; j < 32; j++)
+                            cm[j] = n0 + c0 + j < N ? tc_load_c<TC>(C, srow + (long long)(n0 + c0 + j) * ldc) : 0.0f;
+                    }
+                    float v[32];
+                    tmem_ld32(row_addr + (uint32_t)c0, v);
+                    if (c + 1 == nchunks) {
+                        tc_fence_before_sync();
+                        mbar_arrive(&acc_empty[b]);
+                    }
+                    if (epi_mode == 2) {
+                        const bool okc = mbar_wait_or_abort(&cload[bf], (cphase >> bf) & 1u, polls, abort_s);
+                        if (epilogue_any(!okc)) {
+                            if (tid == issuer) {
+                                give_up();
+                                drain_load(gch);
+                                if (c + 1 < nchunks) drain_load(gch + 1);
+                            }
+                            stop = true;
+                            break;
+                        }
+                        cphase ^= 1u << bf;
+                    } else {
+                        if (tid == issuer) bulk_wait_read_n<2>();  // the store of chunk gch - 3 has read it
+                        epilogue_sync();
+                    }
+                    const int row = quarter * 32 + lane;
+                    if constexpr (TC == GemmElem::F32) {
+                        float* buf = epi + bf * kTcTile * 32;
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            float* e = &buf[j * kTcTile + row];
+                            *e = epi_mode == 2 ? fmaf(beta, mv ? cm[j] : *e, alpha * v[j]) : alpha * v[j];
+                        }
+                    } else {
+                        using H = typename std::conditional<TC == GemmElem::F16, __half, __nv_bfloat16>::type;
+                        H* buf = reinterpret_cast<H*>(epi + bf * kTcTile * 32);
+#pragma unroll
+                        for (int j = 0; j < 32; j++) {
+                            const int e = j * kTcTile + row;
+                            tc_store_c<TC>(buf, e,
+                                           epi_mode == 2 ? fmaf(beta, mv ? cm[j] : tc_load_c<TC>(buf, e), alpha * v[j])
+                                                         : alpha * v[j]);
+                        }
+                    }
+                    fence_async_smem();
+                    epilogue_sync();
+                    if (tid == issuer) {
+                        tma_store_2d(gC, m0, n0 + c0, smem_u32(epi) + (uint32_t)(bf * kTcTile * 32 * 4));
+                        bulk_commit();
+                    }
+                }
+                if (stop) break;
+                prev_tma = true;
+                continue;
+            }
+            if (prev_tma) {  // the staging buffers become the per-warp areas: TMA stores must be done
+                if (tid == issuer) bulk_wait_read_all();
+                epilogue_sync();
+                prev_tma = false;
+            }
+            // Lane l handles, for every 32-column chunk, the 4-row runs idx = l + 32 i (i < 8):
+            // column jj = idx / 8, rows rg * 4 .. + 3 (rg = idx % 8) of this warp's quarter. C's
+            // values (read through the row map) do not depend on the MMAs: the first chunk's are
+            // loaded before the accumulator is ready, each next chunk's while the current one is
+            // stored, so a chunk waits for no DRAM round trip of its own.
+            auto load_chunk = [&](int c0, float4 (&cv)[8]) {
+#pragma unroll
+                for (int r = 0; r < 8; r++) {
+                    cv[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (beta == 0.0f || K <= 0) continue;
+                    const int idx = lane + 32 * r;
+                    const int gj = n0 + c0 + (idx >> 3);
+                    const int gr = m0 + quarter * 32 + (idx & 7) * 4;
+                    if (gj >= N || gr >= M) continue;
+                    const int nr = M - gr < 4 ? M - gr : 4;
+                    int sr[4] = {gr, gr + 1, gr + 2, gr + 3};
+                    bool moved = false;
+                    if (rs != nullptr) {
+#pragma unroll
+                        for (int e = 0; e < 4; e++)
+                            if (e < nr) sr[e] = rs[gr + e];
+                        moved = sr[0] != gr || sr[1] != gr + 1 || sr[2] != gr + 2 || sr[3] != gr + 3;
+                    }
+                    cv[r] = tc_load_run<TC>(C, make_int4(sr[0], sr[1], sr[2], sr[3]), gj, ldc, nr, cvec && !moved);
+                }
+            };
+            float4 cv[8], cn[8];
+            load_chunk(0, cn);
+            const bool okw = mbar_wait_or_abort(&acc_full[b], (uint32_t)((i / 2) & 1), polls, abort_s);
+            // (with TMA tiles in this launch the epilogue warps must stay in step: uniform decision)
+            if (epi_mode != 0 ? epilogue_any(!okw) : !okw) {
                 give_up();
                 break;
             }
             tc_fence_after_sync();
-            const long long bidx = t / tiles;
-            const int tile = (int)(t % tiles);
-            const int m0 = (tile % tiles_m) * kTcTile, n0 = (tile / tiles_m) * kTcTile;
-            void* C = static_cast<void*>(static_cast<char*>(Carr[bidx]) + c_off * (TC == GemmElem::F32 ? 4 : 2));
             const uint32_t row_addr = tacc + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kTcTile);
-            constexpr int CES = TC == GemmElem::F32 ? 4 : 2;
-            const bool cvec = (reinterpret_cast<uintptr_t>(C) & (4 * CES - 1)) == 0 && ((long long)ldc * CES) % (4 * CES) == 0;
-            float* stg = epi + quarter * 32 * 32;  // this warp's 32 columns x 32 rows, column-major
             for (int c0 = 0; c0 < kTcTile; c0 += 32) {
                 if (n0 + c0 >= N) break;  // uniform
+#pragma unroll
+                for (int r = 0; r < 8; r++) cv[r] = cn[r];
                 float v[32];
                 tmem_ld32(row_addr + (uint32_t)c0, v);
-                if (c0 + 32 >= kTcTile || n0 + c0 + 32 >= N) {
+                const bool last = c0 + 32 >= kTcTile || n0 + c0 + 32 >= N;
+                if (last) {
                     // the accumulator is in registers: the MMA warp may start the next tile here
                     tc_fence_before_sync();
                     mbar_arrive(&acc_empty[b]);
+                } else {
+                    load_chunk(c0 + 32, cn);
                 }
-                // lane = row: stage alpha * D column by column, then every lane writes 4-row runs
-                // of C (coalesced along the columns) with one vector access each
+                // lane = row: stage alpha * D column by column, then every lane writes its runs
 #pragma unroll
                 for (int j = 0; j < 32; j++) stg[j * 32 + lane] = alpha * v[j];
                 __syncwarp();
                 if (K > 0) {
 #pragma unroll
-                    for (int i = 0; i < 8; i++) {
-                        const int idx = lane + 32 * i;
+                    for (int r = 0; r < 8; r++) {
+                        const int idx = lane + 32 * r;
                         const int jj = idx >> 3, rg = idx & 7;
                         const int gj = n0 + c0 + jj;
                         const int gr = m0 + quarter * 32 + rg * 4;
                         if (gj >= N || gr >= M) continue;
+                        const int nr = M - gr < 4 ? M - gr : 4;
                         const float4 a = *reinterpret_cast<const float4*>(&stg[jj * 32 + rg * 4]);
-                        tc_store_run<TC>(C, gr + (long long)gj * ldc, a, beta, M - gr < 4 ? M - gr : 4, cvec);
+                        const float4 res = beta == 0.0f
+                                               ? a
+                                               : make_float4(fmaf(beta, cv[r].x, a.x), fmaf(beta, cv[r].y, a.y),
+                                                             fmaf(beta, cv[r].z, a.z), fmaf(beta, cv[r].w, a.w));
+                        tc_store_vals<TC>(C, gr + (long long)gj * ldc, res, nr, cvec);
                     }
                 }
                 __syncwarp();
             }
         }
+        if (tid == issuer) bulk_wait_all();  // C is written before the CTA ends
     }
 
     // ---------------------------------------------------------------- teardown
@@ -770,8 +1058,9 @@ static bool tmap_encode(CUtensorMap* map, void* placeholder, bool mn, int rows, 
     TmapEncodeFn enc = tmap_encoder();
     if (enc == nullptr || ((long long)ld * ES) % 16 != 0) return false;
     const CUtensorMapDataType dt = ES == 1 ? CU_TENSOR_MAP_DATA_TYPE_UINT8
-                                           : (T == TcIn::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
-                                                              : CU_TENSOR_MAP_DATA_TYPE_FLOAT16);
+                                           : ES == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                     : (T == TcIn::BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                                        : CU_TENSOR_MAP_DATA_TYPE_FLOAT16);
     const cuuint64_t dims[2] = {(cuuint64_t)(mn ? rows : K), (cuuint64_t)(mn ? K : rows)};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * ES};
     const cuuint32_t box[2] = {(cuuint32_t)(mn ? 128 / ES : 128 / ES), (cuuint32_t)(mn ? 128 / ES : kTcTile)};
@@ -781,11 +1070,33 @@ static bool tmap_encode(CUtensorMap* map, void* placeholder, bool mn, int rows, 
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Template tensor map of C for the TMA epilogue: box 128 rows x 32 columns, no swizzle.
+template <GemmElem TC>
+static bool tmap_encode_c(CUtensorMap* map, void* placeholder, int m, int n, int ldc)
+{
+    constexpr int CES = TC == GemmElem::F32 ? 4 : 2;
+    TmapEncodeFn enc = tmap_encoder();
+    if (enc == nullptr || ((long long)ldc * CES) % 16 != 0) return false;
+    const CUtensorMapDataType dt = TC == GemmElem::F32   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : TC == GemmElem::F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                         : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const cuuint64_t dims[2] = {(cuuint64_t)m, (cuuint64_t)n};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldc * CES};
+    const cuuint32_t box[2] = {(cuuint32_t)kTcTile, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, dt, 2, placeholder, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// presplit > 0 (FP32 operands, transA and not transB): op(A) and op(B)^T arrive as TF32 high
+// planes whose low planes start presplit rows further down the same arrays.
 template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT>
 static cudaError_t tc_launch_t(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                                const void* const* A, long long a_off, int lda, const void* const* B, long long b_off,
                                int ldb, float beta, void* const* C, long long c_off, int ldc, int batch,
-                               unsigned* status, void* tmslots)
+                               unsigned* status, void* tmslots, const int* rowsrc = nullptr, long long rs_stride = 0,
+                               int presplit = 0)
 {
     const size_t smem = TcStages<SPLIT>::SMEM;
     const cudaError_t e = ensure_smem_limit(gemm_tc_kernel<TA, TB, TC, SPLIT>, (int)smem);
@@ -793,16 +1104,26 @@ static cudaError_t tc_launch_t(cudaStream_t st, bool transA, bool transB, int m,
     const int tm = (m + kTcTile - 1) / kTcTile, tn = (n + kTcTile - 1) / kTcTile;
     const long long total = (long long)tm * tn * batch;
     const long long grid = total < sm_count() ? total : sm_count();  // persistent: one CTA per SM
-    CUtensorMap ma{}, mb{};
+    CUtensorMap ma{}, mb{}, mc{};
     bool use_tma = false;
     constexpr bool native = TA != TcIn::F32_TF32 && TA != TcIn::F32_BF16;
-    if (native && tmslots != nullptr && grid * 2 * sizeof(CUtensorMap) <= kTensorMapSlotBytes) {
+    // FP32 operands by TMA only when both are K-contiguous (A transposed, B not): they are staged
+    // K-major, and converted to TF32 in shared memory (or arrive split, presplit)
+    constexpr bool tf32 = TA == TcIn::F32_TF32;
+    const bool slots = tmslots != nullptr && grid * 3 * sizeof(CUtensorMap) <= kTensorMapSlotBytes;
+    if ((native || (tf32 && transA && !transB)) && slots) {
         // op(A) rows = M (MN-major when A is not transposed); op(B)^T rows = N (MN-major when B is)
-        use_tma = tmap_encode<TA>(&ma, tmslots, !transA, m, k, lda) && tmap_encode<TB>(&mb, tmslots, transB, n, k, ldb);
+        use_tma = tmap_encode<TA>(&ma, tmslots, !transA, presplit + m, k, lda) &&
+                  tmap_encode<TB>(&mb, tmslots, transB, presplit + n, k, ldb);
     }
+    if (presplit > 0 && !use_tma) return cudaErrorInvalidValue;  // pre-split operands need TMA
+    // the TMA epilogue: beta = 0 stores alpha * D, otherwise loads C, combines and stores
+    int epi_mode = beta == 0.0f ? 1 : 2;
+    if (epi_mode != 0 && !(slots && tmap_encode_c<TC>(&mc, tmslots, m, n, ldc))) epi_mode = 0;
     gemm_tc_kernel<TA, TB, TC, SPLIT><<<(unsigned)grid, kTcThreads, smem, st>>>(
         m, n, k, alpha, A, a_off, lda, transA ? 1 : 0, B, b_off, ldb, transB ? 1 : 0, beta, C, c_off, ldc, tm, tn,
-        total, status, wait_limit(kTcWaitPolls), ma, mb, static_cast<CUtensorMap*>(tmslots), use_tma ? 1 : 0);
+        total, status, wait_limit(kTcWaitPolls), ma, mb, static_cast<CUtensorMap*>(tmslots), use_tma ? 1 : 0,
+        rowsrc, rs_stride, presplit > 0 ? 1 : 0, presplit, presplit, mc, epi_mode);
     return cudaGetLastError();
 }
 
@@ -837,12 +1158,23 @@ cudaError_t gemm_tc_typed_launch(cudaStream_t st, TcIn ta_kind, TcIn tb_kind, Ge
 cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                            const float* const* A, long long a_off, int lda, const float* const* B, long long b_off,
                            int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split,
-                           unsigned* status)
+                           unsigned* status, void* tmslots)
 {
     return gemm_tc_typed_launch(st, TcIn::F32_TF32, TcIn::F32_TF32, GemmElem::F32, split != 0, transA, transB, m, n,
                                 k, alpha, reinterpret_cast<const void* const*>(A), a_off, lda,
                                 reinterpret_cast<const void* const*>(B), b_off, ldb, beta,
-                                reinterpret_cast<void* const*>(C), c_off, ldc, batch, status, nullptr);
+                                reinterpret_cast<void* const*>(C), c_off, ldc, batch, status, tmslots);
+}
+
+cudaError_t gemm_tc_lu_update(cudaStream_t st, int m, const float* const* L21, const float* const* U12, float* const* LU,
+                              long long c_off, int ldlu, int batch, const int* rowsrc, long long rs_stride,
+                              int lo_rows, unsigned* status, void* tmslots)
+{
+    if (m <= 0 || batch <= 0) return cudaSuccess;
+    return tc_launch_t<TcIn::F32_TF32, TcIn::F32_TF32, GemmElem::F32, true>(
+        st, true, false, m, m, 32, -1.0f, reinterpret_cast<const void* const*>(L21), 0, 32,
+        reinterpret_cast<const void* const*>(U12), 0, 32, 1.0f, reinterpret_cast<void* const*>(LU), c_off, ldlu, batch,
+        status, tmslots, rowsrc, rs_stride, lo_rows);
 }
 
 }  // namespace opsblas

@@ -33,7 +33,7 @@ struct _aclblas_handle {
 namespace opsblas {
 
 constexpr size_t kDefaultWorkspaceBytes = 32u * 1024u * 1024u;
-constexpr size_t kTensorMapSlotBytes = 512u * 2u * 128u;  // up to 512 CTAs x (A, B) x 128-byte map
+constexpr size_t kTensorMapSlotBytes = 512u * 3u * 128u;  // up to 512 CTAs x (A, B, C) x 128-byte map
 
 // Logging through the aclblasLoggerConfigure / aclblasSetLoggerCallback configuration.
 void log_error(const char* api, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
@@ -110,7 +110,27 @@ cudaError_t gemm_tc_typed_launch(cudaStream_t st, TcIn ta, TcIn tb, GemmElem tc,
 cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                            const float* const* A, long long a_off, int lda, const float* const* B, long long b_off,
                            int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split,
-                           unsigned* status);
+                           unsigned* status, void* tmslots);
+
+// Trailing update of the blocked mixed-precision LU: for every matrix b, the m x m block of LU[b]
+// at element offset c_off (leading dimension ldlu) becomes C(src(r), j) - L21[b](r, :) * U12[b](:, j)
+// with split-TF32 tensor-core products; L21 is m x 32 row-major, U12 32 x m column-major (both
+// with leading dimension 32), each given as its TF32 high plane followed, lo_rows rows further,
+// by its low plane; src(r) = rowsrc[b * rs_stride + r] (relative to the block's first row).
+cudaError_t gemm_tc_lu_update(cudaStream_t st, int m, const float* const* L21, const float* const* U12,
+                              float* const* LU, long long c_off, int ldlu, int batch, const int* rowsrc,
+                              long long rs_stride, int lo_rows, unsigned* status, void* tmslots);
+
+// refine.cu: out[i] = base + i * stride (floats), i < count.
+__global__ void init_ptr_array_kernel(float** out, float* base, long long stride, int count);
+
+// getrf_blocked_tc.cu: 256 < n <= 1024, blocked mixed-precision LU (FP32 panels, split-TF32
+// tensor-core trailing update) in place on LU; scratch: getrf_blocked_tc_scratch_bytes(n, batch)
+// bytes of device memory (256-byte aligned).
+bool getrf_blocked_tc_supported(int n);
+size_t getrf_blocked_tc_scratch_bytes(int n, int batch);
+cudaError_t getrf_blocked_tc_launch(cudaStream_t st, float* const* LUarray, int n, int ldlu, int* piv, int* info,
+                                    int batch, void* scratch, unsigned* status, void* tmslots);
 
 // getrf_tmem.cu: 32 < n <= 256, mixed-precision LU with the matrix resident in TMEM.
 bool getrf_tmem_supported(int n);

@@ -4,9 +4,9 @@
 //   LU = A (copy; A is kept for the residual), P*LU = A factored by aclblasSgetrfBatched's
 //   kernels -- plain FP32 for ACLBLAS_COMPUTE_32F; for ACLBLAS_COMPUTE_32F_FAST_TF32 / _FAST_16BF
 //   with the split TF32 / BF16 trailing update on the tensor cores, the matrix resident in TMEM
-//   (getrf_tmem.cu, 32 < n <= 256); other orders factor in plain FP32 (above n = 256 the matrix
-//   does not fit one SM's tensor memory, and a split update on the CUDA cores measured slower
-//   than the plain kernel), after which refinement converges at once;
+//   (getrf_tmem.cu, 32 < n <= 256); for TF32 with 256 < n <= 1024 the blocked LU with FP32
+//   panels and the tensor-core trailing update (getrf_blocked_tc.cu), when the workspace also
+//   holds its scratch; other cases factor in plain FP32, after which refinement converges at once;
 //   X = LU \ B (aclblasSgetrsBatched's kernels);
 //   repeat up to maxIter times: r = B - A X in FP64 on the GPU, backward error
 //     berr = max_c ||r_c||_inf / (||A||_inf ||x_c||_inf + ||b_c||_inf) in FP64;
@@ -27,14 +27,24 @@ __global__ void init_ptr_array_kernel(float** out, float* base, long long stride
         out[i] = base + i * stride;
 }
 
-// dst[b](i, j) = src[b](i, j), i < rows, j < cols
+// dst[b](i, j) = src[b](i, j), i < rows, j < cols. One CTA per matrix, a warp per column at a
+// time, 16-byte accesses when both columns are 16-byte aligned.
 __global__ void copy_batched_kernel(const float* const* src, int lds, float* const* dst, int ldd, int rows, int cols)
 {
-    const float* s = src[blockIdx.x];  // one CTA per matrix
+    const float* s = src[blockIdx.x];
     float* d = dst[blockIdx.x];
-    for (long long e = threadIdx.x; e < (long long)rows * cols; e += blockDim.x) {
-        const long long i = e % rows, j = e / rows;
-        d[i + j * ldd] = s[i + j * lds];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const bool vec = ((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d)) & 15) == 0 && lds % 4 == 0 &&
+                     ldd % 4 == 0;
+    for (int j = warp; j < cols; j += nw) {
+        const float* sc = s + (long long)j * lds;
+        float* dc = d + (long long)j * ldd;
+        int i = 0;
+        if (vec) {
+            for (; i + 128 <= rows; i += 128)
+                reinterpret_cast<float4*>(dc + i)[lane] = reinterpret_cast<const float4*>(sc + i)[lane];
+        }
+        for (i += lane; i < rows; i += 32) dc[i] = sc[i];
     }
 }
 
@@ -226,6 +236,11 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
                   handle->workspace_size);
         return ACLBLAS_STATUS_EXECUTION_FAILED;
     }
+    // TF32 above n = 256: the blocked tensor-core LU when the workspace also holds its scratch
+    // (after the refinement's part, 256-byte aligned); else plain FP32 factors
+    const size_t bt_off = (need + 255) / 256 * 256;
+    const bool blocked = mode == 1 && getrf_blocked_tc_supported(n) &&
+                         handle->workspace_size >= bt_off + getrf_blocked_tc_scratch_bytes(n, batchCount);
     char* ws = static_cast<char*>(handle->workspace);
     float* dbase = reinterpret_cast<float*>(ws);
     float** dptr = reinterpret_cast<float**>(ws + dbytes * batchCount);
@@ -244,6 +259,9 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     if (tmem) {
         err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode,
                                 handle->dstatus);
+    } else if (blocked) {
+        err = getrf_blocked_tc_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, ws + bt_off,
+                                      handle->dstatus, handle->tmslots);
     } else {  // plain FP32 factors: the batched getrf's kernels
         aclblasStatus_t s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;

@@ -26,7 +26,15 @@
 /* Pivot search of FindPivotRow (blas/getrf_batched/arch35/sgetrf_batched_kernel.cpp:52-79):
  * the first row r >= col with the largest |A(r,col)| strictly greater than zero; when every
  * candidate is zero or NaN the result is col. Also returns the relative gap between the two
- * largest candidate magnitudes, the tie measure used by the tests. */
+ * largest candidate magnitudes, the tie measure used by the tests.
+ *
+ * Exact ties above n = 256. The reference searches with 256 threads, thread t striding over
+ * rows col+t, col+t+256, ..., and its tree reduction keeps the lower THREAD index on an exact
+ * tie of magnitudes. For n <= 256 every thread holds at most one row and that equals the
+ * lower row; above n = 256 a tie between rows col+t+256 and col+u (t < u) goes to the higher
+ * row col+t+256. This function keeps the first row in every case. The tests compare pivots only
+ * for matrices whose two largest candidates differ by more than 1e-5 relative at every step, so
+ * the difference never reaches a comparison. */
 static int find_pivot(const float* A, int lda, int col, int n, double* gap)
 {
     float best = 0.0f, second = 0.0f;

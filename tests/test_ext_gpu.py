@@ -63,6 +63,8 @@ GEMM_CASES = [
     ("T", "T", 96, 100, 200, 1.0, 0.0, "E4M3", "E5M2", "F16", 2, 4e-3),
     ("N", "N", 257, 129, 300, 1.0, 0.0, "F32", "F32", "F32", 6, 2e-3),
     ("T", "T", 140, 70, 130, 1.0, -1.0, "F32", "F32", "F32", 5, 2e-2),
+    ("T", "N", 300, 260, 200, 1.0, 0.5, "F32", "F32", "F32", 6, 2e-3),   # FP32 by TMA, converted in shared memory
+    ("T", "N", 128, 64, 36, -1.0, 1.0, "F32", "F32", "F32", 6, 2e-3),
 ]
 DT = {"F32": 0, "F16": 1, "BF16": 27, "E5M2": 35, "E4M3": 36}
 
@@ -334,3 +336,75 @@ def test_tmem_mixed_lu_singular(handle, compute):
     inf = to_host(info)
     assert inf[0] == 1 and inf[1] >= 1 and inf[2] >= 1 and inf[3] >= 1
     assert all(i <= c + 1 for i, c in zip(inf, [0, 31, 32, 77]))
+
+
+@pytest.mark.parametrize("n", [257, 300, 512, 545, 700])
+def test_blocked_tc_lu_reconstructs(handle, n):
+    """TF32 mode above n = 256 (blocked LU: FP32 panels, split-TF32 tcgen05 trailing updates fed
+    by TMA, row interchanges folded into the update's reads): P*A = L*U in FP64 to the split's
+    precision, the pivots form a permutation, and refinement reaches an FP64 backward error <= 1e-6.
+    545 and 700 factor their first panels with 1024-thread CTAs; 300 and 545 end on a partial panel."""
+    import torch
+
+    batch, nrhs = 3, 2
+    A64, a32 = conditioned_batch(n, batch, 1e3, seed=n)
+    b = np.random.default_rng(n).standard_normal((batch, nrhs, n)).astype(np.float32)
+    X, LU, piv, info, berr, iters = handle.refine(to_dev(a32, "cuda"), to_dev(b, "cuda"), n, nrhs,
+                                                  compute=6, max_iter=10, tol=1e-6)
+    torch.cuda.synchronize()
+    assert int(info.max()) == 0 and int(info.min()) == 0
+    lu, pv = to_host(LU), to_host(piv)
+    for q in range(batch):
+        assert sorted(_apply_pivots(np.arange(n)[:, None].astype(float), pv[q])[:, 0].astype(int)) == list(range(n))
+        F = lu[q].T.astype(np.float64)
+        L = np.tril(F, -1) + np.eye(n)
+        U = np.triu(F)
+        PA = _apply_pivots(a32[q].T.astype(np.float64), pv[q])
+        rel = np.linalg.norm(PA - L @ U) / np.linalg.norm(PA)
+        assert rel < 3e-6, (q, rel)
+    assert float(to_host(berr).max()) <= 1e-6
+    st, flags = handle.device_status()
+    assert st == 0 and flags == 0
+
+
+def test_blocked_tc_lu_singular(handle):
+    """A zero column stops the blocked factorisation with info <= that column + 1; the other
+    matrices of the batch are factored and refined as usual."""
+    import torch
+
+    n, batch, nrhs = 320, 4, 1
+    A64, a32 = conditioned_batch(n, batch, 1e2, seed=3)
+    for q, col in enumerate([0, 40, 300]):
+        a32[q, col, :] = 0.0
+    b = np.random.default_rng(5).standard_normal((batch, nrhs, n)).astype(np.float32)
+    X, LU, piv, info, berr, iters = handle.refine(to_dev(a32, "cuda"), to_dev(b, "cuda"), n, nrhs, compute=6,
+                                                  max_iter=5, tol=1e-6)
+    torch.cuda.synchronize()
+    inf = to_host(info)
+    assert inf[0] == 1 and 1 <= inf[1] <= 41 and 1 <= inf[2] <= 301
+    assert inf[3] == 0 and float(to_host(berr)[3]) <= 1e-6
+
+
+def test_blocked_tc_lu_full_occupancy(handle):
+    """n = 512 at the benchmark's kappa = 1e4, 300 matrices (two waves of panel CTAs): every matrix
+    converges to an FP64 backward error <= 1e-6."""
+    import torch
+
+    n, batch, nrhs = 512, 300, 4
+    g = torch.Generator(device="cuda").manual_seed(11)
+    q1, _ = torch.linalg.qr(torch.randn(batch, n, n, device="cuda", dtype=torch.float64, generator=g))
+    q2, _ = torch.linalg.qr(torch.randn(batch, n, n, device="cuda", dtype=torch.float64, generator=g))
+    s = torch.logspace(0, 4, n, device="cuda", dtype=torch.float64)
+    A = ((q1 * s) @ q2.transpose(1, 2)).transpose(1, 2).contiguous().float()
+    del q1, q2
+    B = torch.randn(batch, nrhs, n, device="cuda", generator=g)
+    X, LU, piv, info, berr, iters = handle.refine(A, B, n, nrhs, compute=6, max_iter=10, tol=1e-6)
+    torch.cuda.synchronize()
+    assert int(info.abs().max()) == 0
+    a64 = A.double().transpose(1, 2)
+    x64 = X.double().transpose(1, 2)
+    b64 = B.double().transpose(1, 2)
+    r = b64 - a64 @ x64
+    an = a64.abs().sum(2).amax(1)
+    e = (r.abs().amax(1) / (an[:, None] * x64.abs().amax(1) + b64.abs().amax(1))).amax(1)
+    assert float(e.max()) <= 1e-6, float(e.max())
