@@ -219,7 +219,7 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasGemmBatchedEx(
  * (aclblasSetWorkspace); EXECUTION_FAILED if it is smaller. With _FAST_TF32 and 256 < n <= 1024
  * the factorization is blocked (FP32 panels of 32 columns, split-TF32 tensor-core trailing
  * updates) when the workspace holds, after that amount rounded up to 256, another P + 16 bytes
- * per matrix + 512, P = the sum of 2*(n-32)*128, 3*(n-32)*128 and 4*n, each rounded up to 256;
+ * per matrix + 512, P = 2*(n-32)*128 rounded up to 256, twice;
  * with less, and for _FAST_16BF above n = 256, the factors are plain FP32. */
 ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     aclblasHandle_t handle, int n, int nrhs, const float* const Aarray[], int lda, float* const LUarray[], int ldlu,

@@ -229,7 +229,7 @@ class Handle:
         need = (((n * nrhs * 4 + 255) // 256) * 256 + 20) * batch + 512
         if 256 < n <= 1024:  # scratch of the blocked tensor-core LU (TF32 mode), after the refinement's part
             plane = (n - 32) * 32 * 4
-            per = sum((x + 255) // 256 * 256 for x in (2 * plane, 3 * plane, 4 * n))
+            per = 2 * ((2 * plane + 255) // 256 * 256)
             need = (need + 255) // 256 * 256 + per * batch + batch * 16 + 512
         if self._ws is None or self._ws.numel() < need:
             self._ws = torch.empty(max(need, 32 << 20), dtype=torch.uint8, device=dev)

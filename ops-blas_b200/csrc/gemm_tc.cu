@@ -183,6 +183,20 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* mbar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
 }
 
+// q = t / tiles, r = t % tiles, in 32-bit arithmetic when t fits (64-bit division is a long
+// instruction sequence on the epilogue's critical path)
+__device__ __forceinline__ void tile_split(long long t, int tiles, long long& q, int& r)
+{
+    if (t >= 0 && t <= 0xffffffffLL) {
+        const unsigned tu = (unsigned)t, qq = tu / (unsigned)tiles;
+        q = qq;
+        r = (int)(tu - qq * (unsigned)tiles);
+    } else {
+        q = t / tiles;
+        r = (int)(t % tiles);
+    }
+}
+
 template <GemmElem TC>
 __device__ __forceinline__ float tc_load_c(const void* C, long long idx)
 {
@@ -246,13 +260,16 @@ __device__ __forceinline__ void tc_store_vals(void* C, long long idx, const floa
     for (int e = 0; e < n && e < 4; e++) tc_store_c<TC>(C, idx + e, rv[e]);
 }
 
-template <bool SPLIT>
+// Shared-memory plan. LU: the LU trailing update (K = 32, one K tile a tile): one operand stage,
+// and a ring of eight C chunks so that the next tile's C is loaded while this one is combined.
+template <bool SPLIT, bool LU = false>
 struct TcStages {
-    static constexpr int S = SPLIT ? 2 : 4;
+    static constexpr int S = LU ? 1 : (SPLIT ? 2 : 4);
+    static constexpr int RING = LU ? 8 : 5;                         // TMA epilogue staging buffers
     static constexpr int PARTS = SPLIT ? 2 : 1;                     // hi (+ lo)
     static constexpr int STAGE_BYTES = 2 * PARTS * kTcOperandBytes;  // A and B
-    // epilogue staging: three 128 x 32 FP32 chunks of C (the TMA epilogue), or 4 KB per warp
-    static constexpr int EPI_BYTES = 3 * kTcTile * 32 * 4;
+    // epilogue staging: a ring of RING 128 x 32 FP32 chunks of C (the TMA epilogue), or 4 KB per warp
+    static constexpr int EPI_BYTES = RING * kTcTile * 32 * 4;
     // stages | barriers (0..511) | tensor maps (512..895) | staging (from 1024) | alignment slack
     static constexpr size_t SMEM = (size_t)S * STAGE_BYTES + 1024 + EPI_BYTES + 1024;
 };
@@ -518,21 +535,22 @@ __device__ __forceinline__ void converters_sync()
     asm volatile("bar.sync 2, %0;" ::"n"(kTcProducers - 32) : "memory");
 }
 
-template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT>
+template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT, bool LU>
 __global__ void __launch_bounds__(kTcThreads, 1)
 gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__ Aarr, long long a_off, int lda,
                int tA, const void* const* __restrict__ Barr, long long b_off, int ldb, int tB, float beta,
                void* const* __restrict__ Carr, long long c_off, int ldc, int tiles_m, int tiles_n, long long total,
                unsigned* __restrict__ status, unsigned polls, const __grid_constant__ CUtensorMap tmA,
                const __grid_constant__ CUtensorMap tmB, CUtensorMap* __restrict__ gslots, int use_tma,
-               const int* __restrict__ rowsrc, long long rs_stride, int presplit, int a_lo_rows, int b_lo_rows,
-               const __grid_constant__ CUtensorMap tmC, int epi_mode)
+               int presplit, int a_lo_rows, int b_lo_rows,
+               const __grid_constant__ CUtensorMap tmC, int epi_mode, int contig)
 {
     static_assert(tc_esize(TA) == tc_esize(TB), "A and B share the MMA kind");
     constexpr int ES = tc_esize(TA);
     using L = TcLayout<ES>;
-    using ST = TcStages<SPLIT>;
+    using ST = TcStages<SPLIT, LU>;
     constexpr int S = ST::S;
+    constexpr int R = ST::RING;
     using SA = typename TcSrc<TA>::type;
     using SB = typename TcSrc<TB>::type;
 
@@ -546,14 +564,19 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
     uint64_t* acc_full = ready + S;
     uint64_t* acc_empty = acc_full + 2;
     uint64_t* drain = acc_empty + 2;
-    uint64_t* cload = drain + 1;  // TMA epilogue: the three staging buffers' loads of C
-    uint32_t* taddr_s = reinterpret_cast<uint32_t*>(cload + 3);
+    uint64_t* cload = drain + 1;  // TMA epilogue: the staging buffers' loads of C
+    uint32_t* taddr_s = reinterpret_cast<uint32_t*>(cload + R);
     int* abort_s = reinterpret_cast<int*>(taddr_s + 1);
     CUtensorMap* smap = reinterpret_cast<CUtensorMap*>(sm + S * ST::STAGE_BYTES + 512);  // A, B, C (128-aligned)
     float* epi = reinterpret_cast<float*>(sm + S * ST::STAGE_BYTES + 1024);             // epilogue staging
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles = tiles_m * tiles_n;
+    // the CTA's tiles: every gridDim.x-th one, or (contig) one contiguous range, so that
+    // consecutive tiles mostly belong to the same matrix and keep its tensor maps
+    const long long t_first = contig ? (long long)blockIdx.x * total / gridDim.x : (long long)blockIdx.x;
+    const long long t_last = contig ? ((long long)blockIdx.x + 1) * total / gridDim.x : total;
+    const long long t_step = contig ? 1 : (long long)gridDim.x;
     const bool amn = tA == 0;  // op(A) = A: M contiguous
     const bool bmn = tB != 0;  // op(B)^T rows = B's columns when transposed: N contiguous
     const bool amn_s = tc_smem_mn<TA>(amn), bmn_s = tc_smem_mn<TB>(bmn);  // orientation in shared memory
@@ -579,7 +602,7 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
             mbar_init(&acc_empty[q], kTcEpilogue);
         }
         mbar_init(drain, 1);
-        for (int q = 0; q < 3; q++) mbar_init(&cload[q], 1);
+        for (int q = 0; q < R; q++) mbar_init(&cload[q], 1);
         *abort_s = 0;
         fence_mbar_init();
     }
@@ -613,11 +636,12 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
         long long g = 0;          // K tiles issued by this CTA (the ring position)
         long long issued = 0;     // K tiles whose loads were actually issued (warp 0 tracks it)
         long long mapped = -1;    // the matrix the global maps point at
-        for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+        for (long long t = t_first; t < t_last; t += t_step) {
             // every producer thread takes the same path through every tile (named barrier 1)
             if (producers_any(aborted())) break;
-            const long long bidx = t / tiles;
-            const int tile = (int)(t % tiles);
+            long long bidx;
+            int tile;
+            tile_split(t, tiles, bidx, tile);
             const int m0 = (tile % tiles_m) * kTcTile, n0 = (tile / tiles_m) * kTcTile;
             const SA* A = static_cast<const SA*>(Aarr[bidx]) + a_off;
             const SB* B = static_cast<const SB*>(Barr[bidx]) + b_off;
@@ -757,7 +781,7 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                 tc_idesc(tc_format(TA), tc_format(TB), amn_s ? 1u : 0u, bmn_s ? 1u : 0u, kTcTile, kTcTile);
             long long g = 0;
             long long i = 0;  // local tile count
-            for (long long t = blockIdx.x; t < total; t += gridDim.x, i++) {
+            for (long long t = t_first; t < t_last; t += t_step, i++) {
                 const int b = (int)(i & 1);
                 if (i >= 2 && !mbar_wait_or_abort(&acc_empty[b], (uint32_t)((i / 2 - 1) & 1), polls, abort_s)) {
                     give_up();
@@ -802,6 +826,8 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
         long long mapped_c = -1;
         bool prev_tma = false;
         long long gch = 0;      // TMA epilogue chunks so far (the staging buffer ring position)
+        long long gis = 0;      // issuer: chunks whose loads of C were issued (runs ahead of gch)
+        void* pre_c = nullptr;  // the next tile's matrix pointer, read ahead
         uint32_t cphase = 0;    // bit k: the phase to wait for on cload[k]
         if (epi_mode != 0 && tid == issuer) {
             const uint4* pc = reinterpret_cast<const uint4*>(&tmC);
@@ -810,21 +836,28 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
             for (int k = 0; k < 8; k++) dc[k] = pc[k];
         }
         long long i = 0;
-        for (long long t = blockIdx.x; t < total; t += gridDim.x, i++) {
+        for (long long t = t_first; t < t_last; t += t_step, i++) {
             const int b = (int)(i & 1);
-            const long long bidx = t / tiles;
-            const int tile = (int)(t % tiles);
+            long long bidx;
+            int tile;
+            tile_split(t, tiles, bidx, tile);
             const int m0 = (tile % tiles_m) * kTcTile, n0 = (tile / tiles_m) * kTcTile;
-            void* C = static_cast<void*>(static_cast<char*>(Carr[bidx]) + c_off * CES);
+            void* C = static_cast<void*>(static_cast<char*>(i > 0 ? pre_c : Carr[bidx]) + c_off * CES);
+            // the next tile's matrix pointer: its load's latency hides behind this tile
+            long long bnx = bidx;
+            int tlx = tile;
+            if (t + t_step < t_last) {
+                tile_split(t + t_step, tiles, bnx, tlx);
+                pre_c = Carr[bnx];
+            }
             const bool cvec = (reinterpret_cast<uintptr_t>(C) & (4 * CES - 1)) == 0 && ((long long)ldc * CES) % (4 * CES) == 0;
-            const int* rs = rowsrc != nullptr ? rowsrc + bidx * rs_stride : nullptr;
-            const int gi = m0 + quarter * 32 + lane;  // this lane's row
             if (epi_mode != 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0) {
-                // ---- TMA epilogue in 128 x 32 chunks through three rotating staging buffers:
-                // beta = 0: alpha * D staged and stored by TMA; otherwise the chunk of C is loaded
-                // by TMA (the first one before the accumulator is ready, each next one while the
-                // current one is combined), combined in place (beta * C + alpha * D) and stored.
-                // Rows that the row map takes from other rows read those rows' values directly.
+                // ---- TMA epilogue in 128 x 32 chunks through a ring of R staging buffers:
+                // beta = 0: alpha * D staged and stored by TMA; otherwise every chunk of the tile's
+                // C is loaded by TMA before the accumulator is ready (up to 64 KB in flight; with
+                // the LU's ring of eight, each chunk of the CTA's next tile of the same matrix is
+                // loaded as soon as this tile's chunk is stored), combined in place
+                // (beta * C + alpha * D) and stored.
                 if (bidx != mapped_c) {
                     if (warp == kTcProducers / 32 + 1) {
                         if (lane == 0) {
@@ -838,52 +871,47 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                     }
                     mapped_c = bidx;
                 }
-                // a row that the row map takes from another row reads that row's C itself (32
-                // independent loads per chunk, issued before the chunk's waits) in place of the
-                // staged values of its own row
-                int srow = gi;
-                if (epi_mode == 2 && rs != nullptr && gi < M) srow = rs[gi];
-                const bool mv = srow != gi;
                 const int nchunks = (N - n0) < kTcTile ? (N - n0 + 31) / 32 : kTcTile / 32;
                 epilogue_sync();
-                // chunk gcc's load of C into buffer gcc % 3, whose last store was chunk gcc - 3's
-                // (stores are issued up to the current chunk - 1: `lookahead` loads run one ahead)
-                auto load_chunk_tma = [&](long long gcc, int c0, bool lookahead) {  // issuer only
-                    const int bf = (int)(gcc % 3);
-                    if (lookahead)
-                        bulk_wait_read_n<1>();
-                    else
-                        bulk_wait_read_n<2>();
+                // chunk g's load of C goes to buffer g % R, whose last store was chunk g - R's. The
+                // tile's chunks not issued ahead (g = gch + c, c < 4): stores are committed up to
+                // chunk gch - 1, so at most R - 4 of them may still be reading their buffers.
+                auto issue_load = [&](long long g, int lm0, int ln0) {  // issuer only
+                    const int bf = (int)(g % R);
                     mbar_arrive_expect_tx(&cload[bf], (uint32_t)(kTcTile * 32 * CES));
-                    tma_load_2d(smem_u32(epi) + (uint32_t)(bf * kTcTile * 32 * 4), gC, m0, n0 + c0, &cload[bf]);
+                    tma_load_2d(smem_u32(epi) + (uint32_t)(bf * kTcTile * 32 * 4), gC, lm0, ln0, &cload[bf]);
                 };
-                // after a give-up: loads of C still in flight land before the CTA ends
-                auto drain_load = [&](long long gcc) {
-                    const int bf = (int)(gcc % 3);
-                    mbar_wait_bounded(&cload[bf], (cphase >> bf) & 1u, kTcWaitPolls);
+                if (epi_mode == 2 && tid == issuer && gis < gch + nchunks) {
+                    bulk_wait_read_n<R - 4>();
+                    for (; gis < gch + nchunks; gis++) issue_load(gis, m0, n0 + (int)(gis - gch) * 32);
+                }
+                // the CTA's next tile, when it belongs to the same matrix (same tensor map): its
+                // chunks are loaded ahead, one after each of this tile's stores (LU ring only)
+                const bool ahead = R >= 8 && epi_mode == 2 && t + t_step < t_last && bnx == bidx;
+                const int m2 = (tlx % tiles_m) * kTcTile, n2 = (tlx / tiles_m) * kTcTile;
+                const int nchunks2 = (N - n2) < kTcTile ? (N - n2 + 31) / 32 : kTcTile / 32;
+                // after a give-up: the loads of C issued from chunk g0 on land before the CTA ends
+                auto drain_loads = [&](long long g0) {
+                    for (long long g = g0; g < gis; g++) {
+                        const int bf = (int)(g % R);
+                        mbar_wait_bounded(&cload[bf], (cphase >> bf) & 1u, kTcWaitPolls);
+                    }
                 };
-                if (epi_mode == 2 && tid == issuer) load_chunk_tma(gch, 0, false);
+                const long long gch0 = gch;
                 const bool ok = mbar_wait_or_abort(&acc_full[b], (uint32_t)((i / 2) & 1), polls, abort_s);
                 if (epilogue_any(!ok)) {
                     if (tid == issuer) {
                         give_up();
-                        if (epi_mode == 2) drain_load(gch);
+                        if (epi_mode == 2) drain_loads(gch0);
                     }
                     break;
                 }
                 tc_fence_after_sync();
                 const uint32_t row_addr = tacc + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * kTcTile);
                 bool stop = false;
-                for (int c = 0; c < nchunks; c++, gch++) {
+                for (int c = 0; c < nchunks; c++) {
                     const int c0 = c * 32;
-                    const int bf = (int)(gch % 3);
-                    if (epi_mode == 2 && tid == issuer && c + 1 < nchunks) load_chunk_tma(gch + 1, c0 + 32, true);
-                    float cm[32];
-                    if (mv) {
-#pragma unroll
-                        for (int j = 0; j < 32; j++)
-                            cm[j] = n0 + c0 + j < N ? tc_load_c<TC>(C, srow + (long long)(n0 + c0 + j) * ldc) : 0.0f;
-                    }
+                    const int bf = (int)((gch0 + c) % R);
                     float v[32];
                     tmem_ld32(row_addr + (uint32_t)c0, v);
                     if (c + 1 == nchunks) {
@@ -895,34 +923,42 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                         if (epilogue_any(!okc)) {
                             if (tid == issuer) {
                                 give_up();
-                                drain_load(gch);
-                                if (c + 1 < nchunks) drain_load(gch + 1);
+                                drain_loads(gch0 + c);
                             }
                             stop = true;
                             break;
                         }
                         cphase ^= 1u << bf;
                     } else {
-                        if (tid == issuer) bulk_wait_read_n<2>();  // the store of chunk gch - 3 has read it
+                        // the store of chunk gch0 + c - R has read the buffer (R - 1 later ones may be reading)
+                        if (tid == issuer) bulk_wait_read_n<R - 1>();
                         epilogue_sync();
                     }
                     const int row = quarter * 32 + lane;
                     if constexpr (TC == GemmElem::F32) {
                         float* buf = epi + bf * kTcTile * 32;
+                        if (epi_mode == 2) {
 #pragma unroll
-                        for (int j = 0; j < 32; j++) {
-                            float* e = &buf[j * kTcTile + row];
-                            *e = epi_mode == 2 ? fmaf(beta, mv ? cm[j] : *e, alpha * v[j]) : alpha * v[j];
+                            for (int j = 0; j < 32; j++) {
+                                float* e = &buf[j * kTcTile + row];
+                                *e = fmaf(beta, *e, alpha * v[j]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; j++) buf[j * kTcTile + row] = alpha * v[j];
                         }
                     } else {
                         using H = typename std::conditional<TC == GemmElem::F16, __half, __nv_bfloat16>::type;
                         H* buf = reinterpret_cast<H*>(epi + bf * kTcTile * 32);
+                        if (epi_mode == 2) {
 #pragma unroll
-                        for (int j = 0; j < 32; j++) {
-                            const int e = j * kTcTile + row;
-                            tc_store_c<TC>(buf, e,
-                                           epi_mode == 2 ? fmaf(beta, mv ? cm[j] : tc_load_c<TC>(buf, e), alpha * v[j])
-                                                         : alpha * v[j]);
+                            for (int j = 0; j < 32; j++) {
+                                const int e = j * kTcTile + row;
+                                tc_store_c<TC>(buf, e, fmaf(beta, tc_load_c<TC>(buf, e), alpha * v[j]));
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < 32; j++) tc_store_c<TC>(buf, j * kTcTile + row, alpha * v[j]);
                         }
                     }
                     fence_async_smem();
@@ -930,8 +966,16 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                     if (tid == issuer) {
                         tma_store_2d(gC, m0, n0 + c0, smem_u32(epi) + (uint32_t)(bf * kTcTile * 32 * 4));
                         bulk_commit();
+                        // the next tile's chunk c: g = gch0 + nchunks + c, its buffer's last store is
+                        // chunk g - R <= gch0 + c + 4 - R, with stores committed up to chunk gch0 + c
+                        if (ahead && c < nchunks2 && gis == gch0 + nchunks + c) {
+                            bulk_wait_read_n<R - 4>();
+                            issue_load(gis, m2, n2 + c0);
+                            gis++;
+                        }
                     }
                 }
+                gch = gch0 + nchunks;
                 if (stop) break;
                 prev_tma = true;
                 continue;
@@ -943,7 +987,7 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
             }
             // Lane l handles, for every 32-column chunk, the 4-row runs idx = l + 32 i (i < 8):
             // column jj = idx / 8, rows rg * 4 .. + 3 (rg = idx % 8) of this warp's quarter. C's
-            // values (read through the row map) do not depend on the MMAs: the first chunk's are
+            // values do not depend on the MMAs: the first chunk's are
             // loaded before the accumulator is ready, each next chunk's while the current one is
             // stored, so a chunk waits for no DRAM round trip of its own.
             auto load_chunk = [&](int c0, float4 (&cv)[8]) {
@@ -956,15 +1000,7 @@ gemm_tc_kernel(int M, int N, int K, float alpha, const void* const* __restrict__
                     const int gr = m0 + quarter * 32 + (idx & 7) * 4;
                     if (gj >= N || gr >= M) continue;
                     const int nr = M - gr < 4 ? M - gr : 4;
-                    int sr[4] = {gr, gr + 1, gr + 2, gr + 3};
-                    bool moved = false;
-                    if (rs != nullptr) {
-#pragma unroll
-                        for (int e = 0; e < 4; e++)
-                            if (e < nr) sr[e] = rs[gr + e];
-                        moved = sr[0] != gr || sr[1] != gr + 1 || sr[2] != gr + 2 || sr[3] != gr + 3;
-                    }
-                    cv[r] = tc_load_run<TC>(C, make_int4(sr[0], sr[1], sr[2], sr[3]), gj, ldc, nr, cvec && !moved);
+                    cv[r] = tc_load_run<TC>(C, make_int4(gr, gr + 1, gr + 2, gr + 3), gj, ldc, nr, cvec);
                 }
             };
             float4 cv[8], cn[8];
@@ -1091,15 +1127,14 @@ static bool tmap_encode_c(CUtensorMap* map, void* placeholder, int m, int n, int
 
 // presplit > 0 (FP32 operands, transA and not transB): op(A) and op(B)^T arrive as TF32 high
 // planes whose low planes start presplit rows further down the same arrays.
-template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT>
+template <TcIn TA, TcIn TB, GemmElem TC, bool SPLIT, bool LU = false>
 static cudaError_t tc_launch_t(cudaStream_t st, bool transA, bool transB, int m, int n, int k, float alpha,
                                const void* const* A, long long a_off, int lda, const void* const* B, long long b_off,
                                int ldb, float beta, void* const* C, long long c_off, int ldc, int batch,
-                               unsigned* status, void* tmslots, const int* rowsrc = nullptr, long long rs_stride = 0,
-                               int presplit = 0)
+                               unsigned* status, void* tmslots, int presplit = 0)
 {
-    const size_t smem = TcStages<SPLIT>::SMEM;
-    const cudaError_t e = ensure_smem_limit(gemm_tc_kernel<TA, TB, TC, SPLIT>, (int)smem);
+    const size_t smem = TcStages<SPLIT, LU>::SMEM;
+    const cudaError_t e = ensure_smem_limit(gemm_tc_kernel<TA, TB, TC, SPLIT, LU>, (int)smem);
     if (e != cudaSuccess) return e;
     const int tm = (m + kTcTile - 1) / kTcTile, tn = (n + kTcTile - 1) / kTcTile;
     const long long total = (long long)tm * tn * batch;
@@ -1120,10 +1155,10 @@ static cudaError_t tc_launch_t(cudaStream_t st, bool transA, bool transB, int m,
     // the TMA epilogue: beta = 0 stores alpha * D, otherwise loads C, combines and stores
     int epi_mode = beta == 0.0f ? 1 : 2;
     if (epi_mode != 0 && !(slots && tmap_encode_c<TC>(&mc, tmslots, m, n, ldc))) epi_mode = 0;
-    gemm_tc_kernel<TA, TB, TC, SPLIT><<<(unsigned)grid, kTcThreads, smem, st>>>(
+    gemm_tc_kernel<TA, TB, TC, SPLIT, LU><<<(unsigned)grid, kTcThreads, smem, st>>>(
         m, n, k, alpha, A, a_off, lda, transA ? 1 : 0, B, b_off, ldb, transB ? 1 : 0, beta, C, c_off, ldc, tm, tn,
         total, status, wait_limit(kTcWaitPolls), ma, mb, static_cast<CUtensorMap*>(tmslots), use_tma ? 1 : 0,
-        rowsrc, rs_stride, presplit > 0 ? 1 : 0, presplit, presplit, mc, epi_mode);
+        presplit > 0 ? 1 : 0, presplit, presplit, mc, epi_mode, LU ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -1166,15 +1201,15 @@ cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int
                                 reinterpret_cast<void* const*>(C), c_off, ldc, batch, status, tmslots);
 }
 
-cudaError_t gemm_tc_lu_update(cudaStream_t st, int m, const float* const* L21, const float* const* U12, float* const* LU,
-                              long long c_off, int ldlu, int batch, const int* rowsrc, long long rs_stride,
-                              int lo_rows, unsigned* status, void* tmslots)
+cudaError_t gemm_tc_lu_update(cudaStream_t st, int m, const float* const* Aop, const float* const* Bop,
+                              float* const* C, long long c_off, int ldc, int batch, int lo_rows, unsigned* status,
+                              void* tmslots)
 {
     if (m <= 0 || batch <= 0) return cudaSuccess;
-    return tc_launch_t<TcIn::F32_TF32, TcIn::F32_TF32, GemmElem::F32, true>(
-        st, true, false, m, m, 32, -1.0f, reinterpret_cast<const void* const*>(L21), 0, 32,
-        reinterpret_cast<const void* const*>(U12), 0, 32, 1.0f, reinterpret_cast<void* const*>(LU), c_off, ldlu, batch,
-        status, tmslots, rowsrc, rs_stride, lo_rows);
+    return tc_launch_t<TcIn::F32_TF32, TcIn::F32_TF32, GemmElem::F32, true, true>(
+        st, true, false, m, m, 32, -1.0f, reinterpret_cast<const void* const*>(Aop), 0, 32,
+        reinterpret_cast<const void* const*>(Bop), 0, 32, 1.0f, reinterpret_cast<void* const*>(C), c_off, ldc, batch,
+        status, tmslots, lo_rows);
 }
 
 }  // namespace opsblas

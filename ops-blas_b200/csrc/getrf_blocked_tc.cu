@@ -2,26 +2,27 @@
 // the trailing update on the tcgen05 tensor cores.
 //
 // Used by aclblasSgetrfsRefineBatchedEx with ACLBLAS_COMPUTE_32F_FAST_TF32 when the matrix no
-// longer fits one SM's tensor memory (getrf_tmem.cu covers n <= 256). Per panel k0 = 0, 32, ...:
-//   1. lu_panel_kernel, one CTA per matrix, thread t = panel row k0 + t:
-//      * writes the previous panel's U12 (kept in scratch) into its final rows k0-32..k0-1;
+// longer fits one SM's tensor memory (getrf_tmem.cu covers n <= 256). The factorisation works on
+// the matrix stored by rows (T(i, j) at LU[j + i * ldlu]): a row is contiguous, so pivot rows,
+// interchanges and the panel's rows are whole cache lines, where by columns every row element is
+// a separate sector.
+//   0. lu_rows_in_kernel: A (by columns) into LU by rows, 32 x 32 tiles through shared memory.
+//   Per panel k0 = 0, 32, ...:
+//   1. lu_panel_kernel, one CTA per matrix, thread t = memory row k0 + t:
 //      * factors the panel (rows k0..n-1, columns k0..k0+31) in FP32 in registers with implicit
-//        pivoting (rows never move; `pos` tracks the reference's in-place order): pivot = the
-//        largest magnitude compared on the exponent and 14 mantissa bits (ties to the lowest
-//        position), multipliers by an approximate reciprocal -- the refinement absorbs both --,
-//        one CTA barrier per column; 1-based pivots in LAPACK's sequential-swap convention;
-//      * writes the factored panel at the final positions, L21 (rows below the diagonal block,
-//        K-contiguous) and U12 = L11^-1 * (the pivot rows' trailing entries) into scratch, both
-//        already split into TF32 high and low planes (plus U12 in FP32 for the final U), and the
-//        row map of the trailing block: position r's trailing data still sits in memory row
-//        src(r) (a row that left the top 32 rows for a pivot row's place keeps its data there);
-//   2. gemm_tc_lu_update: A22(r, :) = A22(src(r), :) - L21(r, :) * U12 on the tensor cores
-//      (split TF32, three products, FP32 accumulation), the four operand planes by TMA, the
-//      result added to A22 by TMA reduce-add; the few rows whose data moved are written from
-//      their source rows -- the row interchanges of the trailing block, with no swap pass;
-// and at the end lu_lgather_kernel applies each panel's later interchanges to its L columns (a
-// gather through shared memory per 32-column block). On an exactly-zero pivot the matrix stops
-// (info = column + 1); its later updates change nothing.
+//        pivoting (`pos` tracks the reference's in-place order): pivot = the largest magnitude
+//        compared on the exponent and 14 mantissa bits (ties to the lowest position), multipliers
+//        by an approximate reciprocal -- the refinement absorbs both --, one CTA barrier per
+//        column; 1-based pivots in LAPACK's sequential-swap convention;
+//      * writes the factored panel at the final positions and moves the rest of every row whose
+//        position changed (at most 64 rows: the whole-row interchanges of the reference,
+//        SwapRows, applied once per panel);
+//      * L21 (rows below the diagonal block, K-contiguous) and U12 = L11^-1 * (the pivot rows'
+//        trailing entries) into scratch as TF32 high and low planes; U12 also into its final rows;
+//   2. gemm_tc_lu_update: T22 -= L21 * U12 on the tensor cores (split TF32, three products, FP32
+//      accumulation), as the column-major product U12^T * L21^T on the by-rows storage;
+//   and lu_rows_out_kernel transposes LU in place back to columns. On an exactly-zero pivot the
+//   matrix stops (info = column + 1); its later updates change nothing.
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -35,23 +36,23 @@ struct __align__(16) BpSmem {
     float crow[2][32][kBpW];  // per column parity and warp: the warp's pivot candidate row
     unsigned ckey[2][32];     //   its key
     float l11[kBpW][kBpW + 1];
-    int prow[kBpW];           // memory row of the pivot row of U row i (position k0 + i)
+    int mv_src[2 * kBpW];     // rows whose position changed: memory row and destination row
+    int mv_dst[2 * kBpW];
+    int mv_cnt;
     int info;
 };
 
 // Scratch per matrix (byte offsets): L21 (n - 32 rows x 32, row-major) as its TF32 high plane
-// followed by its low plane; U12 (32 x (n - 32), column-major: n - 32 "rows" of 32) as high plane,
-// low plane and the FP32 values (the final U rows); the row map (n ints). A plane is
-// (n - 32) x 32 floats, so each low plane starts n - 32 rows after its high plane.
+// followed by its low plane; U12 (32 x (n - 32), column-major: n - 32 "rows" of 32) the same way.
+// A plane is (n - 32) x 32 floats, so each low plane starts n - 32 rows after its high plane.
 struct BpScratch {
-    long long plane, l21, u12, src, per_matrix;
+    long long plane, l21, u12, per_matrix;
     explicit BpScratch(int n)
     {
         plane = (long long)(n - kBpW) * kBpW * 4;
         l21 = 0;
         u12 = (2 * plane + 255) / 256 * 256;
-        src = u12 + (3 * plane + 255) / 256 * 256;
-        per_matrix = src + ((long long)n * 4 + 255) / 256 * 256;
+        per_matrix = u12 + (2 * plane + 255) / 256 * 256;
     }
 };
 
@@ -62,39 +63,83 @@ __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo)
     lo = tf32_rne(x - hi);
 }
 
+// T(i, j) = A(i, j): A by columns (lda) into LU by rows (ldt). Block = 32 x 8 threads, one
+// 32 x 32 tile (blockIdx.y) of one matrix (blockIdx.x).
+__global__ void __launch_bounds__(256)
+lu_rows_in_kernel(const float* const* __restrict__ Aarr, int lda, float* const* __restrict__ Tarr, int ldt, int n)
+{
+    __shared__ float tile[32][33];
+    const int nt = (n + 31) / 32;
+    const int i0 = (int)(blockIdx.y % nt) * 32, j0 = (int)(blockIdx.y / nt) * 32;
+    const float* A = Aarr[blockIdx.x];
+    float* T = Tarr[blockIdx.x];
+    const int x = threadIdx.x & 31, y = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = y; r < 32; r += 8)
+        if (i0 + x < n && j0 + r < n) tile[r][x] = A[(i0 + x) + (long long)(j0 + r) * lda];
+    __syncthreads();
+#pragma unroll
+    for (int r = y; r < 32; r += 8)
+        if (i0 + r < n && j0 + x < n) T[(j0 + x) + (long long)(i0 + r) * ldt] = tile[x][r];
+}
+
+// In-place transpose of the n x n storage matrix S(r, c) = LU[r + c * ld]: the by-rows factors
+// become the by-columns LU. One pair of 32 x 32 tiles (I, J), I <= J, per CTA (blockIdx.y).
+__global__ void __launch_bounds__(256)
+lu_rows_out_kernel(float* const* __restrict__ LUarr, int ld, int n)
+{
+    __shared__ float ta[32][33], tb[32][33];
+    const int nt = (n + 31) / 32;
+    int p = (int)blockIdx.y, I = 0;
+    while (p >= nt - I) {
+        p -= nt - I;
+        I++;
+    }
+    const int J = I + p;
+    float* S = LUarr[blockIdx.x];
+    const int x = threadIdx.x & 31, y = threadIdx.x >> 5;
+    const int a0 = I * 32, b0 = J * 32;
+#pragma unroll
+    for (int r = y; r < 32; r += 8) {
+        if (a0 + x < n && b0 + r < n) ta[r][x] = S[(a0 + x) + (long long)(b0 + r) * ld];  // S(a0+x, b0+r)
+        if (I != J && b0 + x < n && a0 + r < n) tb[r][x] = S[(b0 + x) + (long long)(a0 + r) * ld];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = y; r < 32; r += 8) {
+        // S'(a0 + x, b0 + r) = S(b0 + r, a0 + x) and S'(b0 + x, a0 + r) = S(a0 + r, b0 + x)
+        if (I != J && a0 + x < n && b0 + r < n) S[(a0 + x) + (long long)(b0 + r) * ld] = tb[x][r];
+        if (b0 + x < n && a0 + r < n) S[(b0 + x) + (long long)(a0 + r) * ld] = ta[x][r];
+    }
+}
+
 template <int NT>
 __global__ void __launch_bounds__(NT, 1)
-lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldlu, int k0, int* __restrict__ piv,
+lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* __restrict__ piv,
                 int* __restrict__ info, char* __restrict__ scratch, long long l21_off, long long u12_off,
-                long long src_off, long long per_matrix)
+                long long per_matrix)
 {
     constexpr int NW = NT / 32;
     __shared__ BpSmem S;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long m = blockIdx.x;
-    float* LU = LUarr[m];
+    float* T = LUarr[m];  // by rows: T(i, j) = T[j + i * ldt]
     char* base = scratch + m * per_matrix;
     float* L21 = reinterpret_cast<float*>(base + l21_off);
     float* U12 = reinterpret_cast<float*>(base + u12_off);
-    int* src = reinterpret_cast<int*>(base + src_off);
     int* pm = piv + m * n;
     const int mp = n - k0;                      // panel rows
     const int pw = mp < kBpW ? mp : kBpW;       // panel columns
     const int ntr = n - k0 - kBpW;              // trailing rows and columns
     const long long lo = (long long)(n - kBpW) * kBpW;  // floats from a high plane to its low plane
     const int inf0 = info[m];
+    // whole rows as float4 when every row start is 16-byte aligned (uniform per matrix)
+    const bool vec = (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (ldt & 3) == 0 && pw == kBpW;
 
-    // 1. the previous panel's U12 (FP32 plane) into its final rows (k0 - 32 .. k0 - 1, columns
-    //    k0 .. n - 1)
-    if (k0 > 0 && inf0 == 0) {
-        const int cols = n - k0;
-        for (int e = tid; e < cols * kBpW; e += NT) {
-            const int j = e / kBpW, i = e % kBpW;
-            LU[(k0 - kBpW + i) + (long long)(k0 + j) * ldlu] = U12[2 * lo + j * kBpW + i];
-        }
+    if (tid == 0) {
+        S.info = inf0;
+        S.mv_cnt = 0;
     }
-    if (tid == 0) S.info = inf0;
-    __syncthreads();
     if (inf0 != 0) {  // stopped at an earlier zero pivot: this step's update must change nothing
         for (int e = tid; e < (ntr > 0 ? ntr : 0) * kBpW; e += NT) {
             L21[e] = 0.0f;
@@ -102,18 +147,35 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldlu, int k0, int* 
             U12[e] = 0.0f;
             U12[lo + e] = 0.0f;
         }
-        for (int r = tid; r < ntr; r += NT) src[r] = r;
         return;
     }
 
-    // 2. the panel row of this thread (zeros outside the matrix)
+    // 1. the panel row of this thread (zeros outside the matrix)
     const bool valid = tid < mp;
     float p[kBpW];
 #pragma unroll
-    for (int c = 0; c < kBpW; c++) p[c] = (valid && c < pw) ? LU[(k0 + tid) + (long long)(k0 + c) * ldlu] : 0.0f;
+    for (int c = 0; c < kBpW; c++) p[c] = 0.0f;
+    if (valid) {
+        const float* row = T + (long long)(k0 + tid) * ldt + k0;
+        if (vec) {
+#pragma unroll
+            for (int q = 0; q < kBpW / 4; q++) {
+                const float4 v = reinterpret_cast<const float4*>(row)[q];
+                p[4 * q] = v.x;
+                p[4 * q + 1] = v.y;
+                p[4 * q + 2] = v.z;
+                p[4 * q + 3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < kBpW; c++)
+                if (c < pw) p[c] = row[c];
+        }
+    }
     int pos = k0 + tid;
+    __syncthreads();
 
-    // 3. factor, one CTA barrier per column
+    // 2. factor, one CTA barrier per column
     int done = pw;
 #pragma unroll
     for (int c = 0; c < kBpW; c++) {
@@ -163,15 +225,26 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldlu, int k0, int* 
     }
     const bool stopped = done < pw;
 
-    // 4. the panel at its final positions
+    // 3. the panel at its final rows; L21 (zero after a stop: the update then changes nothing) and
+    //    L11; the rows whose position changed
     if (valid) {
+        float* row = T + (long long)pos * ldt + k0;
+        if (vec) {
 #pragma unroll
-        for (int c = 0; c < kBpW; c++)
-            if (c < pw) LU[pos + (long long)(k0 + c) * ldlu] = p[c];
+            for (int q = 0; q < kBpW / 4; q++)
+                reinterpret_cast<float4*>(row)[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (int c = 0; c < kBpW; c++)
+                if (c < pw) row[c] = p[c];
+        }
+        if (pos != k0 + tid) {
+            const int q = atomicAdd(&S.mv_cnt, 1);
+            S.mv_src[q] = k0 + tid;
+            S.mv_dst[q] = pos;
+        }
     }
-    if (ntr <= 0) return;  // last panel: no trailing block
-    // 5. L21 (zero after a stop: the update then changes nothing), the row map, L11 and pivot rows
-    if (valid && pos >= k0 + kBpW) {
+    if (ntr > 0 && valid && pos >= k0 + kBpW) {
         float4* dh = reinterpret_cast<float4*>(L21 + (long long)(pos - k0 - kBpW) * kBpW);
         float4* dl = reinterpret_cast<float4*>(L21 + lo + (long long)(pos - k0 - kBpW) * kBpW);
 #pragma unroll
@@ -182,29 +255,57 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldlu, int k0, int* 
             dh[q] = make_float4(h[0], h[1], h[2], h[3]);
             dl[q] = make_float4(l[0], l[1], l[2], l[3]);
         }
-        src[pos - k0 - kBpW] = stopped ? pos - k0 - kBpW : tid - kBpW;
     }
     if (valid && pos < k0 + kBpW) {
-        const int i = pos - k0;
-        S.prow[i] = k0 + tid;
 #pragma unroll
-        for (int c = 0; c < kBpW; c++) S.l11[i][c] = p[c];
+        for (int c = 0; c < kBpW; c++) S.l11[pos - k0][c] = p[c];
     }
     __syncthreads();
-    // 6. U12 = L11^-1 * (the pivot rows' trailing entries), one thread per trailing column
+
+    // 4. the rest of each moved row (columns 0..k0-1 and k0+pw..n-1) to its destination row, 64
+    //    columns a round: every value of a round is read before any is written (the moves form
+    //    cycles)
+    const int cnt = S.mv_cnt;
+    if (cnt > 0) {
+        constexpr int EPT = 64 * 2 * kBpW / NT;  // elements a thread a round (64 rows x 64 columns)
+        const int nx = n - pw;                   // columns outside the panel
+        for (int x0 = 0; x0 < nx; x0 += 64) {
+            float v[EPT];
+#pragma unroll
+            for (int u = 0; u < EPT; u++) {
+                const int e = tid + u * NT, r = e >> 6, xc = x0 + (e & 63);
+                v[u] = 0.0f;
+                if (r < cnt && xc < nx) v[u] = T[(long long)S.mv_src[r] * ldt + (xc < k0 ? xc : xc + pw)];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < EPT; u++) {
+                const int e = tid + u * NT, r = e >> 6, xc = x0 + (e & 63);
+                if (r < cnt && xc < nx) T[(long long)S.mv_dst[r] * ldt + (xc < k0 ? xc : xc + pw)] = v[u];
+            }
+            __syncthreads();
+        }
+    }
+    if (ntr <= 0) return;  // last panel: no trailing block
+
+    // 5. U12 = L11^-1 * (the pivot rows' trailing entries, now in rows k0..k0+31), one thread per
+    //    trailing column: the final U rows, and the TF32 planes of the update
     for (int jj = tid; jj < ntr; jj += NT) {
-        const long long col = (long long)(k0 + kBpW + jj) * ldlu;
+        const int col = k0 + kBpW + jj;
         float u[kBpW];
 #pragma unroll
-        for (int i = 0; i < kBpW; i++) u[i] = stopped ? 0.0f : LU[S.prow[i] + col];
+        for (int i = 0; i < kBpW; i++) u[i] = stopped ? 0.0f : T[(long long)(k0 + i) * ldt + col];
 #pragma unroll
         for (int i = 1; i < kBpW; i++)
 #pragma unroll
             for (int c = 0; c < kBpW; c++)
                 if (c < i) u[i] = fmaf(-S.l11[i][c], u[c], u[i]);
+        if (!stopped) {
+#pragma unroll
+            for (int i = 0; i < kBpW; i++) T[(long long)(k0 + i) * ldt + col] = u[i];
+        }
         float4* dh = reinterpret_cast<float4*>(U12 + (long long)jj * kBpW);
         float4* dl = reinterpret_cast<float4*>(U12 + lo + (long long)jj * kBpW);
-        float4* df = reinterpret_cast<float4*>(U12 + 2 * lo + (long long)jj * kBpW);
 #pragma unroll
         for (int q = 0; q < kBpW / 4; q++) {
             float h[4], l[4];
@@ -212,50 +313,6 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldlu, int k0, int* 
             for (int e = 0; e < 4; e++) tf32_split(u[4 * q + e], h[e], l[e]);
             dh[q] = make_float4(h[0], h[1], h[2], h[3]);
             dl[q] = make_float4(l[0], l[1], l[2], l[3]);
-            df[q] = make_float4(u[4 * q], u[4 * q + 1], u[4 * q + 2], u[4 * q + 3]);
-        }
-    }
-}
-
-// After the last panel: the rows of each 32-column block below its diagonal block take their
-// final order. The interchanges of the later panels (applied to every column by the reference's
-// whole-row swaps) are traced back from each final position i to the position that held the row
-// when the block was factored (undoing each later panel's swaps in reverse), and the block is
-// gathered through shared memory. One CTA per matrix, thread = row (up to 1024 rows).
-__global__ void __launch_bounds__(1024, 1)
-lu_lgather_kernel(float* const* __restrict__ LUarr, int n, int ldlu, const int* __restrict__ piv)
-{
-    extern __shared__ float blk[];  // (n - 32) x 32, row i - 32 (p + 1) at blk[... * 33]
-    const int tid = threadIdx.x;
-    const long long m = blockIdx.x;
-    float* LU = LUarr[m];
-    const int* pm = piv + m * n;
-    const int P = (n + kBpW - 1) / kBpW;
-    int pos = tid;  // for row tid: where its row sat after panel p
-    for (int p = P - 2; p >= 0; p--) {
-        // undo panel p + 1's interchanges (in reverse order)
-        const int s0 = (p + 1) * kBpW;
-        const int s1 = min(n, s0 + kBpW);
-        for (int k = s1 - 1; k >= s0; k--) {
-            const int r = pm[k] - 1;
-            if (r < 0 || r == k) continue;  // no interchange (after a stop the pivots are 0)
-            if (pos == k)
-                pos = r;
-            else if (pos == r)
-                pos = k;
-        }
-        const int r0 = (p + 1) * kBpW;  // first row below block p's diagonal block
-        const int rows = n - r0;
-        const int c0 = p * kBpW;
-        __syncthreads();
-        if (tid >= r0 && tid < n) {
-#pragma unroll 4
-            for (int c = 0; c < kBpW; c++) blk[(tid - r0) * (kBpW + 1) + c] = LU[pos + (long long)(c0 + c) * ldlu];
-        }
-        __syncthreads();
-        for (int e = tid; e < rows * kBpW; e += blockDim.x) {
-            const int c = e / rows, i = e % rows;  // coalesced along the column
-            LU[(r0 + i) + (long long)(c0 + c) * ldlu] = blk[i * (kBpW + 1) + c];
         }
     }
 }
@@ -267,8 +324,9 @@ size_t getrf_blocked_tc_scratch_bytes(int n, int batch)
     return (size_t)BpScratch(n).per_matrix * (size_t)batch + (size_t)batch * 16 + 512;
 }
 
-cudaError_t getrf_blocked_tc_launch(cudaStream_t st, float* const* LUarray, int n, int ldlu, int* piv, int* info,
-                                    int batch, void* scratch, unsigned* status, void* tmslots)
+cudaError_t getrf_blocked_tc_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
+                                    int ldlu, int* piv, int* info, int batch, void* scratch, unsigned* status,
+                                    void* tmslots)
 {
     if (!getrf_blocked_tc_supported(n) || batch <= 0) return cudaErrorInvalidValue;
     const BpScratch L(n);
@@ -283,27 +341,26 @@ cudaError_t getrf_blocked_tc_launch(cudaStream_t st, float* const* LUarray, int 
                                                  L.per_matrix / 4, batch);
     init_ptr_array_kernel<<<bgrid, 256, 0, st>>>(u12p, reinterpret_cast<float*>(base + L.u12),
                                                  L.per_matrix / 4, batch);
-    const int* srcmap = reinterpret_cast<const int*>(base + L.src);
+    const int nt = (n + 31) / 32;
+    lu_rows_in_kernel<<<dim3((unsigned)batch, (unsigned)(nt * nt)), 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n);
     for (int k0 = 0; k0 < n; k0 += kBpW) {
         if (n - k0 <= 512)
             lu_panel_kernel<512><<<(unsigned)batch, 512, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21, L.u12,
-                                                                  L.src, L.per_matrix);
+                                                                  L.per_matrix);
         else
             lu_panel_kernel<1024><<<(unsigned)batch, 1024, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
-                                                                    L.u12, L.src, L.per_matrix);
+                                                                    L.u12, L.per_matrix);
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
         const int mt = n - k0 - kBpW;
         if (mt > 0) {
-            err = gemm_tc_lu_update(st, mt, l21p, u12p, LUarray, (long long)(k0 + kBpW) * (1 + (long long)ldlu), ldlu,
-                                    batch, srcmap, L.per_matrix / 4, n - kBpW, status, tmslots);
+            // by rows T22 -= L21 * U12 is, on the storage, C -= U12^T * L21^T (m x m, K = 32)
+            err = gemm_tc_lu_update(st, mt, u12p, l21p, LUarray, (long long)(k0 + kBpW) * (1 + (long long)ldlu), ldlu,
+                                    batch, n - kBpW, status, tmslots);
             if (err != cudaSuccess) return err;
         }
     }
-    const size_t gsm = (size_t)(n - kBpW) * (kBpW + 1) * 4;
-    err = ensure_smem_limit(lu_lgather_kernel, (int)gsm);
-    if (err != cudaSuccess) return err;
-    lu_lgather_kernel<<<(unsigned)batch, 1024, gsm, st>>>(LUarray, n, ldlu, piv);
+    lu_rows_out_kernel<<<dim3((unsigned)batch, (unsigned)(nt * (nt + 1) / 2)), 256, 0, st>>>(LUarray, ldlu, n);
     return cudaGetLastError();
 }
 

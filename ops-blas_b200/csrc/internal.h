@@ -112,25 +112,26 @@ cudaError_t gemm_tc_launch(cudaStream_t st, bool transA, bool transB, int m, int
                            int ldb, float beta, float* const* C, long long c_off, int ldc, int batch, int split,
                            unsigned* status, void* tmslots);
 
-// Trailing update of the blocked mixed-precision LU: for every matrix b, the m x m block of LU[b]
-// at element offset c_off (leading dimension ldlu) becomes C(src(r), j) - L21[b](r, :) * U12[b](:, j)
-// with split-TF32 tensor-core products; L21 is m x 32 row-major, U12 32 x m column-major (both
-// with leading dimension 32), each given as its TF32 high plane followed, lo_rows rows further,
-// by its low plane; src(r) = rowsrc[b * rs_stride + r] (relative to the block's first row).
-cudaError_t gemm_tc_lu_update(cudaStream_t st, int m, const float* const* L21, const float* const* U12,
-                              float* const* LU, long long c_off, int ldlu, int batch, const int* rowsrc,
-                              long long rs_stride, int lo_rows, unsigned* status, void* tmslots);
+// Trailing update of the blocked mixed-precision LU: for every matrix b, the m x m block of C[b] at
+// element offset c_off (column-major, leading dimension ldc) becomes
+// C(r, c) - sum_k Aop[b][k + 32 r] * Bop[b][k + 32 c] with split-TF32 tensor-core products; Aop
+// and Bop hold 32 K-contiguous values per row or column (leading dimension 32), each given as its
+// TF32 high plane followed, lo_rows rows further, by its low plane.
+cudaError_t gemm_tc_lu_update(cudaStream_t st, int m, const float* const* Aop, const float* const* Bop,
+                              float* const* C, long long c_off, int ldc, int batch, int lo_rows, unsigned* status,
+                              void* tmslots);
 
 // refine.cu: out[i] = base + i * stride (floats), i < count.
 __global__ void init_ptr_array_kernel(float** out, float* base, long long stride, int count);
 
 // getrf_blocked_tc.cu: 256 < n <= 1024, blocked mixed-precision LU (FP32 panels, split-TF32
-// tensor-core trailing update) in place on LU; scratch: getrf_blocked_tc_scratch_bytes(n, batch)
-// bytes of device memory (256-byte aligned).
+// tensor-core trailing update): reads A (lda), writes the factors to LU (ldlu; LU must not overlap
+// A); scratch: getrf_blocked_tc_scratch_bytes(n, batch) bytes of device memory (256-byte aligned).
 bool getrf_blocked_tc_supported(int n);
 size_t getrf_blocked_tc_scratch_bytes(int n, int batch);
-cudaError_t getrf_blocked_tc_launch(cudaStream_t st, float* const* LUarray, int n, int ldlu, int* piv, int* info,
-                                    int batch, void* scratch, unsigned* status, void* tmslots);
+cudaError_t getrf_blocked_tc_launch(cudaStream_t st, const float* const* Aarray, int lda, float* const* LUarray, int n,
+                                    int ldlu, int* piv, int* info, int batch, void* scratch, unsigned* status,
+                                    void* tmslots);
 
 // getrf_tmem.cu: 32 < n <= 256, mixed-precision LU with the matrix resident in TMEM.
 bool getrf_tmem_supported(int n);

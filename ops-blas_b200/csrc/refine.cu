@@ -253,15 +253,15 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     fill_int_kernel<<<bgrid, 256, 0, st>>>(done, 0, batchCount);
     fill_int_kernel<<<bgrid, 256, 0, st>>>(iterArray, maxIter, batchCount);
     const bool tmem = mode != 0 && getrf_tmem_supported(n);  // reads A, writes LU: no copy
-    if (!tmem) copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
+    if (!tmem && !blocked) copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
         err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode,
                                 handle->dstatus);
-    } else if (blocked) {
-        err = getrf_blocked_tc_launch(st, LUarray, n, ldlu, PivotArray, infoArray, batchCount, ws + bt_off,
-                                      handle->dstatus, handle->tmslots);
+    } else if (blocked) {  // reads A, writes LU
+        err = getrf_blocked_tc_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount,
+                                      ws + bt_off, handle->dstatus, handle->tmslots);
     } else {  // plain FP32 factors: the batched getrf's kernels
         aclblasStatus_t s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;
