@@ -8,7 +8,7 @@
 // a separate sector.
 //   0. lu_rows_in_kernel: A (by columns) into LU by rows, 32 x 32 tiles through shared memory.
 //   Per panel k0 = 0, 32, ...:
-//   1. lu_panel_kernel, one CTA per matrix, thread t = memory row k0 + t:
+//   1. lu_panel_kernel, one CTA per matrix, a thread per panel row (two above 256 rows):
 //      * factors the panel (rows k0..n-1, columns k0..k0+31) in FP32 in registers with implicit
 //        pivoting (`pos` tracks the reference's in-place order): pivot = the largest magnitude
 //        compared on the exponent and 14 mantissa bits (ties to the lowest position), multipliers
@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include "internal.h"
+#include "small_common.cuh"
 #include "tc_common.cuh"
 
 namespace opsblas {
@@ -113,14 +114,20 @@ lu_rows_out_kernel(float* const* __restrict__ LUarr, int ld, int n)
     }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 1)
+// Rows moved a round by the panel kernel's interchange step: 64 rows x 128 columns.
+constexpr int kMvCols = 128;
+
+// One CTA per matrix; thread t holds memory rows k0 + t + r * NT (r < RPT) of the panel. NT x RPT
+// covers the panel's rows; 128 registers a thread, so that 512 / NT CTAs share an SM.
+template <int NT, int RPT>
+__global__ void __launch_bounds__(NT, 512 / NT)
 lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* __restrict__ piv,
                 int* __restrict__ info, char* __restrict__ scratch, long long l21_off, long long u12_off,
                 long long per_matrix)
 {
     constexpr int NW = NT / 32;
     __shared__ BpSmem S;
+    __shared__ __align__(16) float mvbuf[2 * kBpW * kMvCols];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long m = blockIdx.x;
     float* T = LUarr[m];  // by rows: T(i, j) = T[j + i * ldt]
@@ -150,29 +157,34 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
         return;
     }
 
-    // 1. the panel row of this thread (zeros outside the matrix)
-    const bool valid = tid < mp;
-    float p[kBpW];
+    // 1. this thread's panel rows (zeros outside the matrix)
+    bool valid[RPT];
+    int pos[RPT];
+    float p[RPT][kBpW];
 #pragma unroll
-    for (int c = 0; c < kBpW; c++) p[c] = 0.0f;
-    if (valid) {
-        const float* row = T + (long long)(k0 + tid) * ldt + k0;
-        if (vec) {
+    for (int r = 0; r < RPT; r++) {
+        valid[r] = tid + r * NT < mp;
+        pos[r] = k0 + tid + r * NT;
 #pragma unroll
-            for (int q = 0; q < kBpW / 4; q++) {
-                const float4 v = reinterpret_cast<const float4*>(row)[q];
-                p[4 * q] = v.x;
-                p[4 * q + 1] = v.y;
-                p[4 * q + 2] = v.z;
-                p[4 * q + 3] = v.w;
+        for (int c = 0; c < kBpW; c++) p[r][c] = 0.0f;
+        if (valid[r]) {
+            const float* row = T + (long long)pos[r] * ldt + k0;
+            if (vec) {
+#pragma unroll
+                for (int q = 0; q < kBpW / 4; q++) {
+                    const float4 v = reinterpret_cast<const float4*>(row)[q];
+                    p[r][4 * q] = v.x;
+                    p[r][4 * q + 1] = v.y;
+                    p[r][4 * q + 2] = v.z;
+                    p[r][4 * q + 3] = v.w;
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < kBpW; c++)
+                    if (c < pw) p[r][c] = row[c];
             }
-        } else {
-#pragma unroll
-            for (int c = 0; c < kBpW; c++)
-                if (c < pw) p[c] = row[c];
         }
     }
-    int pos = k0 + tid;
     __syncthreads();
 
     // 2. factor, one CTA barrier per column
@@ -182,16 +194,30 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
         if (c >= pw) break;
         const int k = k0 + c;
         const int buf = c & 1;
-        const bool elig = valid && pos >= k;
-        const float av = fabsf(p[c]);
-        const unsigned mag = (av == av) ? (__float_as_uint(av) >> 9) : 0u;  // NaN never wins
-        const unsigned key = elig ? ((mag << 10) | (1023u - (unsigned)(pos - k0))) : 0u;
-        const unsigned wkey = __reduce_max_sync(0xffffffffu, key);
+        unsigned best = 0u;  // this thread's best candidate key (0: none)
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const float av = fabsf(p[r][c]);
+            const unsigned mag = (av == av) ? (__float_as_uint(av) >> 9) : 0u;  // NaN never wins
+            const unsigned key = (valid[r] && pos[r] >= k) ? ((mag << 10) | (1023u - (unsigned)(pos[r] - k0))) : 0u;
+            best = key > best ? key : best;
+        }
+        const unsigned wkey = __reduce_max_sync(0xffffffffu, best);
         if (lane == 0) S.ckey[buf][warp] = wkey;
-        if (elig && key == wkey) {
+        if (best != 0u && best == wkey) {  // keys are unique: one writer a warp
             float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
 #pragma unroll
-            for (int q = 0; q < kBpW / 4; q++) dst[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
+            for (int r = 0; r < RPT; r++) {
+                const float av = fabsf(p[r][c]);
+                const unsigned mag = (av == av) ? (__float_as_uint(av) >> 9) : 0u;
+                const unsigned key =
+                    (valid[r] && pos[r] >= k) ? ((mag << 10) | (1023u - (unsigned)(pos[r] - k0))) : 0u;
+                if (key == best) {
+#pragma unroll
+                    for (int q = 0; q < kBpW / 4; q++)
+                        dst[q] = make_float4(p[r][4 * q], p[r][4 * q + 1], p[r][4 * q + 2], p[r][4 * q + 3]);
+                }
+            }
         }
         __syncthreads();
         const unsigned qk = lane < NW ? S.ckey[buf][lane] : 0u;
@@ -209,79 +235,106 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
             done = c;
             break;
         }
-        if (pos == ppos)
-            pos = k;
-        else if (pos == k)
-            pos = ppos;
-        if (valid && pos > k) {
-            float rinv;
-            asm("rcp.approx.f32 %0, %1;" : "=f"(rinv) : "f"(pv));
-            const float l = p[c] * rinv;
-            p[c] = l;
+        float rinv;
+        asm("rcp.approx.f32 %0, %1;" : "=f"(rinv) : "f"(pv));
+        float l[RPT];
+        bool upd[RPT];  // rows below the pivot position take the update
 #pragma unroll
-            for (int j = 0; j < kBpW; j++)
-                if (j > c) p[j] = fmaf(-l, prow[j], p[j]);
+        for (int r = 0; r < RPT; r++) {
+            if (pos[r] == ppos)
+                pos[r] = k;
+            else if (pos[r] == k)
+                pos[r] = ppos;
+            upd[r] = valid[r] && pos[r] > k;
+            l[r] = p[r][c] * rinv;
+            if (upd[r]) p[r][c] = l[r];
+        }
+#pragma unroll
+        for (int j = 0; j < kBpW; j++) {
+            if (j > c) {
+                const float u = prow[j];
+#pragma unroll
+                for (int r = 0; r < RPT; r++)
+                    if (upd[r]) p[r][j] = fmaf(-l[r], u, p[r][j]);
+            }
         }
     }
     const bool stopped = done < pw;
 
     // 3. the panel at its final rows; L21 (zero after a stop: the update then changes nothing) and
     //    L11; the rows whose position changed
-    if (valid) {
-        float* row = T + (long long)pos * ldt + k0;
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+        if (!valid[r]) continue;
+        float* row = T + (long long)pos[r] * ldt + k0;
         if (vec) {
 #pragma unroll
             for (int q = 0; q < kBpW / 4; q++)
-                reinterpret_cast<float4*>(row)[q] = make_float4(p[4 * q], p[4 * q + 1], p[4 * q + 2], p[4 * q + 3]);
+                reinterpret_cast<float4*>(row)[q] =
+                    make_float4(p[r][4 * q], p[r][4 * q + 1], p[r][4 * q + 2], p[r][4 * q + 3]);
         } else {
 #pragma unroll
             for (int c = 0; c < kBpW; c++)
-                if (c < pw) row[c] = p[c];
+                if (c < pw) row[c] = p[r][c];
         }
-        if (pos != k0 + tid) {
+        if (pos[r] != k0 + tid + r * NT) {
             const int q = atomicAdd(&S.mv_cnt, 1);
-            S.mv_src[q] = k0 + tid;
-            S.mv_dst[q] = pos;
+            S.mv_src[q] = k0 + tid + r * NT;
+            S.mv_dst[q] = pos[r];
         }
-    }
-    if (ntr > 0 && valid && pos >= k0 + kBpW) {
-        float4* dh = reinterpret_cast<float4*>(L21 + (long long)(pos - k0 - kBpW) * kBpW);
-        float4* dl = reinterpret_cast<float4*>(L21 + lo + (long long)(pos - k0 - kBpW) * kBpW);
+        if (ntr > 0 && pos[r] >= k0 + kBpW) {
+            float4* dh = reinterpret_cast<float4*>(L21 + (long long)(pos[r] - k0 - kBpW) * kBpW);
+            float4* dl = reinterpret_cast<float4*>(L21 + lo + (long long)(pos[r] - k0 - kBpW) * kBpW);
 #pragma unroll
-        for (int q = 0; q < kBpW / 4; q++) {
-            float h[4], l[4];
+            for (int q = 0; q < kBpW / 4; q++) {
+                float h[4], lw[4];
 #pragma unroll
-            for (int e = 0; e < 4; e++) tf32_split(stopped ? 0.0f : p[4 * q + e], h[e], l[e]);
-            dh[q] = make_float4(h[0], h[1], h[2], h[3]);
-            dl[q] = make_float4(l[0], l[1], l[2], l[3]);
+                for (int e = 0; e < 4; e++) tf32_split(stopped ? 0.0f : p[r][4 * q + e], h[e], lw[e]);
+                dh[q] = make_float4(h[0], h[1], h[2], h[3]);
+                dl[q] = make_float4(lw[0], lw[1], lw[2], lw[3]);
+            }
         }
-    }
-    if (valid && pos < k0 + kBpW) {
+        if (pos[r] < k0 + kBpW) {
 #pragma unroll
-        for (int c = 0; c < kBpW; c++) S.l11[pos - k0][c] = p[c];
+            for (int c = 0; c < kBpW; c++) S.l11[pos[r] - k0][c] = p[r][c];
+        }
     }
     __syncthreads();
 
-    // 4. the rest of each moved row (columns 0..k0-1 and k0+pw..n-1) to its destination row, 64
-    //    columns a round: every value of a round is read before any is written (the moves form
-    //    cycles)
-    const int cnt = S.mv_cnt;
+    // 4. the rest of each moved row (columns 0..k0-1 and k0+pw..n-1) to its destination row,
+    //    kMvCols columns a round staged in shared memory by cp.async: a round reads all its values
+    //    before any is written (the moves form cycles)
+    const int cnt = S.mv_cnt;  // <= 64: each of the panel's interchanges moves two rows
     if (cnt > 0) {
-        constexpr int EPT = 64 * 2 * kBpW / NT;  // elements a thread a round (64 rows x 64 columns)
-        const int nx = n - pw;                   // columns outside the panel
-        for (int x0 = 0; x0 < nx; x0 += 64) {
-            float v[EPT];
+        const int nx = n - pw;  // columns outside the panel
+        auto col_of = [&](int x) { return x < k0 ? x : x + pw; };
+        for (int x0 = 0; x0 < nx; x0 += kMvCols) {
+            for (int e = tid; e < cnt * (kMvCols / 4); e += NT) {
+                const int r = e / (kMvCols / 4), xq = x0 + (e % (kMvCols / 4)) * 4;
+                float* d = mvbuf + r * kMvCols + (xq - x0);
+                const float* srow = T + (long long)S.mv_src[r] * ldt;
+                if (vec && xq + 3 < nx) {
+                    cp_async16(d, srow + col_of(xq));  // four columns on the same side of the panel
+                } else {
 #pragma unroll
-            for (int u = 0; u < EPT; u++) {
-                const int e = tid + u * NT, r = e >> 6, xc = x0 + (e & 63);
-                v[u] = 0.0f;
-                if (r < cnt && xc < nx) v[u] = T[(long long)S.mv_src[r] * ldt + (xc < k0 ? xc : xc + pw)];
+                    for (int u = 0; u < 4; u++)
+                        if (xq + u < nx) cp_async4(d + u, srow + col_of(xq + u));
+                }
             }
+            cp_async_commit();
+            cp_async_wait_all();
             __syncthreads();
+            for (int e = tid; e < cnt * (kMvCols / 4); e += NT) {
+                const int r = e / (kMvCols / 4), xq = x0 + (e % (kMvCols / 4)) * 4;
+                const float* sv = mvbuf + r * kMvCols + (xq - x0);
+                float* drow = T + (long long)S.mv_dst[r] * ldt;
+                if (vec && xq + 3 < nx) {
+                    *reinterpret_cast<float4*>(drow + col_of(xq)) = *reinterpret_cast<const float4*>(sv);
+                } else {
 #pragma unroll
-            for (int u = 0; u < EPT; u++) {
-                const int e = tid + u * NT, r = e >> 6, xc = x0 + (e & 63);
-                if (r < cnt && xc < nx) T[(long long)S.mv_dst[r] * ldt + (xc < k0 ? xc : xc + pw)] = v[u];
+                    for (int u = 0; u < 4; u++)
+                        if (xq + u < nx) drow[col_of(xq + u)] = sv[u];
+                }
             }
             __syncthreads();
         }
@@ -308,11 +361,11 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
         float4* dl = reinterpret_cast<float4*>(U12 + lo + (long long)jj * kBpW);
 #pragma unroll
         for (int q = 0; q < kBpW / 4; q++) {
-            float h[4], l[4];
+            float h[4], lw[4];
 #pragma unroll
-            for (int e = 0; e < 4; e++) tf32_split(u[4 * q + e], h[e], l[e]);
+            for (int e = 0; e < 4; e++) tf32_split(u[4 * q + e], h[e], lw[e]);
             dh[q] = make_float4(h[0], h[1], h[2], h[3]);
-            dl[q] = make_float4(l[0], l[1], l[2], l[3]);
+            dl[q] = make_float4(lw[0], lw[1], lw[2], lw[3]);
         }
     }
 }
@@ -344,12 +397,20 @@ cudaError_t getrf_blocked_tc_launch(cudaStream_t st, const float* const* Aarray,
     const int nt = (n + 31) / 32;
     lu_rows_in_kernel<<<dim3((unsigned)batch, (unsigned)(nt * nt)), 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n);
     for (int k0 = 0; k0 < n; k0 += kBpW) {
-        if (n - k0 <= 512)
-            lu_panel_kernel<512><<<(unsigned)batch, 512, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21, L.u12,
-                                                                  L.per_matrix);
+        // the CTA shape by panel rows: small CTAs share an SM, two rows a thread above 256
+        const int mp = n - k0;
+        if (mp <= 128)
+            lu_panel_kernel<128, 1><<<(unsigned)batch, 128, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
+                                                                     L.u12, L.per_matrix);
+        else if (mp <= 256)
+            lu_panel_kernel<256, 1><<<(unsigned)batch, 256, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
+                                                                     L.u12, L.per_matrix);
+        else if (mp <= 512)
+            lu_panel_kernel<256, 2><<<(unsigned)batch, 256, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
+                                                                     L.u12, L.per_matrix);
         else
-            lu_panel_kernel<1024><<<(unsigned)batch, 1024, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
-                                                                    L.u12, L.per_matrix);
+            lu_panel_kernel<512, 2><<<(unsigned)batch, 512, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
+                                                                     L.u12, L.per_matrix);
         err = cudaGetLastError();
         if (err != cudaSuccess) return err;
         const int mt = n - k0 - kBpW;
