@@ -643,7 +643,7 @@ def run_section(args):
     elif args.section == "grouped":
         out = section_grouped(ob, h, dev, peak, reps=2, instances=5000 if args.small else 50000)
     elif args.section == "mixed":
-        out = section_mixed(ob, h, dev, reps=2, sizes=((256, 148), (512, 32)) if args.small else ((256, 2048), (512, 256)))
+        out = section_mixed(ob, h, dev, reps=2, sizes=((256, 148), (512, 160)) if args.small else ((256, 2048), (512, 256)))
     elif args.section == "gels":
         out = section_gels(ob, h, dev, peak, reps=2, batch=16384 if args.small else 65536)
     elif args.section == "geqrf":
