@@ -236,7 +236,9 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
  * leaves the handle workspace alone. Its scratch is a fixed array of
  * ACLBLAS_REFINE_STATIC_SCRATCH_BYTES in the library's device image, one per device; a call
  * needs (n*nrhs*4 rounded up to 256 + 20) * batchCount + 512 bytes of it, and a larger request
- * returns ACLBLAS_STATUS_INVALID_VALUE without launching anything. The first call on each device
+ * returns ACLBLAS_STATUS_INVALID_VALUE without launching anything. With _FAST_TF32 and
+ * 256 < n <= 1024 the factorization is blocked when the rest of the scratch holds the blocked LU's
+ * part (as aclblasSgetrfsRefineBatchedEx decides with its workspace), else plain FP32. The first call on each device
  * (with the handle's device current) sets up the scratch address; make it before any stream
  * capture. The address is kept for the life of the process, so the entry point must not be used
  * on a device after a cudaDeviceReset of that device. The scratch is shared by all handles and streams of the process: calls that overlap

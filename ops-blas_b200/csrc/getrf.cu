@@ -8,8 +8,11 @@
 // (:127-137). The B200 kernels are:
 //   n <= 32 : getrf_small_kernel, one warp segment per matrix, rows in registers;
 //   32 < n <= 128 : getrf_reg_kernel (getrf_reg.cu), matrix in registers across the CTA;
-//   128 < n <= 640 : getrf_large_kernel (getrf_large.cu), blocked, matrix in global memory;
-//   n  > 640 : getrf_generic_kernel, one CTA per matrix, unblocked in global memory.
+//   128 < n <= 1024 : the blocked LU on a by-rows copy made in place (getrf_blocked_tc.cu:
+//                     panel kernels and a tiled trailing update), given 4 bytes of handle
+//                     workspace per matrix; without them getrf_large_kernel (getrf_large.cu,
+//                     n <= 640, blocked, one CTA per matrix in global memory);
+//   otherwise : getrf_generic_kernel, one CTA per matrix, unblocked in global memory.
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -156,8 +159,10 @@ getrf_generic_kernel(float* const* __restrict__ Aarray, int n, int lda, int* __r
 
 using namespace opsblas;
 
-extern "C" aclblasStatus_t aclblasSgetrfBatched(
-    aclblasHandle_t handle, int n, float* const Aarray[], int lda, int* PivotArray, int* infoArray, int batchSize)
+// The body of aclblasSgetrfBatched; stat: batchSize ints of device scratch for the blocked path
+// (nullptr: that path is not taken).
+aclblasStatus_t opsblas::getrf_batched_impl(aclblasHandle_t handle, int n, float* const Aarray[], int lda,
+                                            int* PivotArray, int* infoArray, int batchSize, int* stat)
 {
     static const char* kApi = "aclblasSgetrfBatched";
     if (handle == nullptr) {
@@ -220,6 +225,8 @@ extern "C" aclblasStatus_t aclblasSgetrfBatched(
         reg_default_shape(n, rows, warps);
         return launch_status(kApi, getrf_reg_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize, rows,
                                                     warps));
+    } else if (getrf_rows_supported(n) && stat != nullptr) {
+        return launch_status(kApi, getrf_rows_launch(st, Aarray, n, lda, PivotArray, infoArray, stat, batchSize));
     } else if (getrf_large_supported(n)) {
         return launch_status(kApi, getrf_large_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize));
     } else {
@@ -231,4 +238,15 @@ extern "C" aclblasStatus_t aclblasSgetrfBatched(
                                                                                        infoArray);
     }
     return launch_status(kApi, cudaGetLastError());
+}
+
+extern "C" aclblasStatus_t aclblasSgetrfBatched(
+    aclblasHandle_t handle, int n, float* const Aarray[], int lda, int* PivotArray, int* infoArray, int batchSize)
+{
+    // the blocked path keeps the matrices' stop codes in the first 4 * batchSize workspace bytes
+    int* stat = nullptr;
+    if (handle != nullptr && batchSize > 0 && handle->workspace != nullptr &&
+        handle->workspace_size >= sizeof(int) * (size_t)batchSize)
+        stat = static_cast<int*>(handle->workspace);
+    return getrf_batched_impl(handle, n, Aarray, lda, PivotArray, infoArray, batchSize, stat);
 }

@@ -35,12 +35,12 @@ constexpr int kBpW = 32;  // panel width = the update's K
 
 struct __align__(16) BpSmem {
     float crow[2][32][kBpW];  // per column parity and warp: the warp's pivot candidate row
-    unsigned ckey[2][32];     //   its key
+    unsigned ckey[2][32];     //   its key (the exact search: its magnitude bits)
+    int cpos[2][32];          //   (the exact search) its position
     float l11[kBpW][kBpW + 1];
     int mv_src[2 * kBpW];     // rows whose position changed: memory row and destination row
     int mv_dst[2 * kBpW];
     int mv_cnt;
-    int info;
 };
 
 // Scratch per matrix (byte offsets): L21 (n - 32 rows x 32, row-major) as its TF32 high plane
@@ -119,11 +119,18 @@ constexpr int kMvCols = 128;
 
 // One CTA per matrix; thread t holds memory rows k0 + t + r * NT (r < RPT) of the panel. NT x RPT
 // covers the panel's rows; 128 registers a thread, so that 512 / NT CTAs share an SM.
-template <int NT, int RPT>
+// EXACT (the plain FP32 factorisation): the reference's arithmetic -- first maximum of the exact
+// magnitudes, true division, and after a stop at column kk of the panel only the U rows above kk
+// (the trailing update then takes rows from kk on with K = kk - k0); no TF32 planes (the update
+// reads L21 and U12 from LU). Otherwise (mixed): the approximate pivot key and reciprocal, TF32
+// planes, and a stop zeroes the update. PIVOT = false: no pivoting (the reference's no-pivot
+// variant). st[m]: the matrix's info code so far (0, or the stop column + 1); info, when not
+// nullptr, receives the same.
+template <int NT, int RPT, bool EXACT, bool PIVOT>
 __global__ void __launch_bounds__(NT, 512 / NT)
 lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* __restrict__ piv,
-                int* __restrict__ info, char* __restrict__ scratch, long long l21_off, long long u12_off,
-                long long per_matrix)
+                int* __restrict__ info, int* __restrict__ st, char* __restrict__ scratch, long long l21_off,
+                long long u12_off, long long per_matrix)
 {
     constexpr int NW = NT / 32;
     __shared__ BpSmem S;
@@ -131,28 +138,26 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long m = blockIdx.x;
     float* T = LUarr[m];  // by rows: T(i, j) = T[j + i * ldt]
-    char* base = scratch + m * per_matrix;
-    float* L21 = reinterpret_cast<float*>(base + l21_off);
-    float* U12 = reinterpret_cast<float*>(base + u12_off);
-    int* pm = piv + m * n;
+    int* pm = PIVOT ? piv + m * n : nullptr;
     const int mp = n - k0;                      // panel rows
     const int pw = mp < kBpW ? mp : kBpW;       // panel columns
     const int ntr = n - k0 - kBpW;              // trailing rows and columns
     const long long lo = (long long)(n - kBpW) * kBpW;  // floats from a high plane to its low plane
-    const int inf0 = info[m];
+    float* L21 = EXACT ? nullptr : reinterpret_cast<float*>(scratch + m * per_matrix + l21_off);
+    float* U12 = EXACT ? nullptr : reinterpret_cast<float*>(scratch + m * per_matrix + u12_off);
+    const int inf0 = st[m];
     // whole rows as float4 when every row start is 16-byte aligned (uniform per matrix)
     const bool vec = (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (ldt & 3) == 0 && pw == kBpW;
 
-    if (tid == 0) {
-        S.info = inf0;
-        S.mv_cnt = 0;
-    }
-    if (inf0 != 0) {  // stopped at an earlier zero pivot: this step's update must change nothing
-        for (int e = tid; e < (ntr > 0 ? ntr : 0) * kBpW; e += NT) {
-            L21[e] = 0.0f;
-            L21[lo + e] = 0.0f;
-            U12[e] = 0.0f;
-            U12[lo + e] = 0.0f;
+    if (tid == 0) S.mv_cnt = 0;
+    if (inf0 != 0) {  // stopped at an earlier zero pivot
+        if (!EXACT) {  // this step's update must change nothing
+            for (int e = tid; e < (ntr > 0 ? ntr : 0) * kBpW; e += NT) {
+                L21[e] = 0.0f;
+                L21[lo + e] = 0.0f;
+                U12[e] = 0.0f;
+                U12[lo + e] = 0.0f;
+            }
         }
         return;
     }
@@ -194,59 +199,116 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
         if (c >= pw) break;
         const int k = k0 + c;
         const int buf = c & 1;
-        unsigned best = 0u;  // this thread's best candidate key (0: none)
+        int ppos;
+        const float* prow;
+        bool nocand = false;  // (mixed search) no candidate key at all: treated as a zero pivot
+        if (!PIVOT) {  // the row at position k
 #pragma unroll
-        for (int r = 0; r < RPT; r++) {
-            const float av = fabsf(p[r][c]);
-            const unsigned mag = (av == av) ? (__float_as_uint(av) >> 9) : 0u;  // NaN never wins
-            const unsigned key = (valid[r] && pos[r] >= k) ? ((mag << 10) | (1023u - (unsigned)(pos[r] - k0))) : 0u;
-            best = key > best ? key : best;
-        }
-        const unsigned wkey = __reduce_max_sync(0xffffffffu, best);
-        if (lane == 0) S.ckey[buf][warp] = wkey;
-        if (best != 0u && best == wkey) {  // keys are unique: one writer a warp
-            float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
-#pragma unroll
-            for (int r = 0; r < RPT; r++) {
-                const float av = fabsf(p[r][c]);
-                const unsigned mag = (av == av) ? (__float_as_uint(av) >> 9) : 0u;
-                const unsigned key =
-                    (valid[r] && pos[r] >= k) ? ((mag << 10) | (1023u - (unsigned)(pos[r] - k0))) : 0u;
-                if (key == best) {
+            for (int r = 0; r < RPT; r++)
+                if (valid[r] && pos[r] == k) {
+                    float4* dst = reinterpret_cast<float4*>(S.crow[buf][0]);
 #pragma unroll
                     for (int q = 0; q < kBpW / 4; q++)
                         dst[q] = make_float4(p[r][4 * q], p[r][4 * q + 1], p[r][4 * q + 2], p[r][4 * q + 3]);
                 }
+            __syncthreads();
+            ppos = k;
+            prow = S.crow[buf][0];
+        } else if (EXACT) {
+            // first maximum of |x| over the positions >= k: the largest magnitude (as its bits; NaN
+            // counts as zero and never wins), then the lowest position among equals
+            unsigned bm = 0u;
+            int bp = 0x7fffffff;
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                if (!(valid[r] && pos[r] >= k)) continue;
+                const float av = fabsf(p[r][c]);
+                const unsigned mag = av == av ? __float_as_uint(av) : 0u;
+                if (mag > bm || (mag == bm && pos[r] < bp)) {
+                    bm = mag;
+                    bp = pos[r];
+                }
             }
+            const unsigned wm = __reduce_max_sync(0xffffffffu, bm);
+            const int wp = (int)__reduce_min_sync(0xffffffffu, bm == wm ? (unsigned)bp : 0x7fffffffu);
+            if (lane == 0) {
+                S.ckey[buf][warp] = wm;
+                S.cpos[buf][warp] = wp;
+            }
+#pragma unroll
+            for (int r = 0; r < RPT; r++)
+                if (valid[r] && pos[r] == wp && bp == wp) {
+                    float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
+#pragma unroll
+                    for (int q = 0; q < kBpW / 4; q++)
+                        dst[q] = make_float4(p[r][4 * q], p[r][4 * q + 1], p[r][4 * q + 2], p[r][4 * q + 3]);
+                }
+            __syncthreads();
+            const unsigned qm = lane < NW ? S.ckey[buf][lane] : 0u;
+            const int qp = lane < NW ? S.cpos[buf][lane] : 0x7fffffff;
+            const unsigned gm = __reduce_max_sync(0xffffffffu, qm);
+            ppos = (int)__reduce_min_sync(0xffffffffu, qm == gm ? (unsigned)qp : 0x7fffffffu);
+            const int bw = __ffs(__ballot_sync(0xffffffffu, lane < NW && qm == gm && qp == ppos)) - 1;
+            prow = S.crow[buf][bw < 0 ? 0 : bw];  // (position k is always a candidate: bw >= 0)
+        } else {
+            unsigned best = 0u;  // this thread's best candidate key (0: none)
+#pragma unroll
+            for (int r = 0; r < RPT; r++) {
+                const float av = fabsf(p[r][c]);
+                const unsigned mag = (av == av) ? (__float_as_uint(av) >> 9) : 0u;  // NaN never wins
+                const unsigned key =
+                    (valid[r] && pos[r] >= k) ? ((mag << 10) | (1023u - (unsigned)(pos[r] - k0))) : 0u;
+                best = key > best ? key : best;
+            }
+            const unsigned wkey = __reduce_max_sync(0xffffffffu, best);
+            if (lane == 0) S.ckey[buf][warp] = wkey;
+            if (best != 0u && best == wkey) {  // keys are unique: one writer a warp
+                float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
+#pragma unroll
+                for (int r = 0; r < RPT; r++) {
+                    const float av = fabsf(p[r][c]);
+                    const unsigned mag = (av == av) ? (__float_as_uint(av) >> 9) : 0u;
+                    const unsigned key =
+                        (valid[r] && pos[r] >= k) ? ((mag << 10) | (1023u - (unsigned)(pos[r] - k0))) : 0u;
+                    if (key == best) {
+#pragma unroll
+                        for (int q = 0; q < kBpW / 4; q++)
+                            dst[q] = make_float4(p[r][4 * q], p[r][4 * q + 1], p[r][4 * q + 2], p[r][4 * q + 3]);
+                    }
+                }
+            }
+            __syncthreads();
+            const unsigned qk = lane < NW ? S.ckey[buf][lane] : 0u;
+            const unsigned bk = __reduce_max_sync(0xffffffffu, qk);
+            const int bw = __ffs(__ballot_sync(0xffffffffu, lane < NW && qk == bk)) - 1;
+            nocand = bk == 0u;
+            ppos = nocand ? k : k0 + 1023 - (int)(bk & 1023u);
+            prow = S.crow[buf][bw];
         }
-        __syncthreads();
-        const unsigned qk = lane < NW ? S.ckey[buf][lane] : 0u;
-        const unsigned bk = __reduce_max_sync(0xffffffffu, qk);
-        const int bw = __ffs(__ballot_sync(0xffffffffu, lane < NW && qk == bk)) - 1;
-        const int ppos = k0 + 1023 - (int)(bk & 1023u);
-        const float* prow = S.crow[buf][bw];
         const float pv = prow[c];
-        if (tid == 0) pm[k] = ppos + 1;
-        if (pv == 0.0f || bk == 0u) {  // exactly-zero pivot column: stop here (uniform)
+        if (PIVOT && tid == 0) pm[k] = ppos + 1;
+        if (pv == 0.0f || nocand) {  // exactly-zero pivot: stop here, before the interchange (uniform)
             if (tid == 0) {
-                S.info = k + 1;
-                info[m] = k + 1;
+                st[m] = k + 1;
+                if (info != nullptr && info != st) info[m] = k + 1;
             }
             done = c;
             break;
         }
-        float rinv;
-        asm("rcp.approx.f32 %0, %1;" : "=f"(rinv) : "f"(pv));
+        float rinv = 0.0f;
+        if (!EXACT) asm("rcp.approx.f32 %0, %1;" : "=f"(rinv) : "f"(pv));
         float l[RPT];
         bool upd[RPT];  // rows below the pivot position take the update
 #pragma unroll
         for (int r = 0; r < RPT; r++) {
-            if (pos[r] == ppos)
-                pos[r] = k;
-            else if (pos[r] == k)
-                pos[r] = ppos;
+            if (PIVOT) {
+                if (pos[r] == ppos)
+                    pos[r] = k;
+                else if (pos[r] == k)
+                    pos[r] = ppos;
+            }
             upd[r] = valid[r] && pos[r] > k;
-            l[r] = p[r][c] * rinv;
+            l[r] = EXACT ? p[r][c] / pv : p[r][c] * rinv;
             if (upd[r]) p[r][c] = l[r];
         }
 #pragma unroll
@@ -277,12 +339,12 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
             for (int c = 0; c < kBpW; c++)
                 if (c < pw) row[c] = p[r][c];
         }
-        if (pos[r] != k0 + tid + r * NT) {
+        if (PIVOT && pos[r] != k0 + tid + r * NT) {
             const int q = atomicAdd(&S.mv_cnt, 1);
             S.mv_src[q] = k0 + tid + r * NT;
             S.mv_dst[q] = pos[r];
         }
-        if (ntr > 0 && pos[r] >= k0 + kBpW) {
+        if (!EXACT && ntr > 0 && pos[r] >= k0 + kBpW) {
             float4* dh = reinterpret_cast<float4*>(L21 + (long long)(pos[r] - k0 - kBpW) * kBpW);
             float4* dl = reinterpret_cast<float4*>(L21 + lo + (long long)(pos[r] - k0 - kBpW) * kBpW);
 #pragma unroll
@@ -342,32 +404,185 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
     if (ntr <= 0) return;  // last panel: no trailing block
 
     // 5. U12 = L11^-1 * (the pivot rows' trailing entries, now in rows k0..k0+31), one thread per
-    //    trailing column: the final U rows, and the TF32 planes of the update
+    //    trailing column, in the reference's order (row i takes columns 0..i-1 in turn): the final U
+    //    rows (above the stop column only, EXACT) and the TF32 planes of the update (mixed)
+    const int urows = EXACT ? done : kBpW;
     for (int jj = tid; jj < ntr; jj += NT) {
         const int col = k0 + kBpW + jj;
         float u[kBpW];
 #pragma unroll
-        for (int i = 0; i < kBpW; i++) u[i] = stopped ? 0.0f : T[(long long)(k0 + i) * ldt + col];
+        for (int i = 0; i < kBpW; i++) u[i] = (stopped && !EXACT) ? 0.0f : T[(long long)(k0 + i) * ldt + col];
 #pragma unroll
         for (int i = 1; i < kBpW; i++)
 #pragma unroll
             for (int c = 0; c < kBpW; c++)
-                if (c < i) u[i] = fmaf(-S.l11[i][c], u[c], u[i]);
-        if (!stopped) {
+                if (c < i && i < urows) u[i] = fmaf(-S.l11[i][c], u[c], u[i]);
+        if (EXACT || !stopped) {
 #pragma unroll
-            for (int i = 0; i < kBpW; i++) T[(long long)(k0 + i) * ldt + col] = u[i];
+            for (int i = 1; i < kBpW; i++)
+                if (i < urows) T[(long long)(k0 + i) * ldt + col] = u[i];
         }
-        float4* dh = reinterpret_cast<float4*>(U12 + (long long)jj * kBpW);
-        float4* dl = reinterpret_cast<float4*>(U12 + lo + (long long)jj * kBpW);
+        if (!EXACT) {
+            float4* dh = reinterpret_cast<float4*>(U12 + (long long)jj * kBpW);
+            float4* dl = reinterpret_cast<float4*>(U12 + lo + (long long)jj * kBpW);
 #pragma unroll
-        for (int q = 0; q < kBpW / 4; q++) {
-            float h[4], lw[4];
+            for (int q = 0; q < kBpW / 4; q++) {
+                float h[4], lw[4];
 #pragma unroll
-            for (int e = 0; e < 4; e++) tf32_split(u[4 * q + e], h[e], lw[e]);
-            dh[q] = make_float4(h[0], h[1], h[2], h[3]);
-            dl[q] = make_float4(lw[0], lw[1], lw[2], lw[3]);
+                for (int e = 0; e < 4; e++) tf32_split(u[4 * q + e], h[e], lw[e]);
+                dh[q] = make_float4(h[0], h[1], h[2], h[3]);
+                dl[q] = make_float4(lw[0], lw[1], lw[2], lw[3]);
+            }
         }
     }
+}
+
+// Trailing update of the plain factorisation, by rows: T(i, j) -= sum_k T(i, k0 + k) T(k0 + k, j)
+// for rows i from r0 = k0 + 32 (or the stop column) and columns j from k0 + 32, K = 32 (or the
+// columns before the stop), one fmaf at a time in increasing k -- the reference's sequence of
+// rank-1 updates, so the result is bit-identical to it. A CTA computes a 128 x 128 tile, each
+// thread an 8 x 8 block (rows 8 ty .., columns 8 tx ..) from L and U staged in shared memory.
+// st[m]: the matrix's info code (the update is skipped for a matrix stopped earlier). The grid's
+// row tiles cover n - k0 rows (a stop adds up to 31 rows to the block).
+constexpr int kRuTile = 128;
+
+__global__ void __launch_bounds__(256, 2)
+lu_rows_update_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, const int* __restrict__ st,
+                      int tiles_m, int tiles_n)
+{
+    __shared__ __align__(16) float Ls[kBpW][kRuTile];  // Ls[k][row]
+    __shared__ __align__(16) float Us[kBpW][kRuTile];  // Us[k][col]
+    const int tiles = tiles_m * tiles_n;
+    const long long m = blockIdx.x / tiles;
+    const int tile = (int)(blockIdx.x % tiles);
+    const int code = st[m];
+    int r0 = k0 + kBpW, K = kBpW;
+    if (code != 0) {
+        if (code - 1 < k0) return;  // stopped in an earlier panel: no more updates
+        K = code - 1 - k0;          // stopped in this panel at column k0 + K
+        r0 = k0 + K;
+        if (K == 0) return;
+    }
+    const int c0 = k0 + kBpW;
+    const int rows = n - r0, cols = n - c0;
+    const int tr = (tile % tiles_m) * kRuTile, tc = (tile / tiles_m) * kRuTile;
+    if (tr >= rows || tc >= cols) return;
+    float* T = LUarr[m];
+    const bool vec = (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (ldt & 3) == 0;
+    const int tid = threadIdx.x;
+    // L: rows r0 + tr + i, columns k0 .. k0 + K - 1; U: rows k0 .. k0 + K - 1, columns c0 + tc + j
+    for (int e = tid; e < kRuTile * kBpW; e += 256) {
+        const int i = e / kBpW, k = e % kBpW;
+        Ls[k][i] = (tr + i < rows && k < K) ? T[(long long)(r0 + tr + i) * ldt + k0 + k] : 0.0f;
+    }
+    for (int e = tid; e < kRuTile * kBpW; e += 256) {
+        const int k = e / kRuTile, j = e % kRuTile;
+        Us[k][j] = (tc + j < cols && k < K) ? T[(long long)(k0 + k) * ldt + c0 + tc + j] : 0.0f;
+    }
+    __syncthreads();
+    const int tx = tid & 15, ty = tid >> 4;  // 16 x 16 threads
+    const int ib = tr + 8 * ty, jb = tc + 8 * tx;
+    const bool full = vec && jb + 7 < cols;
+    float acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+        const float* src = T + (long long)(r0 + ib + a) * ldt + c0 + jb;
+        if (ib + a >= rows) {
+#pragma unroll
+            for (int b = 0; b < 8; b++) acc[a][b] = 0.0f;
+        } else if (full) {
+            const float4 x = reinterpret_cast<const float4*>(src)[0], y = reinterpret_cast<const float4*>(src)[1];
+            acc[a][0] = x.x, acc[a][1] = x.y, acc[a][2] = x.z, acc[a][3] = x.w;
+            acc[a][4] = y.x, acc[a][5] = y.y, acc[a][6] = y.z, acc[a][7] = y.w;
+        } else {
+#pragma unroll
+            for (int b = 0; b < 8; b++) acc[a][b] = jb + b < cols ? src[b] : 0.0f;
+        }
+    }
+    auto step = [&](int k) {
+        const float4 l0 = *reinterpret_cast<const float4*>(&Ls[k][8 * ty]);
+        const float4 l1 = *reinterpret_cast<const float4*>(&Ls[k][8 * ty + 4]);
+        const float4 u0 = *reinterpret_cast<const float4*>(&Us[k][8 * tx]);
+        const float4 u1 = *reinterpret_cast<const float4*>(&Us[k][8 * tx + 4]);
+        const float lv[8] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
+        const float uv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int b = 0; b < 8; b++) acc[a][b] = fmaf(-lv[a], uv[b], acc[a][b]);
+    };
+    if (K == kBpW) {
+#pragma unroll 4
+        for (int k = 0; k < kBpW; k++) step(k);
+    } else {
+        for (int k = 0; k < K; k++) step(k);
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+        if (ib + a >= rows) continue;
+        float* dst = T + (long long)(r0 + ib + a) * ldt + c0 + jb;
+        if (full) {
+            reinterpret_cast<float4*>(dst)[0] = make_float4(acc[a][0], acc[a][1], acc[a][2], acc[a][3]);
+            reinterpret_cast<float4*>(dst)[1] = make_float4(acc[a][4], acc[a][5], acc[a][6], acc[a][7]);
+        } else {
+#pragma unroll
+            for (int b = 0; b < 8; b++)
+                if (jb + b < cols) dst[b] = acc[a][b];
+        }
+    }
+}
+
+// The panel kernel's CTA shape by panel rows: small CTAs share an SM, two rows a thread above 256.
+template <bool EXACT, bool PIVOT>
+static cudaError_t panel_launch(cudaStream_t st, float* const* T, int n, int ldt, int k0, int* piv, int* info,
+                                int* stat, char* scratch, long long l21_off, long long u12_off, long long per_matrix,
+                                int batch)
+{
+    const int mp = n - k0;
+    const unsigned g = (unsigned)batch;
+    if (mp <= 128)
+        lu_panel_kernel<128, 1, EXACT, PIVOT><<<g, 128, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
+                                                                  u12_off, per_matrix);
+    else if (mp <= 256)
+        lu_panel_kernel<256, 1, EXACT, PIVOT><<<g, 256, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
+                                                                  u12_off, per_matrix);
+    else if (mp <= 512)
+        lu_panel_kernel<256, 2, EXACT, PIVOT><<<g, 256, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
+                                                                  u12_off, per_matrix);
+    else
+        lu_panel_kernel<512, 2, EXACT, PIVOT><<<g, 512, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
+                                                                  u12_off, per_matrix);
+    return cudaGetLastError();
+}
+
+bool getrf_rows_supported(int n) { return n > 128 && n <= 1024; }
+
+cudaError_t getrf_rows_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int* stat,
+                              int batch)
+{
+    if (!getrf_rows_supported(n) || batch <= 0) return cudaErrorInvalidValue;
+    cudaError_t err = cudaMemsetAsync(stat, 0, sizeof(int) * (size_t)batch, st);
+    if (err == cudaSuccess && info != nullptr) err = cudaMemsetAsync(info, 0, sizeof(int) * (size_t)batch, st);
+    if (err == cudaSuccess && piv != nullptr) err = cudaMemsetAsync(piv, 0, sizeof(int) * (size_t)n * batch, st);
+    if (err != cudaSuccess) return err;
+    const int nt = (n + 31) / 32;
+    const dim3 tgrid((unsigned)batch, (unsigned)(nt * (nt + 1) / 2));
+    lu_rows_out_kernel<<<tgrid, 256, 0, st>>>(Aarray, lda, n);  // in place: by columns -> by rows
+    for (int k0 = 0; k0 < n; k0 += kBpW) {
+        err = piv != nullptr ? panel_launch<true, true>(st, Aarray, n, lda, k0, piv, info, stat, nullptr, 0, 0, 0, batch)
+                             : panel_launch<true, false>(st, Aarray, n, lda, k0, nullptr, info, stat, nullptr, 0, 0, 0,
+                                                         batch);
+        if (err != cudaSuccess) return err;
+        if (n - k0 - kBpW > 0) {
+            const int tm = (n - k0 + kRuTile - 1) / kRuTile, tn = (n - k0 - kBpW + kRuTile - 1) / kRuTile;
+            lu_rows_update_kernel<<<(unsigned)((long long)batch * tm * tn), 256, 0, st>>>(Aarray, n, lda, k0, stat, tm,
+                                                                                          tn);
+            err = cudaGetLastError();
+            if (err != cudaSuccess) return err;
+        }
+    }
+    lu_rows_out_kernel<<<tgrid, 256, 0, st>>>(Aarray, lda, n);  // by rows -> by columns
+    return cudaGetLastError();
 }
 
 bool getrf_blocked_tc_supported(int n) { return n > 256 && n <= 1024; }
@@ -397,21 +612,8 @@ cudaError_t getrf_blocked_tc_launch(cudaStream_t st, const float* const* Aarray,
     const int nt = (n + 31) / 32;
     lu_rows_in_kernel<<<dim3((unsigned)batch, (unsigned)(nt * nt)), 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n);
     for (int k0 = 0; k0 < n; k0 += kBpW) {
-        // the CTA shape by panel rows: small CTAs share an SM, two rows a thread above 256
-        const int mp = n - k0;
-        if (mp <= 128)
-            lu_panel_kernel<128, 1><<<(unsigned)batch, 128, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
-                                                                     L.u12, L.per_matrix);
-        else if (mp <= 256)
-            lu_panel_kernel<256, 1><<<(unsigned)batch, 256, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
-                                                                     L.u12, L.per_matrix);
-        else if (mp <= 512)
-            lu_panel_kernel<256, 2><<<(unsigned)batch, 256, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
-                                                                     L.u12, L.per_matrix);
-        else
-            lu_panel_kernel<512, 2><<<(unsigned)batch, 512, 0, st>>>(LUarray, n, ldlu, k0, piv, info, base, L.l21,
-                                                                     L.u12, L.per_matrix);
-        err = cudaGetLastError();
+        err = panel_launch<false, true>(st, LUarray, n, ldlu, k0, piv, info, info, base, L.l21, L.u12, L.per_matrix,
+                                        batch);
         if (err != cudaSuccess) return err;
         const int mt = n - k0 - kBpW;
         if (mt > 0) {

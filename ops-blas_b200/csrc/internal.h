@@ -133,6 +133,17 @@ cudaError_t getrf_blocked_tc_launch(cudaStream_t st, const float* const* Aarray,
                                     int ldlu, int* piv, int* info, int batch, void* scratch, unsigned* status,
                                     void* tmslots);
 
+// getrf_blocked_tc.cu: 128 < n <= 1024, the plain FP32 blocked LU on a by-rows copy made in place
+// (bit-identical to the reference's unblocked order); piv and info may be nullptr (no-pivot mode:
+// piv == nullptr); stat: batch ints of device scratch (the matrices' stop codes).
+bool getrf_rows_supported(int n);
+// aclblasSgetrfBatched with the blocked path's stop codes in `stat` (batch ints of device memory
+// that the caller does not use otherwise; nullptr: the blocked path is not taken).
+aclblasStatus_t getrf_batched_impl(aclblasHandle_t handle, int n, float* const Aarray[], int lda, int* PivotArray,
+                                   int* infoArray, int batchSize, int* stat);
+cudaError_t getrf_rows_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int* stat,
+                              int batch);
+
 // getrf_tmem.cu: 32 < n <= 256, mixed-precision LU with the matrix resident in TMEM.
 bool getrf_tmem_supported(int n);
 // Reads A (lda), writes the factors to LU (ldlu); A may equal LU. prec 1: TF32 split update,

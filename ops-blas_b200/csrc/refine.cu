@@ -262,8 +262,11 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     } else if (blocked) {  // reads A, writes LU
         err = getrf_blocked_tc_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount,
                                       ws + bt_off, handle->dstatus, handle->tmslots);
-    } else {  // plain FP32 factors: the batched getrf's kernels
-        aclblasStatus_t s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
+    } else {  // plain FP32 factors: the batched getrf's kernels (stop codes after the refinement's part)
+        int* stat = handle->workspace_size >= bt_off + sizeof(int) * (size_t)batchCount
+                        ? reinterpret_cast<int*>(ws + bt_off)
+                        : nullptr;
+        aclblasStatus_t s = getrf_batched_impl(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount, stat);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;
     }
     if (err != cudaSuccess || nrhs == 0) return launch_status(kApi, err);
@@ -425,14 +428,23 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
     fill_int_kernel<<<bgrid, 256, 0, st>>>(done, 0, batchCount);
     fill_int_kernel<<<bgrid, 256, 0, st>>>(iterArray, maxIter, batchCount);
     const bool tmem = mode != 0 && getrf_tmem_supported(n);  // reads A, writes LU: no copy
-    if (!tmem) copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
+    // the blocked tensor-core LU (TF32 above n = 256) when the static scratch also holds its scratch,
+    // after the refinement's part -- as the workspace entry point decides with its workspace
+    const size_t used = ((dbytes + 20) * (size_t)batchCount + 512 + 255) / 256 * 256;
+    const bool blocked = mode == 1 && getrf_blocked_tc_supported(n) &&
+                         used + getrf_blocked_tc_scratch_bytes(n, batchCount) <= cap;
+    if (!tmem && !blocked) copy_batched_kernel<<<(unsigned)batchCount, 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n, n);
     err = cudaGetLastError();
     if (err != cudaSuccess) return launch_status(kApi, err);
     if (tmem) {
         err = getrf_tmem_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, mode,
                                 handle->dstatus);
-    } else {  // plain FP32 factors: the batched getrf's kernels
-        s = aclblasSgetrfBatched(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount);
+    } else if (blocked) {  // reads A, writes LU
+        err = getrf_blocked_tc_launch(st, Aarray, lda, LUarray, n, ldlu, PivotArray, infoArray, batchCount, ws + used,
+                                      handle->dstatus, handle->tmslots);
+    } else {  // plain FP32 factors: the batched getrf's kernels (stop codes in the static scratch)
+        int* stat = used + sizeof(int) * (size_t)batchCount <= cap ? reinterpret_cast<int*>(ws + used) : nullptr;
+        s = getrf_batched_impl(handle, n, LUarray, ldlu, PivotArray, infoArray, batchCount, stat);
         if (s != ACLBLAS_STATUS_SUCCESS) return s;
     }
     if (err != cudaSuccess || nrhs == 0) return launch_status(kApi, err);

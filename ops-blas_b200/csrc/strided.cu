@@ -78,7 +78,13 @@ extern "C" aclblasStatus_t aclblasSgetrfStridedBatched(aclblasHandle_t handle, i
     if (s != ACLBLAS_STATUS_SUCCESS) return s;
     s = launch_status(kApi, build_ptrs(handle->stream, A, strideA * (long long)sizeof(float), batchSize, p[0]));
     if (s != ACLBLAS_STATUS_SUCCESS) return s;
-    return aclblasSgetrfBatched(handle, n, reinterpret_cast<float* const*>(p[0]), lda, PivotArray, infoArray, batchSize);
+    // the blocked factorisation's stop codes after the pointer array, when the workspace holds them
+    const size_t each = (((size_t)batchSize * sizeof(void*)) + 255) & ~(size_t)255;
+    int* stat = handle->workspace_size >= each + sizeof(int) * (size_t)batchSize
+                    ? reinterpret_cast<int*>(static_cast<char*>(handle->workspace) + each)
+                    : nullptr;
+    return getrf_batched_impl(handle, n, reinterpret_cast<float* const*>(p[0]), lda, PivotArray, infoArray, batchSize,
+                              stat);
 }
 
 extern "C" aclblasStatus_t aclblasSgetrsStridedBatched(aclblasHandle_t handle, aclblasOperation_t trans, int n,
