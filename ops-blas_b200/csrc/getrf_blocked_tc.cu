@@ -57,6 +57,12 @@ struct BpScratch {
     }
 };
 
+// 16-byte cp.async that reads src_bytes (0 or 16) and zero-fills the rest.
+__device__ __forceinline__ void cp_async16_zf(uint32_t saddr, const void* gmem, int src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(gmem), "r"(src_bytes) : "memory");
+}
+
 // hi = x rounded to TF32 (nearest even), lo = (x - hi) rounded to TF32.
 __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo)
 {
@@ -440,18 +446,21 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
 // Trailing update of the plain factorisation, by rows: T(i, j) -= sum_k T(i, k0 + k) T(k0 + k, j)
 // for rows i from r0 = k0 + 32 (or the stop column) and columns j from k0 + 32, K = 32 (or the
 // columns before the stop), one fmaf at a time in increasing k -- the reference's sequence of
-// rank-1 updates, so the result is bit-identical to it. A CTA computes a 128 x 128 tile, each
-// thread an 8 x 8 block (rows 8 ty .., columns 8 tx ..) from L and U staged in shared memory.
-// st[m]: the matrix's info code (the update is skipped for a matrix stopped earlier). The grid's
-// row tiles cover n - k0 rows (a stop adds up to 31 rows to the block).
-constexpr int kRuTile = 128;
+// rank-1 updates, so the result is bit-identical to it. A CTA of 128 threads computes a 64 x 128
+// tile, each thread an 8 x 8 block (rows ty + 8 a, columns 8 tx ..): L (row-major, row stride 36
+// floats: the eight row values of a step are conflict-free broadcasts) and U arrive in shared
+// memory by cp.async while the thread's C block is loaded into registers, so a tile waits for one
+// memory round trip; 144 registers, three CTAs an SM. st[m]: the matrix's info code (the update
+// is skipped for a matrix stopped earlier). The grid's row tiles cover n - k0 rows (a stop adds up
+// to 31 rows to the block).
+constexpr int kRuRows = 64, kRuCols = 128, kRuLd = 36;
 
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(128, 3)
 lu_rows_update_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, const int* __restrict__ st,
                       int tiles_m, int tiles_n)
 {
-    __shared__ __align__(16) float Ls[kBpW][kRuTile];  // Ls[k][row]
-    __shared__ __align__(16) float Us[kBpW][kRuTile];  // Us[k][col]
+    __shared__ __align__(16) float Ls[kRuRows][kRuLd];    // Ls[row][k]
+    __shared__ __align__(16) float Us[kBpW][kRuCols];     // Us[k][col]
     const int tiles = tiles_m * tiles_n;
     const long long m = blockIdx.x / tiles;
     const int tile = (int)(blockIdx.x % tiles);
@@ -465,29 +474,52 @@ lu_rows_update_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, 
     }
     const int c0 = k0 + kBpW;
     const int rows = n - r0, cols = n - c0;
-    const int tr = (tile % tiles_m) * kRuTile, tc = (tile / tiles_m) * kRuTile;
+    const int tr = (tile % tiles_m) * kRuRows, tc = (tile / tiles_m) * kRuCols;
     if (tr >= rows || tc >= cols) return;
     float* T = LUarr[m];
     const bool vec = (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (ldt & 3) == 0;
     const int tid = threadIdx.x;
     // L: rows r0 + tr + i, columns k0 .. k0 + K - 1; U: rows k0 .. k0 + K - 1, columns c0 + tc + j
-    for (int e = tid; e < kRuTile * kBpW; e += 256) {
-        const int i = e / kBpW, k = e % kBpW;
-        Ls[k][i] = (tr + i < rows && k < K) ? T[(long long)(r0 + tr + i) * ldt + k0 + k] : 0.0f;
+    if (vec) {
+#pragma unroll
+        for (int u = 0; u < kRuRows * kBpW / 4 / 128; u++) {
+            const int e = tid + 128 * u, i = e / (kBpW / 4), kq = (e % (kBpW / 4)) * 4;
+            const bool ok = tr + i < rows && kq < K;
+            cp_async16_zf(smem_u32(&Ls[i][kq]), T + (long long)(ok ? r0 + tr + i : r0) * ldt + k0 + kq, ok ? 16 : 0);
+        }
+#pragma unroll
+        for (int u = 0; u < kRuCols * kBpW / 4 / 128; u++) {
+            const int e = tid + 128 * u, k = e / (kRuCols / 4), jq = (e % (kRuCols / 4)) * 4;
+            const bool ok = k < K && tc + jq + 3 < cols;
+            if (ok || tc + jq >= cols || k >= K) {
+                cp_async16_zf(smem_u32(&Us[k][jq]), T + (long long)(k0 + (k < K ? k : 0)) * ldt + c0 + (ok ? tc + jq : 0),
+                                 ok ? 16 : 0);
+            } else {  // the ragged right edge
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    Us[k][jq + q] = tc + jq + q < cols ? T[(long long)(k0 + k) * ldt + c0 + tc + jq + q] : 0.0f;
+            }
+        }
+        cp_async_commit();
+    } else {
+        for (int e = tid; e < kRuRows * kBpW; e += 128) {
+            const int i = e / kBpW, k = e % kBpW;
+            Ls[i][k] = (tr + i < rows && k < K) ? T[(long long)(r0 + tr + i) * ldt + k0 + k] : 0.0f;
+        }
+        for (int e = tid; e < kRuCols * kBpW; e += 128) {
+            const int k = e / kRuCols, j = e % kRuCols;
+            Us[k][j] = (tc + j < cols && k < K) ? T[(long long)(k0 + k) * ldt + c0 + tc + j] : 0.0f;
+        }
     }
-    for (int e = tid; e < kRuTile * kBpW; e += 256) {
-        const int k = e / kRuTile, j = e % kRuTile;
-        Us[k][j] = (tc + j < cols && k < K) ? T[(long long)(k0 + k) * ldt + c0 + tc + j] : 0.0f;
-    }
-    __syncthreads();
-    const int tx = tid & 15, ty = tid >> 4;  // 16 x 16 threads
-    const int ib = tr + 8 * ty, jb = tc + 8 * tx;
+    const int tx = tid & 15, ty = tid >> 4;  // 16 x 8 threads
+    const int jb = tc + 8 * tx;
     const bool full = vec && jb + 7 < cols;
     float acc[8][8];
 #pragma unroll
     for (int a = 0; a < 8; a++) {
-        const float* src = T + (long long)(r0 + ib + a) * ldt + c0 + jb;
-        if (ib + a >= rows) {
+        const int i = tr + ty + 8 * a;
+        const float* src = T + (long long)(r0 + i) * ldt + c0 + jb;
+        if (i >= rows) {
 #pragma unroll
             for (int b = 0; b < 8; b++) acc[a][b] = 0.0f;
         } else if (full) {
@@ -499,12 +531,14 @@ lu_rows_update_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, 
             for (int b = 0; b < 8; b++) acc[a][b] = jb + b < cols ? src[b] : 0.0f;
         }
     }
+    if (vec) cp_async_wait_all();
+    __syncthreads();
     auto step = [&](int k) {
-        const float4 l0 = *reinterpret_cast<const float4*>(&Ls[k][8 * ty]);
-        const float4 l1 = *reinterpret_cast<const float4*>(&Ls[k][8 * ty + 4]);
+        float lv[8];
+#pragma unroll
+        for (int a = 0; a < 8; a++) lv[a] = Ls[ty + 8 * a][k];
         const float4 u0 = *reinterpret_cast<const float4*>(&Us[k][8 * tx]);
         const float4 u1 = *reinterpret_cast<const float4*>(&Us[k][8 * tx + 4]);
-        const float lv[8] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
         const float uv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
 #pragma unroll
         for (int a = 0; a < 8; a++)
@@ -519,8 +553,9 @@ lu_rows_update_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, 
     }
 #pragma unroll
     for (int a = 0; a < 8; a++) {
-        if (ib + a >= rows) continue;
-        float* dst = T + (long long)(r0 + ib + a) * ldt + c0 + jb;
+        const int i = tr + ty + 8 * a;
+        if (i >= rows) continue;
+        float* dst = T + (long long)(r0 + i) * ldt + c0 + jb;
         if (full) {
             reinterpret_cast<float4*>(dst)[0] = make_float4(acc[a][0], acc[a][1], acc[a][2], acc[a][3]);
             reinterpret_cast<float4*>(dst)[1] = make_float4(acc[a][4], acc[a][5], acc[a][6], acc[a][7]);
@@ -574,8 +609,8 @@ cudaError_t getrf_rows_launch(cudaStream_t st, float* const* Aarray, int n, int 
                                                          batch);
         if (err != cudaSuccess) return err;
         if (n - k0 - kBpW > 0) {
-            const int tm = (n - k0 + kRuTile - 1) / kRuTile, tn = (n - k0 - kBpW + kRuTile - 1) / kRuTile;
-            lu_rows_update_kernel<<<(unsigned)((long long)batch * tm * tn), 256, 0, st>>>(Aarray, n, lda, k0, stat, tm,
+            const int tm = (n - k0 + kRuRows - 1) / kRuRows, tn = (n - k0 - kBpW + kRuCols - 1) / kRuCols;
+            lu_rows_update_kernel<<<(unsigned)((long long)batch * tm * tn), 128, 0, st>>>(Aarray, n, lda, k0, stat, tm,
                                                                                           tn);
             err = cudaGetLastError();
             if (err != cudaSuccess) return err;
