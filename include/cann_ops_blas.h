@@ -94,7 +94,10 @@ ACLBLAS_EXPORT aclblasStatus_t aclblasGetDeviceStatus(aclblasHandle_t handle, un
  * Deliberate strengthening: for a singular matrix (info = k > 0) PivotArray[k..n-1] is
  * written as 0, the value the reference's golden model expects
  * (test/getrf_batched/sgetrf_batched/sgetrf_batched_golden.h:78-82) and its test wrapper
- * only gets by pre-zeroing. */
+ * only gets by pre-zeroing. For 128 < n <= 1024 the factorisation is blocked and uses the first
+ * 4 * batchSize bytes of the handle workspace (the reference's kernel uses none); with a smaller
+ * workspace it takes an unblocked-order kernel with the same results (n <= 640) or the generic
+ * one. Results are bit-identical either way. */
 ACLBLAS_EXPORT aclblasStatus_t aclblasSgetrfBatched(
     aclblasHandle_t handle, int n, float* const Aarray[], int lda, int* PivotArray, int* infoArray, int batchSize);
 
