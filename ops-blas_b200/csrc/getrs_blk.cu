@@ -15,24 +15,26 @@
 #include <cuda_runtime.h>
 
 #include "internal.h"
+#include "small_common.cuh"
 
 namespace opsblas {
 
 constexpr int kBsThreads = 256;
 constexpr int kBsRC = 16;  // right-hand sides per pass
 constexpr int kBsB = 32;   // block rows
-constexpr int kBsLd = 33;  // padded row stride of the staged diagonal block
+constexpr int kBsLd = 36;  // row stride of a staged diagonal block (16-byte rows for cp.async)
 
-size_t getrs_blk_smem(int n) { return (size_t)n * kBsRC * 4 + kBsB * kBsLd * 4 + (size_t)n * 4 * 2 + 16; }
+// xs, two diagonal-block buffers, perm and pivots
+size_t getrs_blk_smem(int n) { return (size_t)n * kBsRC * 4 + 2 * kBsB * kBsLd * 4 + (size_t)n * 4 * 2 + 16; }
 
 __global__ void __launch_bounds__(kBsThreads)
 getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const int* __restrict__ ipiv,
                  float* const* __restrict__ Barray, int ldb, int nrhs)
 {
     extern __shared__ __align__(16) float sm[];
-    float* xs = sm;                                          // [n][kBsRC]
-    float* blk = xs + (size_t)n * kBsRC;                     // [kBsB][kBsLd]: blk[j * kBsLd + i]
-    int* perm = reinterpret_cast<int*>(blk + kBsB * kBsLd);  // [n]: source row of position i
+    float* xs = sm;                                              // [n][kBsRC]
+    float* blks = xs + (size_t)n * kBsRC;                        // 2 x [kBsB][kBsLd]: blk[j * kBsLd + i]
+    int* perm = reinterpret_cast<int*>(blks + 2 * kBsB * kBsLd);  // [n]: source row of position i
     int* pv = perm + n;                                      // [n]: pivots
     const long long m = blockIdx.x;
     float* B = Barray[m];
@@ -40,6 +42,24 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
     const float* A = Aarray[m];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     auto at = [&](int i, int j) { return A[i + (long long)j * lda]; };
+    const bool vec = (reinterpret_cast<uintptr_t>(A) & 15) == 0 && (lda & 3) == 0;
+    // the diagonal block at (r0, r0) into buffer `buf`: by cp.async (one 16-byte copy a thread)
+    // when the matrix is 16-byte aligned and the block whole, else element-wise; the caller
+    // waits (cp_async_wait_all) and syncs before reading it
+    auto stage_blk = [&](int r0, int buf) {
+        float* blk = blks + buf * kBsB * kBsLd;
+        const int bs = min(kBsB, n - r0);
+        if (vec && bs == kBsB) {
+            const int j = tid >> 3, iq = (tid & 7) * 4;  // 256 threads = 32 columns x 8 quads
+            cp_async16(blk + j * kBsLd + iq, A + (r0 + iq) + (long long)(r0 + j) * lda);
+            cp_async_commit();
+        } else {
+            for (int e = tid; e < kBsB * kBsB; e += kBsThreads) {
+                const int j = e / kBsB, i = e % kBsB;
+                blk[j * kBsLd + i] = (i < bs && j < bs) ? at(r0 + i, r0 + j) : 0.0f;
+            }
+        }
+    };
 
     // ---- interchanges (sgetrs_batched_kernel.cpp:94-100: out-of-range or zero pivots skipped) ----
     for (int i = tid; i < n; i += kBsThreads) {
@@ -68,12 +88,12 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
         __syncthreads();
 
         // ------------------------------------------------------------ forward, unit L --
-        for (int r0 = 0; r0 < n; r0 += kBsB) {
+        // the next block's diagonal is staged while the rows below the current one update
+        stage_blk(0, 0);
+        for (int r0 = 0, bi = 0; r0 < n; r0 += kBsB, bi ^= 1) {
             const int bs = min(kBsB, n - r0);
-            for (int e = tid; e < kBsB * kBsB; e += kBsThreads) {
-                const int j = e / kBsB, i = e % kBsB;
-                blk[j * kBsLd + i] = (i < bs && j < bs) ? at(r0 + i, r0 + j) : 0.0f;
-            }
+            const float* blk = blks + bi * kBsB * kBsLd;
+            cp_async_wait_all();
             __syncthreads();
             // two right-hand sides per warp, their dependency chains interleaved
             for (int c = warp; c < cw; c += 2 * (kBsThreads / 32)) {
@@ -104,16 +124,17 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                 }
             }
             __syncthreads();
+            if (r0 + kBsB < n) stage_blk(r0 + kBsB, bi ^ 1);
             for (int i = r0 + bs + tid; i < n; i += kBsThreads) {
                 float4 acc[kBsRC / 4];
 #pragma unroll
                 for (int q = 0; q < kBsRC / 4; q++) acc[q] = reinterpret_cast<const float4*>(xs + i * kBsRC)[q];
-                for (int jb = 0; jb < bs; jb += 8) {
-                    float lv[8];  // eight independent loads in flight
+                for (int jb = 0; jb < bs; jb += 16) {
+                    float lv[16];  // sixteen of the row's L values in flight: two round trips a block
 #pragma unroll
-                    for (int u = 0; u < 8; u++) lv[u] = jb + u < bs ? at(i, r0 + jb + u) : 0.0f;
+                    for (int u = 0; u < 16; u++) lv[u] = jb + u < bs ? at(i, r0 + jb + u) : 0.0f;
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
+                    for (int u = 0; u < 16; u++) {
                         if (jb + u >= bs) break;
                         const float nl = -lv[u];
 #pragma unroll
@@ -134,13 +155,13 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
 
         // ---------------------------------------------------------------- backward, U --
         const int nblk = (n + kBsB - 1) / kBsB;
-        for (int kb = nblk - 1; kb >= 0; kb--) {
+        __syncthreads();  // the forward sweep's last reads of both buffers are done
+        stage_blk((nblk - 1) * kBsB, 0);
+        for (int kb = nblk - 1, bi = 0; kb >= 0; kb--, bi ^= 1) {
             const int r0 = kb * kBsB;
             const int bs = min(kBsB, n - r0);
-            for (int e = tid; e < kBsB * kBsB; e += kBsThreads) {
-                const int j = e / kBsB, i = e % kBsB;
-                blk[j * kBsLd + i] = (i < bs && j < bs) ? at(r0 + i, r0 + j) : 0.0f;
-            }
+            const float* blk = blks + bi * kBsB * kBsLd;
+            cp_async_wait_all();
             __syncthreads();
             // two right-hand sides per warp; every lane divides (no divergence), lane j's quotient
             // x_j = y_j / U(j,j) is the one broadcast
@@ -180,16 +201,17 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                 }
             }
             __syncthreads();
+            if (kb > 0) stage_blk(r0 - kBsB, bi ^ 1);
             for (int i = tid; i < r0; i += kBsThreads) {
                 float4 acc[kBsRC / 4];
 #pragma unroll
                 for (int q = 0; q < kBsRC / 4; q++) acc[q] = reinterpret_cast<const float4*>(xs + i * kBsRC)[q];
-                for (int jt = bs; jt > 0; jt -= 8) {  // j = jt-1 down to jt-8, descending
-                    float uv[8];
+                for (int jt = bs; jt > 0; jt -= 16) {  // j = jt-1 down to jt-16, descending
+                    float uv[16];  // sixteen of the row's U values in flight
 #pragma unroll
-                    for (int u = 0; u < 8; u++) uv[u] = jt - 1 - u >= 0 ? at(i, r0 + jt - 1 - u) : 0.0f;
+                    for (int u = 0; u < 16; u++) uv[u] = jt - 1 - u >= 0 ? at(i, r0 + jt - 1 - u) : 0.0f;
 #pragma unroll
-                    for (int u = 0; u < 8; u++) {
+                    for (int u = 0; u < 16; u++) {
                         const int j = jt - 1 - u;
                         if (j < 0) break;
                         const float nu = -uv[u];
