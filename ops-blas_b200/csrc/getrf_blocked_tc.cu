@@ -533,17 +533,26 @@ lu_rows_update_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, 
     }
     if (vec) cp_async_wait_all();
     __syncthreads();
+    // one step of k: acc -= l * u, as packed f32x2 fmas (each lane an IEEE fma: fma(u, -l, acc)
+    // == fmaf(-l, u, acc) bit for bit)
     auto step = [&](int k) {
         float lv[8];
 #pragma unroll
         for (int a = 0; a < 8; a++) lv[a] = Ls[ty + 8 * a][k];
         const float4 u0 = *reinterpret_cast<const float4*>(&Us[k][8 * tx]);
         const float4 u1 = *reinterpret_cast<const float4*>(&Us[k][8 * tx + 4]);
-        const float uv[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+        const float2 up[4] = {make_float2(u0.x, u0.y), make_float2(u0.z, u0.w), make_float2(u1.x, u1.y),
+                              make_float2(u1.z, u1.w)};
 #pragma unroll
-        for (int a = 0; a < 8; a++)
+        for (int a = 0; a < 8; a++) {
+            const float2 nl = make_float2(-lv[a], -lv[a]);
 #pragma unroll
-            for (int b = 0; b < 8; b++) acc[a][b] = fmaf(-lv[a], uv[b], acc[a][b]);
+            for (int b = 0; b < 4; b++) {
+                const float2 r = __ffma2_rn(up[b], nl, make_float2(acc[a][2 * b], acc[a][2 * b + 1]));
+                acc[a][2 * b] = r.x;
+                acc[a][2 * b + 1] = r.y;
+            }
+        }
     };
     if (K == kBpW) {
 #pragma unroll 4
