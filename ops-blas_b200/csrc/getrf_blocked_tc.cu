@@ -8,7 +8,7 @@
 // a separate sector.
 //   0. lu_rows_in_kernel: A (by columns) into LU by rows, 32 x 32 tiles through shared memory.
 //   Per panel k0 = 0, 32, ...:
-//   1. lu_panel_kernel, one CTA per matrix, a thread per panel row (two above 256 rows):
+//   1. lu_panel_kernel, one CTA per matrix, two panel rows a thread:
 //      * factors the panel (rows k0..n-1, columns k0..k0+31) in FP32 in registers with implicit
 //        pivoting (`pos` tracks the reference's in-place order): pivot = the largest magnitude
 //        compared on the exponent and 14 mantissa bits (ties to the lowest position), multipliers
@@ -120,8 +120,12 @@ lu_rows_out_kernel(float* const* __restrict__ LUarr, int ld, int n)
     }
 }
 
-// Rows moved a round by the panel kernel's interchange step: 64 rows x 128 columns.
-constexpr int kMvCols = 128;
+// Rows moved a round by the panel kernel's interchange step: 64 rows x MVC columns (128, or 64
+// for the small CTAs, so that their shared memory lets more of them share an SM).
+template <int NT>
+struct PanelMv {
+    static constexpr int MVC = NT >= 256 ? 128 : 64;
+};
 
 // One CTA per matrix; thread t holds memory rows k0 + t + r * NT (r < RPT) of the panel. NT x RPT
 // covers the panel's rows; 128 registers a thread, so that 512 / NT CTAs share an SM.
@@ -140,6 +144,7 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
 {
     constexpr int NW = NT / 32;
     __shared__ BpSmem S;
+    constexpr int kMvCols = PanelMv<NT>::MVC;
     __shared__ __align__(16) float mvbuf[2 * kBpW * kMvCols];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long m = blockIdx.x;
@@ -317,13 +322,24 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
             l[r] = EXACT ? p[r][c] / pv : p[r][c] * rinv;
             if (upd[r]) p[r][c] = l[r];
         }
+        // p[j] -= l * u[j] for j > c: packed f32x2 fmas on the column pairs right of c (each lane
+        // an IEEE fma, fma(u, -l, p) == fmaf(-l, u, p) bit for bit)
 #pragma unroll
-        for (int j = 0; j < kBpW; j++) {
+        for (int j = 0; j < kBpW; j += 2) {
             if (j > c) {
-                const float u = prow[j];
+                const float2 u = make_float2(prow[j], prow[j + 1]);
 #pragma unroll
                 for (int r = 0; r < RPT; r++)
-                    if (upd[r]) p[r][j] = fmaf(-l[r], u, p[r][j]);
+                    if (upd[r]) {
+                        const float2 q = __ffma2_rn(u, make_float2(-l[r], -l[r]), make_float2(p[r][j], p[r][j + 1]));
+                        p[r][j] = q.x;
+                        p[r][j + 1] = q.y;
+                    }
+            } else if (j + 1 > c) {
+                const float u = prow[j + 1];
+#pragma unroll
+                for (int r = 0; r < RPT; r++)
+                    if (upd[r]) p[r][j + 1] = fmaf(-l[r], u, p[r][j + 1]);
             }
         }
     }
@@ -576,7 +592,7 @@ lu_rows_update_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, 
     }
 }
 
-// The panel kernel's CTA shape by panel rows: small CTAs share an SM, two rows a thread above 256.
+// The panel kernel's CTA shape by panel rows: two rows a thread, small CTAs share an SM.
 template <bool EXACT, bool PIVOT>
 static cudaError_t panel_launch(cudaStream_t st, float* const* T, int n, int ldt, int k0, int* piv, int* info,
                                 int* stat, char* scratch, long long l21_off, long long u12_off, long long per_matrix,
@@ -585,10 +601,10 @@ static cudaError_t panel_launch(cudaStream_t st, float* const* T, int n, int ldt
     const int mp = n - k0;
     const unsigned g = (unsigned)batch;
     if (mp <= 128)
-        lu_panel_kernel<128, 1, EXACT, PIVOT><<<g, 128, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
-                                                                  u12_off, per_matrix);
+        lu_panel_kernel<64, 2, EXACT, PIVOT><<<g, 64, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
+                                                                u12_off, per_matrix);
     else if (mp <= 256)
-        lu_panel_kernel<256, 1, EXACT, PIVOT><<<g, 256, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
+        lu_panel_kernel<128, 2, EXACT, PIVOT><<<g, 128, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
                                                                   u12_off, per_matrix);
     else if (mp <= 512)
         lu_panel_kernel<256, 2, EXACT, PIVOT><<<g, 256, 0, st>>>(T, n, ldt, k0, piv, info, stat, scratch, l21_off,
