@@ -35,8 +35,10 @@ constexpr int kBpW = 32;  // panel width = the update's K
 
 struct __align__(16) BpSmem {
     float crow[2][32][kBpW];  // per column parity and warp: the warp's pivot candidate row
-    unsigned ckey[2][32];     //   its key (the exact search: its magnitude bits)
-    int cpos[2][32];          //   (the exact search) its position
+    // per column (mod 3) the CTA's best pivot candidate: key << 5 | warp, by atomicMax; the
+    // exact search keys on the magnitude bits and then the position, the mixed one on its
+    // 32-bit approximate key
+    unsigned long long pkey[3];
     float l11[kBpW][kBpW + 1];
     int mv_src[2 * kBpW];     // rows whose position changed: memory row and destination row
     int mv_dst[2 * kBpW];
@@ -124,7 +126,7 @@ lu_rows_out_kernel(float* const* __restrict__ LUarr, int ld, int n)
 // for the small CTAs, so that their shared memory lets more of them share an SM).
 template <int NT>
 struct PanelMv {
-    static constexpr int MVC = NT >= 256 ? 128 : 64;
+    static constexpr int MVC = NT >= 128 ? 64 : 32;  // two buffers of 64 x MVC floats
 };
 
 // One CTA per matrix; thread t holds memory rows k0 + t + r * NT (r < RPT) of the panel. NT x RPT
@@ -145,7 +147,7 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
     constexpr int NW = NT / 32;
     __shared__ BpSmem S;
     constexpr int kMvCols = PanelMv<NT>::MVC;
-    __shared__ __align__(16) float mvbuf[2 * kBpW * kMvCols];
+    __shared__ __align__(16) float mvbuf[2][2 * kBpW * kMvCols];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long m = blockIdx.x;
     float* T = LUarr[m];  // by rows: T(i, j) = T[j + i * ldt]
@@ -160,7 +162,11 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
     // whole rows as float4 when every row start is 16-byte aligned (uniform per matrix)
     const bool vec = (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (ldt & 3) == 0 && pw == kBpW;
 
-    if (tid == 0) S.mv_cnt = 0;
+    if (tid == 0) {
+        S.mv_cnt = 0;
+        S.pkey[0] = 0ull;
+        S.pkey[1] = 0ull;
+    }
     if (inf0 != 0) {  // stopped at an earlier zero pivot
         if (!EXACT) {  // this step's update must change nothing
             for (int e = tid; e < (ntr > 0 ? ntr : 0) * kBpW; e += NT) {
@@ -242,10 +248,10 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
             }
             const unsigned wm = __reduce_max_sync(0xffffffffu, bm);
             const int wp = (int)__reduce_min_sync(0xffffffffu, bm == wm ? (unsigned)bp : 0x7fffffffu);
-            if (lane == 0) {
-                S.ckey[buf][warp] = wm;
-                S.cpos[buf][warp] = wp;
-            }
+            // the warp's best into the CTA's: magnitude, then the lower position, then the warp
+            if (lane == 0 && wp != 0x7fffffff)
+                atomicMax(&S.pkey[c % 3], ((unsigned long long)wm << 32) |
+                                              ((unsigned long long)(1023 - (wp - k0)) << 5) | (unsigned)warp);
 #pragma unroll
             for (int r = 0; r < RPT; r++)
                 if (valid[r] && pos[r] == wp && bp == wp) {
@@ -254,13 +260,11 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
                     for (int q = 0; q < kBpW / 4; q++)
                         dst[q] = make_float4(p[r][4 * q], p[r][4 * q + 1], p[r][4 * q + 2], p[r][4 * q + 3]);
                 }
+            if (tid == 0) S.pkey[(c + 1) % 3] = 0ull;  // read last at column c - 2, before this barrier
             __syncthreads();
-            const unsigned qm = lane < NW ? S.ckey[buf][lane] : 0u;
-            const int qp = lane < NW ? S.cpos[buf][lane] : 0x7fffffff;
-            const unsigned gm = __reduce_max_sync(0xffffffffu, qm);
-            ppos = (int)__reduce_min_sync(0xffffffffu, qm == gm ? (unsigned)qp : 0x7fffffffu);
-            const int bw = __ffs(__ballot_sync(0xffffffffu, lane < NW && qm == gm && qp == ppos)) - 1;
-            prow = S.crow[buf][bw < 0 ? 0 : bw];  // (position k is always a candidate: bw >= 0)
+            const unsigned long long key = S.pkey[c % 3];  // (position k is always a candidate)
+            ppos = k0 + 1023 - (int)((key >> 5) & 1023u);
+            prow = S.crow[buf][(int)(key & 31u)];
         } else {
             unsigned best = 0u;  // this thread's best candidate key (0: none)
 #pragma unroll
@@ -272,7 +276,7 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
                 best = key > best ? key : best;
             }
             const unsigned wkey = __reduce_max_sync(0xffffffffu, best);
-            if (lane == 0) S.ckey[buf][warp] = wkey;
+            if (lane == 0 && wkey != 0u) atomicMax(&S.pkey[c % 3], ((unsigned long long)wkey << 5) | (unsigned)warp);
             if (best != 0u && best == wkey) {  // keys are unique: one writer a warp
                 float4* dst = reinterpret_cast<float4*>(S.crow[buf][warp]);
 #pragma unroll
@@ -288,13 +292,13 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
                     }
                 }
             }
+            if (tid == 0) S.pkey[(c + 1) % 3] = 0ull;  // read last at column c - 2, before this barrier
             __syncthreads();
-            const unsigned qk = lane < NW ? S.ckey[buf][lane] : 0u;
-            const unsigned bk = __reduce_max_sync(0xffffffffu, qk);
-            const int bw = __ffs(__ballot_sync(0xffffffffu, lane < NW && qk == bk)) - 1;
+            const unsigned long long key = S.pkey[c % 3];
+            const unsigned bk = (unsigned)(key >> 5);
             nocand = bk == 0u;
             ppos = nocand ? k : k0 + 1023 - (int)(bk & 1023u);
-            prow = S.crow[buf][bw];
+            prow = S.crow[buf][(int)(key & 31u)];
         }
         const float pv = prow[c];
         if (PIVOT && tid == 0) pm[k] = ppos + 1;
@@ -391,11 +395,15 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
     const int cnt = S.mv_cnt;  // <= 64: each of the panel's interchanges moves two rows
     if (cnt > 0) {
         const int nx = n - pw;  // columns outside the panel
+        const int rounds = (nx + kMvCols - 1) / kMvCols;
         auto col_of = [&](int x) { return x < k0 ? x : x + pw; };
-        for (int x0 = 0; x0 < nx; x0 += kMvCols) {
+        // round rd: columns rd * kMvCols .. of every moved row into buffer rd & 1 (one cp.async group)
+        auto fetch = [&](int rd) {
+            const int x0 = rd * kMvCols;
+            float* b = mvbuf[rd & 1];
             for (int e = tid; e < cnt * (kMvCols / 4); e += NT) {
                 const int r = e / (kMvCols / 4), xq = x0 + (e % (kMvCols / 4)) * 4;
-                float* d = mvbuf + r * kMvCols + (xq - x0);
+                float* d = b + r * kMvCols + (xq - x0);
                 const float* srow = T + (long long)S.mv_src[r] * ldt;
                 if (vec && xq + 3 < nx) {
                     cp_async16(d, srow + col_of(xq));  // four columns on the same side of the panel
@@ -406,11 +414,22 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
                 }
             }
             cp_async_commit();
-            cp_async_wait_all();
+        };
+        // two rounds in flight: a round's values are all read (into its buffer) before any of them
+        // is written; rounds cover disjoint columns
+        fetch(0);
+        if (rounds > 1) fetch(1);
+        for (int rd = 0; rd < rounds; rd++) {
+            if (rd + 1 < rounds)
+                cp_async_wait_group<1>();
+            else
+                cp_async_wait_group<0>();
             __syncthreads();
+            const int x0 = rd * kMvCols;
+            const float* b = mvbuf[rd & 1];
             for (int e = tid; e < cnt * (kMvCols / 4); e += NT) {
                 const int r = e / (kMvCols / 4), xq = x0 + (e % (kMvCols / 4)) * 4;
-                const float* sv = mvbuf + r * kMvCols + (xq - x0);
+                const float* sv = b + r * kMvCols + (xq - x0);
                 float* drow = T + (long long)S.mv_dst[r] * ldt;
                 if (vec && xq + 3 < nx) {
                     *reinterpret_cast<float4*>(drow + col_of(xq)) = *reinterpret_cast<const float4*>(sv);
@@ -421,6 +440,7 @@ lu_panel_kernel(float* const* __restrict__ LUarr, int n, int ldt, int k0, int* _
                 }
             }
             __syncthreads();
+            if (rd + 2 < rounds) fetch(rd + 2);
         }
     }
     if (ntr <= 0) return;  // last panel: no trailing block
