@@ -60,10 +60,8 @@ refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, con
                        int it, int final_check, int* __restrict__ done, double* __restrict__ berr,
                        int* __restrict__ iters)
 {
-    extern __shared__ double xs[];  // [n + 8][kResMaxRhs]
-    __shared__ double red[kResThreads / 32];
+    extern __shared__ double xs[];  // [n + 16][kResMaxRhs]
     __shared__ double s_anorm;
-    __shared__ double s_berr;
     const long long m = blockIdx.x;
     const float* A = Aarray[m];
     const float* B = Barray[m];
@@ -75,15 +73,30 @@ refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, con
         if (tid == 0 && !final_check) Dact[m] = nullptr;
         return;
     }
-    auto block_max = [&](double v) {
+    const int lane = tid & 31, warp = tid >> 5;
+    // block maxima of K values per thread at once: shuffles within the warp, one row of K per warp
+    // in shared memory, then a thread per value across the warps -- two barriers for all K
+    __shared__ double red[kResThreads / 32][2 * kResMaxRhs + 1];
+    __shared__ double s_max[2 * kResMaxRhs + 1];
+    auto block_max_all = [&](auto& v) {
+        constexpr int K = (int)(sizeof(v) / sizeof(double));
+        static_assert(K <= 2 * kResMaxRhs + 1, "reduction width");
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
-        if ((tid & 31) == 0) red[tid >> 5] = v;
+        for (int q = 0; q < K; q++) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v[q] = fmax(v[q], __shfl_xor_sync(0xffffffffu, v[q], off));
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < K; q++) red[warp][q] = v[q];
+        }
         __syncthreads();
-        double r = red[0];
-        for (int q = 1; q < kResThreads / 32; q++) r = fmax(r, red[q]);
+        if (tid < K) {
+            double r = red[0][tid];
+            for (int w = 1; w < kResThreads / 32; w++) r = fmax(r, red[w][tid]);
+            s_max[tid] = r;
+        }
         __syncthreads();
-        return r;
     };
     // r = b - A x per right-hand-side chunk; the row sums of |A| (for ||A||_inf) are gathered in
     // the first chunk's pass over A, so A is read once per chunk. The column maxima of |x| and |b|
@@ -94,50 +107,66 @@ refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, con
     for (int c0 = 0; c0 < nrhs; c0 += kResMaxRhs) {
         const int cw = min(kResMaxRhs, nrhs - c0);
         __syncthreads();
-        for (int e = tid; e < (n + 8) * kResMaxRhs; e += kResThreads) {  // 8 zero rows of padding
-            const int i = e / kResMaxRhs, c = e % kResMaxRhs;
-            xs[i * kResMaxRhs + c] = (c < cw && i < n) ? (double)X[i + (long long)(c0 + c) * ldx] : 0.0;
+        // X chunk into shared memory as FP64, eight loads in flight before their stores
+        const int total = (n + 16) * kResMaxRhs;  // 16 zero rows of padding
+        for (int base = tid; base < total; base += 8 * kResThreads) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int e = base + u * kResThreads, i = e / kResMaxRhs, c = e % kResMaxRhs;
+                v[u] = (e < total && c < cw && i < n) ? X[i + (long long)(c0 + c) * ldx] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (base + u * kResThreads < total) xs[base + u * kResThreads] = (double)v[u];
         }
         __syncthreads();
-        for (int c = 0; c < cw; c++) {
-            double xm = 0.0, bm = 0.0;
+        {  // column maxima of |x| and |b| (FP32 values: their maxima are exact)
+            double v[2 * kResMaxRhs];
+#pragma unroll
+            for (int q = 0; q < 2 * kResMaxRhs; q++) v[q] = 0.0;
             for (int i = tid; i < n; i += kResThreads) {
-                xm = fmax(xm, fabs(xs[i * kResMaxRhs + c]));
-                bm = fmax(bm, fabs((double)B[i + (long long)(c0 + c) * ldb]));
+                float bv[kResMaxRhs];
+#pragma unroll
+                for (int c = 0; c < kResMaxRhs; c++) bv[c] = c < cw ? B[i + (long long)(c0 + c) * ldb] : 0.0f;
+#pragma unroll
+                for (int c = 0; c < kResMaxRhs; c++) {
+                    v[c] = fmax(v[c], fabs(xs[i * kResMaxRhs + c]));
+                    v[kResMaxRhs + c] = fmax(v[kResMaxRhs + c], (double)fabsf(bv[c]));
+                }
             }
-            xm = block_max(xm);
-            bm = block_max(bm);
-            if (tid == 0) {
-                s_xn[c] = xm;
-                s_bn[c] = bm;
+            block_max_all(v);
+            if (tid < kResMaxRhs) {
+                s_xn[tid] = s_max[tid];
+                s_bn[tid] = s_max[kResMaxRhs + tid];
             }
         }
-        double rmaxs[kResMaxRhs];
+        double rmaxs[kResMaxRhs + 1];  // [kResMaxRhs]: the row sums' maximum (first chunk)
 #pragma unroll
-        for (int c = 0; c < kResMaxRhs; c++) rmaxs[c] = 0.0;
+        for (int c = 0; c <= kResMaxRhs; c++) rmaxs[c] = 0.0;
         for (int i = tid; i < n; i += kResThreads) {
             double r[kResMaxRhs];
 #pragma unroll
             for (int c = 0; c < kResMaxRhs; c++) r[c] = c < cw ? (double)B[i + (long long)(c0 + c) * ldb] : 0.0;
             double asum = 0.0;
-            for (int j0 = 0; j0 < n; j0 += 8) {
-                float av[8];  // eight independent loads in flight before the FMAs that use them
+            for (int j0 = 0; j0 < n; j0 += 16) {
+                float av[16];  // sixteen independent loads in flight before the FMAs that use them
 #pragma unroll
-                for (int u = 0; u < 8; u++) av[u] = j0 + u < n ? A[i + (long long)(j0 + u) * lda] : 0.0f;
+                for (int u = 0; u < 16; u++) av[u] = j0 + u < n ? A[i + (long long)(j0 + u) * lda] : 0.0f;
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
+                for (int u = 0; u < 16; u++) {
                     const double a = (double)av[u];
                     asum += fabs(a);
                     const double2* xr = reinterpret_cast<const double2*>(xs + (j0 + u) * kResMaxRhs);
 #pragma unroll
                     for (int q = 0; q < kResMaxRhs / 2; q++) {
-                        const double2 v = xr[q];  // rows n..n+7 are zero padding
+                        const double2 v = xr[q];  // rows n..n+15 are zero padding
                         r[2 * q] = fma(-a, v.x, r[2 * q]);
                         r[2 * q + 1] = fma(-a, v.y, r[2 * q + 1]);
                     }
                 }
             }
-            if (c0 == 0) rowmax = fmax(rowmax, asum);
+            rmaxs[kResMaxRhs] = fmax(rmaxs[kResMaxRhs], asum);
 #pragma unroll
             for (int c = 0; c < kResMaxRhs; c++) {
                 if (c < cw) {
@@ -146,19 +175,17 @@ refine_residual_kernel(int n, int nrhs, const float* const* Aarray, int lda, con
                 }
             }
         }
+        block_max_all(rmaxs);
         if (c0 == 0) {
-            const double anorm = block_max(rowmax);
-            if (tid == 0) s_anorm = anorm;
-            __syncthreads();
+            rowmax = s_max[kResMaxRhs];
+            if (tid == 0) s_anorm = rowmax;
         }
-#pragma unroll
-        for (int c = 0; c < kResMaxRhs; c++) {  // compile-time index keeps rmaxs in registers
-            if (c < cw) {                          // cw is uniform: block_max's barriers stay uniform
-                const double rn = block_max(rmaxs[c]);
-                const double den = s_anorm * s_xn[c] + s_bn[c];
-                const double e = den > 0.0 ? rn / den : (rn > 0.0 ? INFINITY : 0.0);
-                worst = fmax(worst, e);
-            }
+        __syncthreads();
+        for (int c = 0; c < cw; c++) {
+            const double rn = s_max[c];
+            const double den = s_anorm * s_xn[c] + s_bn[c];
+            const double e = den > 0.0 ? rn / den : (rn > 0.0 ? INFINITY : 0.0);
+            worst = fmax(worst, e);
         }
     }
     __syncthreads();
@@ -275,7 +302,7 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedEx(
     if (err != cudaSuccess) return launch_status(kApi, err);
     const int rhs_chunk = nrhs < kResMaxRhs ? nrhs : kResMaxRhs;
     (void)rhs_chunk;
-    const size_t rsm = (size_t)(n + 8) * kResMaxRhs * 8;
+    const size_t rsm = (size_t)(n + 16) * kResMaxRhs * 8;
     if (rsm > 200 * 1024) {
         log_error(kApi, "n=%d exceeds the residual kernel's shared-memory limit", n);
         return ACLBLAS_STATUS_NOT_SUPPORTED;
@@ -401,7 +428,7 @@ extern "C" aclblasStatus_t aclblasSgetrfsRefineBatchedStaticScratch(
                   (dbytes + 20) * (size_t)batchCount + 512, cap);
         return ACLBLAS_STATUS_INVALID_VALUE;
     }
-    const size_t rsm = (size_t)(n + 8) * kResMaxRhs * 8;
+    const size_t rsm = (size_t)(n + 16) * kResMaxRhs * 8;
     if (rsm > 200 * 1024) {
         log_error(kApi, "n=%d exceeds the residual kernel's shared-memory limit", n);
         return ACLBLAS_STATUS_NOT_SUPPORTED;
