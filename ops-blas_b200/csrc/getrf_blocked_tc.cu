@@ -72,33 +72,96 @@ __device__ __forceinline__ void tf32_split(float x, float& hi, float& lo)
     lo = tf32_rne(x - hi);
 }
 
-// T(i, j) = A(i, j): A by columns (lda) into LU by rows (ldt). Block = 32 x 8 threads, one
-// 32 x 32 tile (blockIdx.y) of one matrix (blockIdx.x).
+// The transposes move 64 x 64 tiles with 256 threads: each thread has four 16-byte loads (or
+// sixteen 4-byte loads when rows are not 16-byte aligned) of a tile in flight, the tile is
+// re-read across from shared memory (row stride 65: conflict-free) and written as columns.
+constexpr int kTpT = 64;
+
+// tile (r0, c0) of the column-major matrix X (ld) into s[c][r] (r, c < 64, zeros outside n x n)
+__device__ __forceinline__ void tp_load(float (*s)[kTpT + 1], const float* X, long long ld, int r0, int c0, int n,
+                                        bool vec)
+{
+    const int tid = threadIdx.x;
+    if (vec && r0 + kTpT <= n) {
+        constexpr int K = kTpT * kTpT / 4 / 256;
+        float4 v[K];  // every load in flight before the first store
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int e = tid + 256 * k, c = e / (kTpT / 4), rq = (e % (kTpT / 4)) * 4;
+            v[k] = c0 + c < n ? *reinterpret_cast<const float4*>(X + (r0 + rq) + (long long)(c0 + c) * ld)
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int e = tid + 256 * k, c = e / (kTpT / 4), rq = (e % (kTpT / 4)) * 4;
+            s[c][rq] = v[k].x;
+            s[c][rq + 1] = v[k].y;
+            s[c][rq + 2] = v[k].z;
+            s[c][rq + 3] = v[k].w;
+        }
+    } else {
+        constexpr int K = kTpT * kTpT / 256;
+        float v[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int e = tid + 256 * k, c = e / kTpT, r = e % kTpT;
+            v[k] = (r0 + r < n && c0 + c < n) ? X[(r0 + r) + (long long)(c0 + c) * ld] : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int e = tid + 256 * k;
+            s[e / kTpT][e % kTpT] = v[k];
+        }
+    }
+}
+
+// Y(r0 + r, c0 + c) = s[r][c] (the transpose of the tile s holds), column-major Y (ld)
+__device__ __forceinline__ void tp_store(const float (*s)[kTpT + 1], float* Y, long long ld, int r0, int c0, int n,
+                                         bool vec)
+{
+    const int tid = threadIdx.x;
+    if (vec && r0 + kTpT <= n) {
+#pragma unroll
+        for (int k = 0; k < kTpT * kTpT / 4 / 256; k++) {
+            const int e = tid + 256 * k, c = e / (kTpT / 4), rq = (e % (kTpT / 4)) * 4;
+            if (c0 + c < n)
+                *reinterpret_cast<float4*>(Y + (r0 + rq) + (long long)(c0 + c) * ld) =
+                    make_float4(s[rq][c], s[rq + 1][c], s[rq + 2][c], s[rq + 3][c]);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kTpT * kTpT / 256; k++) {
+            const int e = tid + 256 * k, c = e / kTpT, r = e % kTpT;
+            if (r0 + r < n && c0 + c < n) Y[(r0 + r) + (long long)(c0 + c) * ld] = s[r][c];
+        }
+    }
+}
+
+// T(i, j) = A(i, j): A by columns (lda) into LU by rows (ldt), i.e. the storage of T is the
+// transpose of A's. One 64 x 64 tile (blockIdx.y) of one matrix (blockIdx.x).
 __global__ void __launch_bounds__(256)
 lu_rows_in_kernel(const float* const* __restrict__ Aarr, int lda, float* const* __restrict__ Tarr, int ldt, int n)
 {
-    __shared__ float tile[32][33];
-    const int nt = (n + 31) / 32;
-    const int i0 = (int)(blockIdx.y % nt) * 32, j0 = (int)(blockIdx.y / nt) * 32;
+    __shared__ float tile[kTpT][kTpT + 1];
+    const int nt = (n + kTpT - 1) / kTpT;
+    const int i0 = (int)(blockIdx.y % nt) * kTpT, j0 = (int)(blockIdx.y / nt) * kTpT;
     const float* A = Aarr[blockIdx.x];
     float* T = Tarr[blockIdx.x];
-    const int x = threadIdx.x & 31, y = threadIdx.x >> 5;
-#pragma unroll
-    for (int r = y; r < 32; r += 8)
-        if (i0 + x < n && j0 + r < n) tile[r][x] = A[(i0 + x) + (long long)(j0 + r) * lda];
+    const bool vec = (reinterpret_cast<uintptr_t>(A) & 15) == 0 && (lda & 3) == 0 &&
+                     (reinterpret_cast<uintptr_t>(T) & 15) == 0 && (ldt & 3) == 0;
+    tp_load(tile, A, lda, i0, j0, n, vec);  // tile[c][r] = A(i0 + r, j0 + c)
     __syncthreads();
-#pragma unroll
-    for (int r = y; r < 32; r += 8)
-        if (i0 + r < n && j0 + x < n) T[(j0 + x) + (long long)(i0 + r) * ldt] = tile[x][r];
+    tp_store(tile, T, ldt, j0, i0, n, vec);  // storage (j0 + r, i0 + c) = tile[r][c] = A(i0 + c, j0 + r)
 }
 
 // In-place transpose of the n x n storage matrix S(r, c) = LU[r + c * ld]: the by-rows factors
-// become the by-columns LU. One pair of 32 x 32 tiles (I, J), I <= J, per CTA (blockIdx.y).
+// become the by-columns LU (and back). One pair of 64 x 64 tiles (I, J), I <= J, per CTA
+// (blockIdx.y).
 __global__ void __launch_bounds__(256)
 lu_rows_out_kernel(float* const* __restrict__ LUarr, int ld, int n)
 {
-    __shared__ float ta[32][33], tb[32][33];
-    const int nt = (n + 31) / 32;
+    __shared__ float ta[kTpT][kTpT + 1], tb[kTpT][kTpT + 1];
+    const int nt = (n + kTpT - 1) / kTpT;
     int p = (int)blockIdx.y, I = 0;
     while (p >= nt - I) {
         p -= nt - I;
@@ -106,20 +169,13 @@ lu_rows_out_kernel(float* const* __restrict__ LUarr, int ld, int n)
     }
     const int J = I + p;
     float* S = LUarr[blockIdx.x];
-    const int x = threadIdx.x & 31, y = threadIdx.x >> 5;
-    const int a0 = I * 32, b0 = J * 32;
-#pragma unroll
-    for (int r = y; r < 32; r += 8) {
-        if (a0 + x < n && b0 + r < n) ta[r][x] = S[(a0 + x) + (long long)(b0 + r) * ld];  // S(a0+x, b0+r)
-        if (I != J && b0 + x < n && a0 + r < n) tb[r][x] = S[(b0 + x) + (long long)(a0 + r) * ld];
-    }
+    const bool vec = (reinterpret_cast<uintptr_t>(S) & 15) == 0 && (ld & 3) == 0;
+    const int a0 = I * kTpT, b0 = J * kTpT;
+    tp_load(ta, S, ld, a0, b0, n, vec);                 // ta[c][r] = S(a0 + r, b0 + c)
+    if (I != J) tp_load(tb, S, ld, b0, a0, n, vec);     // tb[c][r] = S(b0 + r, a0 + c)
     __syncthreads();
-#pragma unroll
-    for (int r = y; r < 32; r += 8) {
-        // S'(a0 + x, b0 + r) = S(b0 + r, a0 + x) and S'(b0 + x, a0 + r) = S(a0 + r, b0 + x)
-        if (I != J && a0 + x < n && b0 + r < n) S[(a0 + x) + (long long)(b0 + r) * ld] = tb[x][r];
-        if (b0 + x < n && a0 + r < n) S[(b0 + x) + (long long)(a0 + r) * ld] = ta[x][r];
-    }
+    if (I != J) tp_store(tb, S, ld, a0, b0, n, vec);    // S'(a0 + r, b0 + c) = tb[r][c] = S(b0 + c, a0 + r)
+    tp_store(ta, S, ld, b0, a0, n, vec);                // S'(b0 + r, a0 + c) = ta[r][c] = S(a0 + c, b0 + r)
 }
 
 // Rows moved a round by the panel kernel's interchange step: 64 rows x MVC columns (128, or 64
@@ -645,7 +701,7 @@ cudaError_t getrf_rows_launch(cudaStream_t st, float* const* Aarray, int n, int 
     if (err == cudaSuccess && info != nullptr) err = cudaMemsetAsync(info, 0, sizeof(int) * (size_t)batch, st);
     if (err == cudaSuccess && piv != nullptr) err = cudaMemsetAsync(piv, 0, sizeof(int) * (size_t)n * batch, st);
     if (err != cudaSuccess) return err;
-    const int nt = (n + 31) / 32;
+    const int nt = (n + kTpT - 1) / kTpT;
     const dim3 tgrid((unsigned)batch, (unsigned)(nt * (nt + 1) / 2));
     lu_rows_out_kernel<<<tgrid, 256, 0, st>>>(Aarray, lda, n);  // in place: by columns -> by rows
     for (int k0 = 0; k0 < n; k0 += kBpW) {
@@ -689,7 +745,7 @@ cudaError_t getrf_blocked_tc_launch(cudaStream_t st, const float* const* Aarray,
                                                  L.per_matrix / 4, batch);
     init_ptr_array_kernel<<<bgrid, 256, 0, st>>>(u12p, reinterpret_cast<float*>(base + L.u12),
                                                  L.per_matrix / 4, batch);
-    const int nt = (n + 31) / 32;
+    const int nt = (n + kTpT - 1) / kTpT;
     lu_rows_in_kernel<<<dim3((unsigned)batch, (unsigned)(nt * nt)), 256, 0, st>>>(Aarray, lda, LUarray, ldlu, n);
     for (int k0 = 0; k0 < n; k0 += kBpW) {
         err = panel_launch<false, true>(st, LUarray, n, ldlu, k0, piv, info, info, base, L.l21, L.u12, L.per_matrix,
