@@ -62,28 +62,38 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
     };
 
     // ---- interchanges (sgetrs_batched_kernel.cpp:94-100: out-of-range or zero pivots skipped) ----
-    for (int i = tid; i < n; i += kBsThreads) {
-        perm[i] = i;
-        pv[i] = ipiv ? ipiv[m * n + i] - 1 : i;
-    }
+    for (int i = tid; i < n; i += kBsThreads) pv[i] = ipiv ? ipiv[m * n + i] - 1 : i;
     __syncthreads();
-    if (tid == 0) {
-        for (int k = 0; k < n; k++) {
+    // perm[i] = the row that the swap sequence k = 0..n-1 brings to position i: i traced back
+    // through the swaps in reverse order, every position in parallel (instead of one thread
+    // applying the n swaps in turn)
+    for (int i = tid; i < n; i += kBsThreads) {
+        int x = i;
+#pragma unroll 8
+        for (int k = n - 1; k >= 0; k--) {
             const int p = pv[k];
-            if ((unsigned)p < (unsigned)n && p != k) {
-                const int t = perm[k];
-                perm[k] = perm[p];
-                perm[p] = t;
-            }
+            const bool sw = (unsigned)p < (unsigned)n && p != k;
+            x = (sw && x == k) ? p : ((sw && x == p) ? k : x);
         }
+        perm[i] = x;
     }
     __syncthreads();
 
     for (int c0 = 0; c0 < nrhs; c0 += kBsRC) {
         const int cw = min(kBsRC, nrhs - c0);
-        for (int e = tid; e < n * kBsRC; e += kBsThreads) {
-            const int i = e % n, c = e / n;
-            xs[i * kBsRC + c] = c < cw ? B[perm[i] + (long long)(c0 + c) * ldb] : 0.0f;
+        // B gathered through the interchanges, eight loads in flight before their stores
+        for (int base = tid; base < n * kBsRC; base += 8 * kBsThreads) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int e = base + u * kBsThreads, i = e % n, c = e / n;
+                v[u] = (e < n * kBsRC && c < cw) ? B[perm[i] + (long long)(c0 + c) * ldb] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int e = base + u * kBsThreads;
+                if (e < n * kBsRC) xs[(e % n) * kBsRC + e / n] = v[u];
+            }
         }
         __syncthreads();
 
