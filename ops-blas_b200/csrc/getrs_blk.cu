@@ -105,6 +105,23 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
             const float* blk = blks + bi * kBsB * kBsLd;
             cp_async_wait_all();
             __syncthreads();
+            if (bs == kBsB) {
+                // a whole block: warp 0 alone, lane = right-hand side, the block's 32 unknowns in
+                // registers, x_i -= L(i,j) x_j for j < i in turn (each element's updates in j order,
+                // as the shuffle form below); a third of the instructions of that form
+                if (warp == 0 && lane < cw) {
+                    float x[kBsB];
+#pragma unroll
+                    for (int i = 0; i < kBsB; i++) x[i] = xs[(r0 + i) * kBsRC + lane];
+#pragma unroll
+                    for (int i = 1; i < kBsB; i++)
+#pragma unroll
+                        for (int j = 0; j < kBsB; j++)
+                            if (j < i) x[i] = fmaf(-blk[j * kBsLd + i], x[j], x[i]);
+#pragma unroll
+                    for (int i = 0; i < kBsB; i++) xs[(r0 + i) * kBsRC + lane] = x[i];
+                }
+            } else {
             // two right-hand sides per warp, their dependency chains interleaved
             for (int c = warp; c < cw; c += 2 * (kBsThreads / 32)) {
                 const int c1 = c + kBsThreads / 32;
@@ -132,6 +149,7 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                     xs[(r0 + lane) * kBsRC + c] = y0;
                     if (two) xs[(r0 + lane) * kBsRC + c1] = y1;
                 }
+            }
             }
             __syncthreads();
             if (r0 + kBsB < n) stage_blk(r0 + kBsB, bi ^ 1);
@@ -173,6 +191,24 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
             const float* blk = blks + bi * kBsB * kBsLd;
             cp_async_wait_all();
             __syncthreads();
+            if (bs == kBsB) {
+                // a whole block: warp 0 alone, lane = right-hand side; for j from the bottom,
+                // x_j /= U(j,j), then x_i -= U(i,j) x_j for i < j (the reference's order)
+                if (warp == 0 && lane < cw) {
+                    float x[kBsB];
+#pragma unroll
+                    for (int i = 0; i < kBsB; i++) x[i] = xs[(r0 + i) * kBsRC + lane];
+#pragma unroll
+                    for (int j = kBsB - 1; j >= 0; j--) {
+                        x[j] = x[j] / blk[j * kBsLd + j];
+#pragma unroll
+                        for (int i = 0; i < kBsB; i++)
+                            if (i < j) x[i] = fmaf(-blk[j * kBsLd + i], x[j], x[i]);
+                    }
+#pragma unroll
+                    for (int i = 0; i < kBsB; i++) xs[(r0 + i) * kBsRC + lane] = x[i];
+                }
+            } else {
             // two right-hand sides per warp; every lane divides (no divergence), lane j's quotient
             // x_j = y_j / U(j,j) is the one broadcast
             for (int c = warp; c < cw; c += 2 * (kBsThreads / 32)) {
@@ -209,6 +245,7 @@ getrs_blk_kernel(const float* const* __restrict__ Aarray, int n, int lda, const 
                     xs[(r0 + lane) * kBsRC + c] = y0;
                     if (two) xs[(r0 + lane) * kBsRC + c1] = y1;
                 }
+            }
             }
             __syncthreads();
             if (kb > 0) stage_blk(r0 - kBsB, bi ^ 1);
