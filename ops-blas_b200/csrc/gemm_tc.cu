@@ -4,28 +4,34 @@
 //   offsets a_off / b_off / c_off added to every matrix pointer)
 //
 // Persistent: one CTA per SM walks the 128 x 128 tiles of C (tile t, t + #CTAs, ...: the CTAs
-// work on neighbouring tiles of the same matrices at the same time, which share operands in L2),
-// nine warps:
+// work on neighbouring tiles of the same matrices at the same time, which share operands in L2;
+// or, for the LU's update, one contiguous range of tiles per CTA, so that consecutive tiles keep
+// their matrix's tensor maps), nine warps:
 //   * warps 0-3 produce: per K tile (128 bytes of K: 64 FP16/BF16, 128 FP8 or 32 TF32 values) they
 //     fill a stage of a ring that runs across tile boundaries with op(A) rows m0..m0+127 and
 //     op(B)^T rows n0..n0+127 in the 128-byte swizzled canonical UMMA layout of the operand's
 //     own orientation in global memory (TcLayout below): K-major for a K-contiguous source (A
 //     with op T, B with op N), MN-major for an MN-contiguous one (A with op N, B with op T) --
 //     except TF32 operands, which are always staged K-major.
-//     Native FP16 / BF16 / FP8 operands whose matrix and leading dimension are 16-byte aligned
-//     move by cp.async (16 bytes per copy, zero fill at the edges, no registers held), and each
-//     producer thread's cp.async.mbarrier.arrive lets full[s] complete once its copies have
-//     landed, so the producers never wait for their own copies; FP32 operands (rounded to TF32 or
-//     BF16, or split into TF32 high and low parts, 16-byte loads in 4 x 4 blocks) and unaligned
-//     matrices go through registers and a proxy fence before the arrival;
+//     With the handle's tensor-map slots, warp 0 loads each stage by TMA: every CTA keeps its
+//     per-matrix maps in a global slot and rewrites their base address when it moves to another
+//     matrix (tensormap.replace + a release / acquire proxy fence). FP32 operands arrive by TMA
+//     when both are K-contiguous and are rounded to TF32 in shared memory by warps 1-3, or arrive
+//     already split into TF32 high and low planes (the LU's update). Otherwise the producers copy
+//     by cp.async (16 bytes per copy, zero fill at the edges) or, for unaligned matrices and FP32
+//     conversions, through registers;
 //   * warp 4 issues the MMAs (one elected thread): per stage four K steps of 32 bytes,
 //     tcgen05.mma kind::f16 / kind::f8f6f4 / kind::tf32 (three products hi*hi + hi*lo + lo*hi
 //     with SPLIT) into one of two 128 x 128 FP32 accumulators in TMEM (256 columns), alternating
 //     per tile; tcgen05.commit frees each stage (empty[s]) and, after a tile's last stage, hands
 //     the accumulator to the epilogue (acc_full[b]);
-//   * warps 5-8 drain the other accumulator meanwhile: each reads its TMEM lane quarter
-//     (tcgen05.ld, 32 rows), releases the accumulator (acc_empty[b]) and applies alpha / beta to
-//     C in C's type, coalesced along the columns.
+//   * warps 5-8 drain the other accumulator meanwhile, in 128 x 32 chunks: each reads its TMEM
+//     lane quarter (tcgen05.ld, 32 rows), releases the accumulator (acc_empty[b]) after the last
+//     chunk, and applies alpha / beta in C's type. With a tensor map for C the chunks of C are
+//     loaded by TMA into a ring of staging buffers before the accumulator is ready (the LU plan:
+//     eight buffers, the next tile's chunks loaded while this tile is combined), combined in
+//     place and stored by TMA; without one, C is read and written with coalesced loads and
+//     stores, the next chunk's values loaded while the current one is stored.
 // Every mbarrier wait is bounded. A wait that gives up sets the CTA's abort flag (every role then
 // stops) and kStatusTcGemmTimeout in the handle's status word; the copies and MMAs already in
 // flight are waited for (bounded) before the TMEM is released, and the tiles not finished keep
