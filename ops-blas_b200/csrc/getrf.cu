@@ -225,7 +225,7 @@ aclblasStatus_t opsblas::getrf_batched_impl(aclblasHandle_t handle, int n, float
         reg_default_shape(n, rows, warps);
         return launch_status(kApi, getrf_reg_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize, rows,
                                                     warps));
-    } else if (getrf_rows_supported(n) && stat != nullptr) {
+    } else if (getrf_rows_supported(n, batchSize) && stat != nullptr) {
         return launch_status(kApi, getrf_rows_launch(st, Aarray, n, lda, PivotArray, infoArray, stat, batchSize));
     } else if (getrf_large_supported(n)) {
         return launch_status(kApi, getrf_large_launch(st, Aarray, n, lda, PivotArray, infoArray, batchSize));

@@ -691,12 +691,18 @@ static cudaError_t panel_launch(cudaStream_t st, float* const* T, int n, int ldt
     return cudaGetLastError();
 }
 
-bool getrf_rows_supported(int n) { return n > 128 && n <= 1024; }
+bool getrf_rows_supported(int n, int batch)
+{
+    if (n <= 128 || n > 1024) return false;
+    // the update's grid (batch x its tiles) must fit a 31-bit grid dimension
+    const long long max_tiles = (long long)((n + kRuRows - 1) / kRuRows) * ((n - kBpW + kRuCols - 1) / kRuCols);
+    return (long long)batch * max_tiles <= 0x7fffffffLL;
+}
 
 cudaError_t getrf_rows_launch(cudaStream_t st, float* const* Aarray, int n, int lda, int* piv, int* info, int* stat,
                               int batch)
 {
-    if (!getrf_rows_supported(n) || batch <= 0) return cudaErrorInvalidValue;
+    if (batch <= 0 || !getrf_rows_supported(n, batch)) return cudaErrorInvalidValue;
     cudaError_t err = cudaMemsetAsync(stat, 0, sizeof(int) * (size_t)batch, st);
     if (err == cudaSuccess && info != nullptr) err = cudaMemsetAsync(info, 0, sizeof(int) * (size_t)batch, st);
     if (err == cudaSuccess && piv != nullptr) err = cudaMemsetAsync(piv, 0, sizeof(int) * (size_t)n * batch, st);

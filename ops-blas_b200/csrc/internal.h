@@ -136,7 +136,7 @@ cudaError_t getrf_blocked_tc_launch(cudaStream_t st, const float* const* Aarray,
 // getrf_blocked_tc.cu: 128 < n <= 1024, the plain FP32 blocked LU on a by-rows copy made in place
 // (bit-identical to the reference's unblocked order); piv and info may be nullptr (no-pivot mode:
 // piv == nullptr); stat: batch ints of device scratch (the matrices' stop codes).
-bool getrf_rows_supported(int n);
+bool getrf_rows_supported(int n, int batch);
 // aclblasSgetrfBatched with the blocked path's stop codes in `stat` (batch ints of device memory
 // that the caller does not use otherwise; nullptr: the blocked path is not taken).
 aclblasStatus_t getrf_batched_impl(aclblasHandle_t handle, int n, float* const Aarray[], int lda, int* PivotArray,
