@@ -5,8 +5,8 @@
 //   N  : row interchanges k = 0..n-1, unit-L forward solve, U backward solve with division;
 //   T/C: U^T forward solve with division, unit L^T backward solve, interchanges k = n-1..0.
 // B200 kernels:
-//   n <= 32, nrhs == 1 : getrs_small_kernel, rows of LU in registers, shuffle broadcasts;
-//   n <= 32, nrhs >= 2 : getrs_rhs_kernel, one lane per right-hand side, LU staged in shared
+//   n <= 32, trans N, nrhs == 1 : getrs_small_kernel, rows of LU in registers, shuffle broadcasts;
+//   n <= 32, otherwise : getrs_rhs_kernel, one lane per right-hand side, LU staged in shared
 //                        memory by cp.async;
 //   n  > 32, trans N   : getrs_trhs_kernel<false> (getrs_trhs.cu), one thread per right-hand side,
 //                        for n <= 128 with at least 65536 right-hand sides in the batch; otherwise

@@ -8,11 +8,14 @@
 namespace opsblas {
 
 // ---------------------------------------------------------------------------------------
-// nrhs == 1, n <= 32: lane r of a warp segment holds row r (trans N) or column r (trans T)
-// of LU in registers and entry r of the right-hand side; the interchanges are folded into
-// the row the lane loads (N) or stores (T); solution entries are broadcast by shuffles.
+// nrhs == 1, n <= 32, trans N: lane r of a warp segment holds row r of LU in registers and
+// entry r of the right-hand side; the interchanges are folded into the row the lane loads;
+// solution entries are broadcast by shuffles. Each x[i] takes its updates in the reference's
+// order (j ascending in the L sweep, descending in the U sweep). Trans T / C goes to
+// getrs_rhs_kernel instead: the reference's L^T sweep adds x[j]'s terms with i ascending,
+// which a lane per column can only follow one position at a time.
 // ---------------------------------------------------------------------------------------
-template <int N, bool TRANS>
+template <int N>
 __global__ void __launch_bounds__(kSmallWarps * 32)
 getrs_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* __restrict__ ipiv,
                    float* const* __restrict__ Barray, int ldb, int batch)
@@ -36,7 +39,7 @@ getrs_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* 
     for (int j = 0; j < N; j++) lu[j] = 0.0f;
     if (rvalid) {
 #pragma unroll
-        for (int j = 0; j < N; j++) lu[j] = TRANS ? A[j + (long long)r * lda] : A[r + (long long)j * lda];
+        for (int j = 0; j < N; j++) lu[j] = A[r + (long long)j * lda];
     }
 
     int* pv = &pbuf[warp][seg * S::SEG];
@@ -45,38 +48,25 @@ getrs_small_kernel(const float* const* __restrict__ Aarray, int lda, const int* 
     const int prow = rvalid ? trace_backward<N>(pv, r) : r;
     const int base = seg * S::SEG;
 
-    float x = rvalid ? B[TRANS ? r : prow] : 0.0f;
-    if (!TRANS) {
+    float x = rvalid ? B[prow] : 0.0f;
 #pragma unroll
-        for (int j = 0; j < N; j++) {
-            const float xj = __shfl_sync(0xffffffffu, x, base + j);
-            if (r > j) x = fmaf(-lu[j], xj, x);
-        }
-#pragma unroll
-        for (int j = N - 1; j >= 0; j--) {
-            if (r == j) x = x / lu[j];
-            const float xj = __shfl_sync(0xffffffffu, x, base + j);
-            if (r < j) x = fmaf(-lu[j], xj, x);
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < N; j++) {
-            if (r == j) x = x / lu[j];
-            const float xj = __shfl_sync(0xffffffffu, x, base + j);
-            if (r > j) x = fmaf(-lu[j], xj, x);
-        }
-#pragma unroll
-        for (int i = N - 1; i >= 0; i--) {
-            const float xi = __shfl_sync(0xffffffffu, x, base + i);
-            if (r < i) x = fmaf(-lu[i], xi, x);
-        }
+    for (int j = 0; j < N; j++) {
+        const float xj = __shfl_sync(0xffffffffu, x, base + j);
+        if (r > j) x = fmaf(-lu[j], xj, x);
     }
-    if (rvalid) B[TRANS ? prow : r] = x;
+#pragma unroll
+    for (int j = N - 1; j >= 0; j--) {
+        if (r == j) x = x / lu[j];
+        const float xj = __shfl_sync(0xffffffffu, x, base + j);
+        if (r < j) x = fmaf(-lu[j], xj, x);
+    }
+    if (rvalid) B[r] = x;
 }
 
 // ---------------------------------------------------------------------------------------
-// nrhs >= 2, n <= 32: the reference's thread-per-right-hand-side structure
-// (sgetrs_batched_kernel.cpp:365-388) with B200 staging. A warp holds 32/LPM matrices; the LPM
+// n <= 32 with nrhs >= 2, or trans T / C with any nrhs: the reference's
+// thread-per-right-hand-side structure (sgetrs_batched_kernel.cpp:365-388) with B200
+// staging. A warp holds 32/LPM matrices; the LPM
 // lanes of a segment own right-hand sides c = q, q+LPM, ... of one matrix and keep that
 // column in registers. The matrix's LU is staged in shared memory by cp.async and read as
 // broadcast 16-byte column chunks; the interchanges become a row map computed once per
@@ -307,11 +297,11 @@ template <int N, bool TRANS>
 inline void launch_getrs_n(cudaStream_t st, const float* const* Aarray, int lda, const int* ipiv,
                            float* const* Barray, int ldb, int nrhs, int batch)
 {
-    if (nrhs == 1) {
+    if (!TRANS && nrhs == 1) {
         using S = SmallShape<N>;
         constexpr int per_cta = kSmallWarps * S::MPW;
         const unsigned grid = (unsigned)((batch + per_cta - 1) / per_cta);
-        getrs_small_kernel<N, TRANS><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, ipiv, Barray, ldb, batch);
+        getrs_small_kernel<N><<<grid, kSmallWarps * 32, 0, st>>>(Aarray, lda, ipiv, Barray, ldb, batch);
     } else if (nrhs <= 4) {
         launch_getrs_rhs<N, 4, TRANS>(st, Aarray, lda, ipiv, Barray, ldb, nrhs, batch);
     } else {

@@ -151,6 +151,45 @@ def test_grouped_against_oracle_sample(ob, handle, oracle_mod):
     plan.close()
 
 
+def _gather(flat, offs, span):
+    """Instances of one group out of a slab: rows of ``span`` floats at the given offsets."""
+    idx = np.asarray(offs, np.int64)[:, None] + np.arange(span, dtype=np.int64)[None, :]
+    return flat[idx]
+
+
+def test_grouped_configuration3_full_draw_against_oracle(ob, handle, oracle_mod):
+    """The grouped configuration in full: 50000 instances with n ~ U{4..128} (seed 0), nrhs = 1,
+    A and B i.i.d. N(0,1), one persistent launch. Every instance's LU, pivots, info and X equal
+    the oracle (the reference's unblocked getrf and trans-N getrs, restated) bit for bit."""
+    import torch
+
+    O = oracle_mod
+    nv = np.random.default_rng(0).integers(4, 129, size=50000)
+    ns = sorted(set(int(v) for v in nv), reverse=True)
+    sizes = [int((nv == n).sum()) for n in ns]
+    nrhss = [1] * len(ns)
+    d = _setup(ob, ns=ns, nrhss=nrhss, sizes=sizes, seed=7)
+    plan = ob.GroupedPlan(handle, ns, nrhss, sizes)
+    A, B, ap, bp, piv, info = _device(ob, d)
+    plan.run(handle, ap, piv, info, bp)
+    torch.cuda.synchronize()
+    plan.close()
+    a, b, p, inf = to_host(A), to_host(B), to_host(piv), to_host(info)
+    i = poff = 0
+    for n, sz in zip(ns, sizes):
+        ao, bo = d["a_offs"][i:i + sz], d["b_offs"][i:i + sz]
+        lu = _gather(d["a"], ao, n * n).reshape(sz, n, n)
+        x = _gather(d["b"], bo, n).reshape(sz, 1, n)
+        opiv, oinfo, _ = O.port_getrf(lu, n, n)
+        O.port_getrs("N", lu, n, n, opiv, x, 1, n)
+        _assert_same((_gather(a, ao, n * n).reshape(sz, n, n), _gather(b, bo, n).reshape(sz, 1, n),
+                      p[poff:poff + sz * n].reshape(sz, n), inf[i:i + sz]),
+                     (lu, x, opiv.reshape(sz, n), np.asarray(oinfo).reshape(-1)))
+        i += sz
+        poff += sz * n
+    assert i == 50000
+
+
 def test_grouped_cuda_graph_replay(ob):
     import torch
 

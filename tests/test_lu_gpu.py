@@ -3,9 +3,7 @@
 Two references:
   * the CPU oracle (oracle/lu_oracle.c, the reference kernels restated with one fmaf per
     update and true division): the CUDA kernels follow the same operation order, so factors,
-    pivots, info, solutions and inverses must agree BIT FOR BIT -- except the transposed solve
-    with a single right-hand side at n <= 32, whose L^T sweep accumulates in a different
-    order (tolerance below);
+    pivots, info, solutions and inverses must agree BIT FOR BIT;
   * the reference's own golden outputs (tests/golden/*.npz, LAPACK through the reference's
     golden headers): info exact, pivots exact when untied, factors under the reference's
     MIXED_TOLERANCE rule and 1e-5 normwise, solutions within the conditioning bound.
@@ -20,7 +18,7 @@ import pytest
 import oracle as O
 from cases import GETRF, GETRI, GETRS
 from conftest import to_dev, to_host
-from test_oracle_pin import GOLD, NORMWISE, TIE, block, c1_inputs, solution_ok
+from test_oracle_pin import GOLD, NORMWISE, TIE, c1_inputs, solution_ok
 
 pytestmark = pytest.mark.gpu
 
@@ -115,17 +113,30 @@ def test_getrf_csv(handle, c):
 def test_getrs_csv(handle, c):
     a = O.case_matrices(c.n, c.lda, c.mtype, c.seed, c.batch)
     b = O.case_rhs(c.n, c.nrhs, c.ldb, c.seed, c.batch)
-    piv, rf, _ = O.port_getrf(a, c.n, c.lda, c.pivot)
+    piv, _, _ = O.port_getrf(a, c.n, c.lda, c.pivot)
     x, hinfo = gpu_getrs(handle, c.trans, a, c.n, c.lda, piv if c.pivot else None, b, c.nrhs, c.ldb)
     assert hinfo == 0
     ox = b.copy()
     O.port_getrs(c.trans, a, c.n, c.lda, piv if c.pivot else None, ox, c.nrhs, c.ldb)
-    if c.trans == "N" or c.n > 32 or c.nrhs > 1:
-        assert_bitwise(x, ox, "X")
-    else:
-        for k in range(c.batch):
-            if rf[k] == 0:
-                assert O.mixed_tolerance_ok(block(x[k:k + 1], c.n, c.nrhs), block(ox[k:k + 1], c.n, c.nrhs)), k
+    assert_bitwise(x, ox, "X")
+
+
+@pytest.mark.parametrize("n", list(range(1, 33)))
+def test_getrs_transposed_single_rhs_bitwise(handle, n):
+    """trans T / C with one right-hand side at every n <= 32 (padded lda and ldb, a batch that
+    is not a multiple of the per-CTA count): the U^T and L^T sweeps add each x[j]'s terms in the
+    reference's order, so X equals the oracle bit for bit."""
+    rng = np.random.default_rng(300 + n)
+    batch, lda, ldb = 37, n + 1, n + 2
+    a = rng.standard_normal((batch, n, lda)).astype(np.float32)
+    piv, _, _ = O.port_getrf(a, n, lda)
+    b = rng.standard_normal((batch, 1, ldb)).astype(np.float32)
+    for trans in ("T", "C"):
+        x, hinfo = gpu_getrs(handle, trans, a, n, lda, piv, b, 1, ldb)
+        assert hinfo == 0
+        ox = b.copy()
+        O.port_getrs(trans, a, n, lda, piv, ox, 1, ldb)
+        assert_bitwise(x, ox, f"X {trans} n={n}")
 
 
 @pytest.mark.parametrize("c", [c for c in GETRI if c.status == "SUCCESS" and c.n > 0 and c.batch > 0],
