@@ -1,11 +1,16 @@
-// Mixed-precision batched LU for 256 < n <= 1024: blocked right-looking, panels of 32 columns,
-// the trailing update on the tcgen05 tensor cores.
-//
-// Used by aclblasSgetrfsRefineBatchedEx with ACLBLAS_COMPUTE_32F_FAST_TF32 when the matrix no
-// longer fits one SM's tensor memory (getrf_tmem.cu covers n <= 256). The factorisation works on
-// the matrix stored by rows (T(i, j) at LU[j + i * ldlu]): a row is contiguous, so pivot rows,
-// interchanges and the panel's rows are whole cache lines, where by columns every row element is
-// a separate sector.
+// Blocked batched LU on the matrix stored by rows, panels of 32 columns, two variants:
+//   * plain FP32 getrf for 128 < n <= 1024 (aclblasSgetrfBatched, getrf_rows_launch): the
+//     reference's arithmetic -- first-maximum pivot on exact magnitudes, true division, stop at
+//     the first exactly-zero pivot -- and a tiled CUDA-core trailing update that applies the
+//     rank-1 updates one fmaf at a time in the reference's order: bit-identical to it;
+//   * mixed precision for 256 < n <= 1024 (aclblasSgetrfsRefineBatchedEx with
+//     ACLBLAS_COMPUTE_32F_FAST_TF32, once the matrix no longer fits one SM's tensor memory:
+//     getrf_tmem.cu covers n <= 256; getrf_blocked_tc_launch): the trailing update on the tcgen05
+//     tensor cores in split TF32.
+// Both work on the matrix stored by rows (T(i, j) at LU[j + i * ldlu]): a row is contiguous, so
+// pivot rows, interchanges and the panel's rows are whole cache lines, where by columns every row
+// element is a separate sector. The steps below describe the mixed variant; the plain one differs
+// where lu_panel_kernel's EXACT says and runs lu_rows_update_kernel as its update.
 //   0. lu_rows_in_kernel: A (by columns) into LU by rows, 32 x 32 tiles through shared memory.
 //   Per panel k0 = 0, 32, ...:
 //   1. lu_panel_kernel, one CTA per matrix, two panel rows a thread:
